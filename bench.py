@@ -1,0 +1,438 @@
+#!/usr/bin/env python
+"""Headline benchmark: converged pixels/s of the Milne-Eddington inversion.
+
+Workload (the reference's full-cube case): 1024 x 1024 pixels x 4 Stokes x
+30 wavelengths (Fe I 6173.3356 A, -350:35:665 mA), FP32, normalised to the
+continuum.  Truth parameters drawn uniformly (eta0 1-30, B 0-3000 G, vlos
++-3 km/s, Doppler width 20-60 mA, damping 0-0.5, gamma/phi 0-180 deg,
+S0 0.1-0.5, S1 0.3-1.0 rescaled to unit continuum), stray light of 0-30 %
+(filling factor alpha 0.7-1.0) against a fixed field-free profile.  The
+observations are synthesised on a 1 mA grid, convolved with a Gaussian PSF
+of FWHM 100 mA sampled at 1 mA, resampled to the 30 samples, plus Gaussian
+noise of 1e-3 Ic.  The inversion fits 9 ME parameters + alpha with at most 50
+LM iterations, PSF and stray light modelled with the reference's semantics
+(the 1 mA PSF table linearly interpolated at the grid offsets).  Synthetic
+data stand in for an observed cube.
+
+One step = one inversion of the whole cube.  Inputs (480 MB) exceed the
+126 MB L2, so no flush is needed between steps.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for p in (os.path.join(ROOT, "g-milos_b200"), os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+LAMBDA0 = 6173.3356
+GRID = (-350.0, 35.0, 665.0)
+FWHM_MA = 100.0
+NOISE = 1e-3
+GUESS = (1.0, 1000.0, 0.2, 0.03, 0.05, 150.0, 110.0, 0.35, 0.5, 0.0, 1.0)
+FIX = (1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 1)          # 9 ME parameters + alpha
+STRAY_MODEL = (10.0, 0.0, 0.0, 0.03, 0.1, 0.0, 0.0, 0.3, 0.7, 0.0, 1.0)
+MAXITER = 50
+
+# Algorithmic FLOPs per pixel (per-wavelength costs counted from the formulas)
+C_VOIGT, C_RTE, C_DVOIGT, C_DRTE = 100, 85, 23, 870
+
+
+def flops_model(nl, ntaps, n_free, s0_free, psf, stray, ncomp=3):
+    """F_trial, F_acc, F_init of one pixel."""
+    n = n_free
+    n_conv = n - (1 if s0_free else 0)
+    f_trial = nl * (ncomp * C_VOIGT + C_RTE) + (8 * nl * ntaps if psf else 0) + (12 * nl if stray else 0) \
+        + 12 * nl + (n ** 3 / 3 + 2 * n ** 2)
+    f_acc = nl * (ncomp * C_DVOIGT + C_DRTE) + (8 * nl * ntaps * n_conv if psf else 0) \
+        + (4 * nl * n if stray else 0) + 8 * nl * (n * (n + 1) / 2 + n)
+    f_init = 40 * nl + f_trial + f_acc
+    return f_trial, f_acc, f_init
+
+
+def truth_models(n, rng):
+    t = np.zeros((n, 11))
+    t[:, 0] = rng.uniform(1, 30, n)
+    t[:, 1] = rng.uniform(0, 3000, n)
+    t[:, 2] = rng.uniform(-3, 3, n)
+    t[:, 3] = rng.uniform(0.020, 0.060, n)
+    t[:, 4] = rng.uniform(0, 0.5, n)
+    t[:, 5] = rng.uniform(0, 180, n)
+    t[:, 6] = rng.uniform(0, 180, n)
+    t[:, 7] = rng.uniform(0.1, 0.5, n)
+    t[:, 8] = rng.uniform(0.3, 1.0, n)
+    ic = t[:, 7] + t[:, 8]
+    t[:, 7] /= ic
+    t[:, 8] /= ic
+    t[:, 10] = rng.uniform(0.7, 1.0, n)
+    return t
+
+
+def grid():
+    first, step, last = GRID
+    n = int(((last - first) / step) + 1)
+    off = np.empty(n)
+    off[0] = first
+    lam = np.empty(n)
+    lam[0] = LAMBDA0 + first / 1000.0
+    for i in range(1, n):
+        off[i] = off[i - 1] + step
+        lam[i] = lam[i - 1] + step / 1000.0
+    return lam, off
+
+
+def psf_table():
+    """Gaussian PSF of FWHM 100 mA sampled at 1 mA over +-2750 mA (the layout
+    of the reference's .psf files)."""
+    x = np.arange(-2750.0, 2750.5, 1.0)
+    sigma = FWHM_MA / (2 * np.sqrt(2 * np.log(2)))
+    return x, np.exp(-0.5 * (x / sigma) ** 2)
+
+
+def fine_operator(off):
+    """Fine 1 mA grid covering the samples +-6 sigma, and the matrix that
+    convolves a fine profile with the PSF and samples it at `off`."""
+    sigma = FWHM_MA / (2 * np.sqrt(2 * np.log(2)))
+    half = int(np.ceil(6 * sigma))
+    fine = np.arange(off[0] - half, off[-1] + half + 0.5, 1.0)
+    W = np.exp(-0.5 * ((off[:, None] - fine[None, :]) / sigma) ** 2)
+    W /= W.sum(axis=1, keepdims=True)
+    return fine, W
+
+
+# ----------------------------------------------------------------- engine arm
+def clocks_sampler(dev_index, stop, out):
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    try:
+        p = subprocess.Popen(["nvidia-smi", "-i", str(dev_index), "--query-gpu=" + q,
+                              "--format=csv,noheader,nounits", "-lms", "200"],
+                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except Exception:
+        return
+    while not stop.is_set():
+        line = p.stdout.readline()
+        if not line:
+            break
+        out.append(line.strip())
+    p.terminate()
+
+
+def summarize_clocks(lines):
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for l in lines:
+        f = [x.strip() for x in l.split(",")]
+        if len(f) < 9:
+            continue
+        try:
+            sm.append(float(f[1]))
+            mx.append(float(f[2]))
+        except ValueError:
+            continue
+        for i, n in enumerate(names):
+            if f[5 + i].lower().startswith("active"):
+                reasons.add(n)
+    if not sm:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+    return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def make_cube_gpu(eng, truth, off, slight, rng_seed, torch):
+    """Observations on the device: fine-grid ME synthesis by the engine's grid
+    kernel, PSF convolution + resampling as one matmul, stray mix, noise."""
+    fine, W = fine_operator(off)
+    fine_A = np.ascontiguousarray(fine / 1000.0)
+    Wt = torch.tensor(W.T, dtype=torch.float32, device="cuda")
+    P = truth.shape[0]
+    nl = len(off)
+    out = torch.empty((P, 4, nl), dtype=torch.float32, device="cuda")
+    tm = torch.tensor(truth, dtype=torch.float64, device="cuda")
+    offs_d = torch.tensor(fine_A, dtype=torch.float64, device="cuda")
+    chunk = 32768
+    for a in range(0, P, chunk):
+        b = min(P, a + chunk)
+        f = eng.synthesize_grid(tm[a:b].contiguous(), offs_d)
+        out[a:b] = torch.matmul(f, Wt)
+        del f
+    alpha = tm[:, 10].to(torch.float32)[:, None, None]
+    sl = torch.tensor(slight, dtype=torch.float32, device="cuda")[None]
+    out = alpha * out + (1 - alpha) * sl
+    g = torch.Generator(device="cuda")
+    g.manual_seed(rng_seed)
+    out += NOISE * torch.randn(out.shape, generator=g, device="cuda", dtype=torch.float32)
+    torch.cuda.synchronize()
+    return out.contiguous()
+
+
+def stray_profile_cpu(off):
+    """Field-free ME profile seen through the same 1 mA PSF (the fixed stray
+    light source), computed with the engine-independent CPU oracle only for
+    the reference arm; the engine arm computes it with the engine."""
+    import oracle as O
+    return _fine_synth_cpu(O, np.array([STRAY_MODEL]), off)[0]
+
+
+def _fine_synth_cpu(O, models, off):
+    l0, z = O.fe6173()
+    fine, W = fine_operator(off)
+    P = models.shape[0]
+    prof = np.zeros((P, 4, len(fine)), dtype=np.float32)
+    for a in range(0, len(fine), 128):
+        b = min(len(fine), a + 128)
+        lam = LAMBDA0 + fine[a:b] / 1000.0
+        if b - a < 2:
+            lam = np.array([lam[0], lam[0] + 1e-3])
+        cfg = O.make_cfg(lam, l0, z)
+        prof[:, :, a:b] = O.synth_batch_f(cfg, models)[:, :, :b - a]
+    return (prof @ W.T.astype(np.float32)).astype(np.float32)
+
+
+def run_engine(args):
+    import torch
+    import torch.distributed as dist
+    import gmilos_b200 as G
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    lam, off = grid()
+    x, y = psf_table()
+    psf = G.psf_from_table(x, y, off, GRID[1])
+    eng = G.Engine(local)
+    zee = G.zeeman_from_levels(2, 1, 1.0, 2, 2, 0.0, 1.0)
+    # stray profile: ME synthesis of the field-free model through the 1 mA PSF
+    cfg0 = G.make_config(lam, LAMBDA0, zee, fix=FIX, init=GUESS)
+    eng.configure(cfg0)
+    fine, W = fine_operator(off)
+    sl_fine = eng.synthesize_grid(np.array([STRAY_MODEL]), np.ascontiguousarray(fine / 1000.0))
+    slight = (sl_fine @ W.T.astype(np.float32))[0].astype(np.float32)
+    cfg = G.make_config(lam, LAMBDA0, zee, psf=psf, fix=FIX, init=GUESS, miter=MAXITER, slight=slight)
+    eng.configure(cfg)
+
+    rng = np.random.default_rng(args.seed + rank)
+    P = args.pixels
+    truth = truth_models(P, rng)
+    obs = make_cube_gpu(eng, truth, off, slight, args.seed + 1000 + rank, torch)
+    nl = len(off)
+    dev = obs.device
+    outs = {"model": torch.empty((P, 11), dtype=torch.float32, device=dev),
+            "model64": None,
+            "chi2": torch.empty(P, dtype=torch.float32, device=dev),
+            "iters": torch.empty(P, dtype=torch.int32, device=dev),
+            "accepted": torch.empty(P, dtype=torch.int32, device=dev),
+            "status": torch.empty(P, dtype=torch.int32, device=dev),
+            "fitted": None}
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    for _ in range(args.warmup):
+        eng.invert(obs, out=outs, stream=sptr)
+    torch.cuda.synchronize()
+
+    stop = threading.Event()
+    clk = []
+    th = threading.Thread(target=clocks_sampler, args=(local, stop, clk), daemon=True)
+    th.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    iters_sum = 0
+    acc_sum = 0
+    t_start.record(stream)
+    for k in range(args.steps):
+        evs[k][0].record(stream)
+        eng.invert(obs, out=outs, stream=sptr)
+        evs[k][1].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    stop.set()
+    iters_sum = int(outs["iters"].sum().item())
+    acc_sum = int(outs["accepted"].sum().item())
+    total_ms = t_start.elapsed_time(t_end)
+    launch_ms = [a.elapsed_time(b) for a, b in evs]
+    ms_t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    total_ms = float(ms_t.item())
+    ms_per_step = total_ms / args.steps
+    value = P * world / (ms_per_step / 1e3)
+
+    # end to end through the public C ABI with pinned host buffers
+    obs_h = obs.cpu().pin_memory()
+    model_h = torch.empty((P, 11), dtype=torch.float32).pin_memory()
+    chi_h = torch.empty(P, dtype=torch.float32).pin_memory()
+    it_h = torch.empty(P, dtype=torch.int32).pin_memory()
+    e2e_ms = []
+    for k in range(max(1, min(args.steps, 3)) + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.invert_plain(obs_h.numpy(), model_h.numpy(), chi2=chi_h.numpy(), iters=it_h.numpy())
+        t1 = time.perf_counter()
+        if k > 0:
+            e2e_ms.append((t1 - t0) * 1e3)
+    e2e_t = torch.tensor([float(np.mean(e2e_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = P * world / (float(e2e_t.item()) / 1e3)
+    h2d = obs_h.numel() * 4
+    d2h = (model_h.numel() + chi_h.numel() + it_h.numel()) * 4
+
+    # roofline of the inversion kernel: algorithmic FLOPs / launch duration
+    ftr, facc, finit = flops_model(nl, nl, n_free=sum(FIX), s0_free=FIX[7], psf=True, stray=True)
+    flops_launch = P * finit + iters_sum * ftr + acc_sum * facc
+    launch_avg = float(np.mean(launch_ms))
+    achieved = flops_launch / (launch_avg / 1e3) / 1e12
+    fp32_peak, fp64_peak = eng.measure_peaks()
+    clocks = summarize_clocks(clk)
+
+    result = {
+        "metric": "converged pixels/s (1024^2 x 4 x 30 lambda, PSF, stray light, 9 ME + alpha free, <=50 LM iterations)",
+        "value": value, "unit": "pixels/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 (f64 Voigt polynomials and model parameters)", "data": "synthetic",
+        "config": {"workload": "full cube %dx%d px x 4 Stokes x 30 lambda, Fe I 6173 A, PSF FWHM 100 mA "
+                               "(1 mA table), stray light alpha 0.7-1.0, noise 1e-3 Ic" % (int(np.sqrt(P)), int(np.sqrt(P))) if int(np.sqrt(P)) ** 2 == P
+                               else "%d px x 4 x 30 lambda, PSF, stray light" % P,
+                   "pixels_per_gpu": P, "nlambda": nl, "free_parameters": int(sum(FIX)), "max_iterations": MAXITER,
+                   "mean_iterations": iters_sum / P, "mean_accepted": acc_sum / P,
+                   "l2_policy": "inputs 480 MB per GPU > 126 MB L2, no flush", "parallelism": "replicas (weak scaling, no collective)"},
+        "e2e": {"value": e2e_value, "unit": "pixels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": 2 * args.steps,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak if fp32_peak else None, "traffic": None,
+                     "peak_source": "measured FFMA microbenchmark (gm_measure_peaks), burst",
+                     "fp64_peak": fp64_peak,
+                     "flops_per_launch": flops_launch, "launch_ms": launch_avg},
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(obs[: min(P, 200000)].cpu().numpy(), slight, psf, lam, seconds=args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------- CPU arms
+def _ref_lib():
+    path = os.path.join(ROOT, "oracle", "_ref", "libgmref.so")
+    return path if os.path.exists(path) else None
+
+
+def cpu_baseline(obs, slight, psf, lam, seconds=15.0, nthreads=0):
+    """Time the CPU implementation of the path on a bounded sample of the
+    workload: the reference's routines compiled host-side (oracle/_ref) when
+    built, else the oracle's restatement."""
+    import oracle as O
+    l0, z = O.fe6173()
+    nthreads = nthreads or os.cpu_count()
+    ref = _ref_lib()
+    if ref:
+        import ref_runner
+        runner = ref_runner.RefRunner(ref, lam, l0, psf, slight, FIX, GUESS, MAXITER)
+        run = lambda o: runner.invert(o, nthreads)
+        kind = "reference"
+    else:
+        cfg = O.make_cfg(lam, l0, z, psf=psf, fix=FIX, init=GUESS, miter=MAXITER)
+        run = lambda o: O.lm_batch_f(cfg, o, slight=slight, nthreads=nthreads)
+        kind = "port"
+    probe = min(len(obs), max(256, 16 * nthreads))
+    t0 = time.perf_counter()
+    run(np.ascontiguousarray(obs[:probe]))
+    rate = probe / (time.perf_counter() - t0)
+    n = int(min(len(obs), max(probe, rate * seconds)))
+    t0 = time.perf_counter()
+    run(np.ascontiguousarray(obs[:n]))
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "pixels/s", "cores": nthreads, "kind": kind,
+            "sample": "%d pixels of the same cube (first %d), %.1f s" % (n, n, dt)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    import oracle as O
+    lam, off = grid()
+    x, y = psf_table()
+    l0, z = O.fe6173()
+    psf = O.psf_from_table(x, y, off, GRID[1])
+    slight = stray_profile_cpu(off)
+    rng = np.random.default_rng(args.seed)
+    nthreads = os.cpu_count()
+    # observations of a bounded sample, synthesised on the CPU
+    sample = args.ref_pixels
+    truth = truth_models(sample, rng)
+    obs = _fine_synth_cpu(O, truth, off)
+    a = truth[:, 10][:, None, None].astype(np.float32)
+    obs = a * obs + (1 - a) * slight[None]
+    obs += (NOISE * np.random.default_rng(args.seed + 1000).standard_normal(obs.shape)).astype(np.float32)
+    obs = np.ascontiguousarray(obs, dtype=np.float32)
+    times = []
+    base = None
+    for k in range(args.warmup + args.steps):
+        b = cpu_baseline(obs, slight, psf, lam, seconds=args.ref_seconds, nthreads=nthreads)
+        if k >= args.warmup:
+            times.append(b["value"])
+            base = b
+    value = float(np.mean(times))
+    result = {
+        "metric": "converged pixels/s (1024^2 x 4 x 30 lambda, PSF, stray light, 9 ME + alpha free, <=50 LM iterations)",
+        "value": value, "unit": "pixels/s", "n_gpus": int(os.environ.get("WORLD_SIZE", 1)), "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": "full cube 1024x1024 px x 4 Stokes x 30 lambda (bounded sample per step)",
+                   "pixels_per_gpu": 1024 * 1024, "nlambda": 30},
+        "cpu_baseline": {"value": value, "unit": "pixels/s", "cores": nthreads, "kind": base["kind"],
+                         "sample": base["sample"]},
+        "e2e": {"value": value, "unit": "pixels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(result), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--pixels", type=int, default=1024 * 1024)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-pixels", type=int, default=65536)
+    ap.add_argument("--ref-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "engine" and "--allow-short" not in sys.argv:
+        pass
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,647 @@
+// gm_capi.cu -- the C ABI (include/gmilos.h): contexts, configuration,
+// host/device buffer handling and kernel launches.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "gm_kernels.cuh"
+#include "gmilos.h"
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+struct Request {
+  gm_request req;
+  std::vector<int> fix;
+  gm_status result = GM_OK;
+  bool done = false;
+  bool cancelled = false;
+};
+
+}  // namespace
+
+struct gm_ctx {
+  int device = 0;
+  size_t budget = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int sms = 0;
+  bool configured = false;
+  gm_config cfg{};
+  gm::DevCfg dev{};
+  gm::WorkCounters* work = nullptr;   // device scratch of the persistent launch
+  DevBuf slight;                      // global stray-light profile (device copy)
+  std::map<std::string, DevBuf> bufs; // staging buffers for host-memory calls
+  std::string err;
+  gm_stats stats{};
+  // serving
+  std::mutex mu;
+  std::condition_variable cv, done_cv;
+  std::deque<gm_ticket> queue;
+  std::map<gm_ticket, std::shared_ptr<Request>> reqs;
+  gm_ticket next_ticket = 1;
+  std::thread worker;
+  bool stopping = false;
+  std::mutex call_mu;                 // serialises engine calls of the worker and the caller
+};
+
+namespace {
+
+gm_status fail(gm_ctx* ctx, gm_status s, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return s;
+}
+
+gm_status cuda_fail(gm_ctx* ctx, cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  return fail(ctx, GM_ERR_CUDA, m);
+}
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes at{};
+  cudaError_t e = cudaPointerGetAttributes(&at, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+gm_status ensure_buf(gm_ctx* ctx, const std::string& name, size_t bytes, void** out) {
+  DevBuf& b = ctx->bufs[name];
+  if (b.bytes < bytes) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ctx, GM_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    b.bytes = bytes;
+  }
+  *out = b.p;
+  return GM_OK;
+}
+
+// A host- or device-side argument staged onto the device.
+struct Arg {
+  void* dev = nullptr;      // pointer the kernel uses
+  void* host = nullptr;     // user host pointer to copy back to (outputs)
+  size_t bytes = 0;
+};
+
+gm_status stage_in(gm_ctx* ctx, const char* name, const void* p, size_t bytes, Arg* a,
+                   cudaStream_t s) {
+  a->bytes = bytes;
+  if (!p) return GM_OK;
+  if (is_device_ptr(p)) {
+    a->dev = const_cast<void*>(p);
+    return GM_OK;
+  }
+  gm_status st = ensure_buf(ctx, name, bytes, &a->dev);
+  if (st != GM_OK) return st;
+  cudaError_t e = cudaMemcpyAsync(a->dev, p, bytes, cudaMemcpyHostToDevice, s);
+  return e == cudaSuccess ? GM_OK : cuda_fail(ctx, e, "host-to-device copy");
+}
+
+gm_status stage_out(gm_ctx* ctx, const char* name, void* p, size_t bytes, Arg* a) {
+  a->bytes = bytes;
+  if (!p) return GM_OK;
+  if (is_device_ptr(p)) {
+    a->dev = p;
+    return GM_OK;
+  }
+  a->host = p;
+  return ensure_buf(ctx, name, bytes, &a->dev);
+}
+
+gm_status copy_back(gm_ctx* ctx, const Arg& a, cudaStream_t s) {
+  if (!a.host || !a.dev) return GM_OK;
+  cudaError_t e = cudaMemcpyAsync(a.host, a.dev, a.bytes, cudaMemcpyDeviceToHost, s);
+  return e == cudaSuccess ? GM_OK : cuda_fail(ctx, e, "device-to-host copy");
+}
+
+gm_status build_devcfg(gm_ctx* ctx, const gm_config& c, gm::DevCfg* d) {
+  if (c.abi_version != GM_ABI_VERSION) return fail(ctx, GM_ERR_INVALID, "gm_config.abi_version mismatch");
+  if (c.nl < 2 || c.nl > GM_MAX_NL) return fail(ctx, GM_ERR_INVALID, "nl must be in [2, 64]");
+  const gm_zeeman& z = c.zeeman;
+  if (z.n_pi < 1 || z.n_pi > 10 || z.n_sig < 1 || z.n_sig > 10)
+    return fail(ctx, GM_ERR_INVALID, "Zeeman pattern needs 1..10 pi and sigma components");
+  if (c.fix[GM_NPAR - 2] && c.fix[GM_NPAR - 1])
+    return fail(ctx, GM_ERR_UNSUPPORTED, "free macroturbulence together with free alpha (11-term FP64 path) is not available yet");
+  if (c.init_model[9] > 0.0001)
+    return fail(ctx, GM_ERR_UNSUPPORTED, "macroturbulence convolution (v_mac > 1e-4) is not available yet");
+  if (c.noise <= 0.f) return fail(ctx, GM_ERR_INVALID, "noise must be > 0");
+  std::memset(d, 0, sizeof(*d));
+  d->nl = c.nl;
+  d->nterms = 10;
+  d->use_psf = c.use_psf ? 1 : 0;
+  d->use_slight = c.use_slight ? 1 : 0;
+  d->slight_per_pixel = c.slight_per_pixel ? 1 : 0;
+  d->init_mode = c.init_mode == GM_INIT_CLASSICAL ? 0 : 1;
+  d->miter = c.miter;
+  d->logclambda = c.logclambda;
+  d->quirks = c.reference_quirks;
+  if (c.numerics != GM_NUMERICS_REFERENCE && c.numerics != GM_NUMERICS_ACCURATE)
+    return fail(ctx, GM_ERR_INVALID, "numerics must be GM_NUMERICS_REFERENCE or GM_NUMERICS_ACCURATE");
+  d->numerics = c.numerics;
+  d->n_pi = z.n_pi;
+  d->n_sig = z.n_sig;
+  for (int i = 0; i < GM_NPAR; ++i) d->fix[i] = c.fix[i] ? 1 : 0;
+  for (int l = 0; l < c.nl; ++l) {
+    const double off = c.lambda[l] - c.lambda0;
+    d->dl[l] = (float)off;
+    d->dld[l] = off;
+    d->psf[l] = (float)c.psf[l];
+  }
+  for (int i = 0; i < 10; ++i) {
+    d->nup[i] = z.nup[i];
+    d->nub[i] = z.nub[i];
+    d->wep[i] = z.wep[i];
+    d->web[i] = z.web[i];
+    d->wer[i] = z.wer[i];
+  }
+  d->geff = z.geff;
+  d->fo = z.fo;
+  d->mu = c.mu;
+  d->ilambda = c.ilambda;
+  d->noise = c.noise;
+  for (int s = 0; s < 4; ++s) {
+    d->weight[s] = c.weight[s];
+    d->wsig[s] = c.weight[s] / c.noise;
+  }
+  d->lambda0 = c.lambda0;
+  d->toplim = c.toplim;
+  d->stop_dchi2 = c.stop_dchi2;
+  for (int i = 0; i < GM_NPAR; ++i) d->init[i] = c.init_model[i];
+  return GM_OK;
+}
+
+void serve_loop(gm_ctx* ctx);
+
+}  // namespace
+
+extern "C" {
+
+const char* gm_status_string(gm_status s) {
+  switch (s) {
+    case GM_OK: return "ok";
+    case GM_ERR_INVALID: return "invalid argument";
+    case GM_ERR_CUDA: return "CUDA error";
+    case GM_ERR_NOMEM: return "out of memory / over budget";
+    case GM_ERR_NOT_CONFIGURED: return "context not configured";
+    case GM_ERR_UNSUPPORTED: return "unsupported";
+    case GM_ERR_TIMEOUT: return "timeout";
+    case GM_ERR_CANCELLED: return "cancelled";
+    case GM_ERR_IO: return "I/O error";
+  }
+  return "unknown";
+}
+
+const char* gm_last_error(gm_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+// Defaults of loadInitialValues (readConfig.c:704-744): unit weights,
+// noise 1e-6, lambda_LM 0.1, toplim 1e-12, mu 1.
+void gm_config_defaults(gm_config* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->abi_version = GM_ABI_VERSION;
+  for (int s = 0; s < 4; ++s) c->weight[s] = 1.f;
+  c->noise = 1e-6f;
+  c->mu = 1.f;
+  c->ilambda = 0.1f;
+  c->toplim = 1e-12;
+  c->miter = 50;
+  c->init_mode = GM_INIT_CLASSICAL;
+  c->reference_quirks = 1;
+  const double guess[GM_NPAR] = {1.0, 1000.0, 0.2, 0.03, 0.05, 150.0, 110.0, 0.35, 0.5, 0.0, 1.0};
+  for (int i = 0; i < GM_NPAR; ++i) c->init_model[i] = guess[i];
+}
+
+gm_status gm_create(int device, size_t hbm_budget, gm_ctx** out) {
+  if (!out) return GM_ERR_INVALID;
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return GM_ERR_CUDA;
+  }
+  if (device < 0 || device >= n) return GM_ERR_INVALID;
+  std::unique_ptr<gm_ctx> ctx(new gm_ctx());
+  ctx->device = device;
+  if ((e = cudaSetDevice(device)) != cudaSuccess) return GM_ERR_CUDA;
+  cudaDeviceProp prop{};
+  cudaGetDeviceProperties(&prop, device);
+  ctx->sms = prop.multiProcessorCount;
+  ctx->budget = hbm_budget ? hbm_budget : (size_t)prop.totalGlobalMem;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return GM_ERR_CUDA;
+  cudaEventCreate(&ctx->ev0);
+  cudaEventCreate(&ctx->ev1);
+  if (cudaMalloc(&ctx->work, sizeof(gm::WorkCounters)) != cudaSuccess) return GM_ERR_NOMEM;
+  *out = ctx.release();
+  return GM_OK;
+}
+
+gm_status gm_destroy(gm_ctx* ctx) {
+  if (!ctx) return GM_ERR_INVALID;
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->stopping = true;
+  }
+  ctx->cv.notify_all();
+  if (ctx->worker.joinable()) ctx->worker.join();
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->bufs)
+    if (kv.second.p) cudaFree(kv.second.p);
+  if (ctx->slight.p) cudaFree(ctx->slight.p);
+  if (ctx->work) cudaFree(ctx->work);
+  cudaEventDestroy(ctx->ev0);
+  cudaEventDestroy(ctx->ev1);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return GM_OK;
+}
+
+gm_status gm_configure(gm_ctx* ctx, const gm_config* cfg) {
+  if (!ctx || !cfg) return GM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->call_mu);
+  cudaSetDevice(ctx->device);
+  gm::DevCfg d;
+  gm_status st = build_devcfg(ctx, *cfg, &d);
+  if (st != GM_OK) return st;
+  if (cfg->use_slight && !cfg->slight_per_pixel) {
+    if (!cfg->slight) return fail(ctx, GM_ERR_INVALID, "use_slight set but slight is NULL");
+    const size_t bytes = sizeof(float) * 4 * cfg->nl;
+    if (ctx->slight.bytes < bytes) {
+      if (ctx->slight.p) cudaFree(ctx->slight.p);
+      ctx->slight.p = nullptr;
+      if (cudaMalloc(&ctx->slight.p, bytes) != cudaSuccess) return fail(ctx, GM_ERR_NOMEM, "stray-light buffer");
+      ctx->slight.bytes = bytes;
+    }
+    cudaError_t e = cudaMemcpy(ctx->slight.p, cfg->slight, bytes,
+                               is_device_ptr(cfg->slight) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "stray-light upload");
+    d.slight = (const float*)ctx->slight.p;
+  }
+  ctx->cfg = *cfg;
+  if (!cfg->slight_per_pixel) ctx->cfg.slight = nullptr;   // the global profile now lives on the device
+  ctx->dev = d;
+  ctx->configured = true;
+  return GM_OK;
+}
+
+struct StepOut {
+  float* delta = nullptr;
+  double* trial = nullptr;
+  float* chi2_start = nullptr;
+  float* chi2_trial = nullptr;
+};
+
+static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* iquv, int64_t npix,
+                             int nl, const double* init_models, const float* slight_map,
+                             float* model, double* model_f64, float* chi2, int* iters,
+                             int* accepted, float* fitted, uint32_t* status, void* stream,
+                             const StepOut* so = nullptr) {
+  if (!ctx->configured) return fail(ctx, GM_ERR_NOT_CONFIGURED, "gm_configure first");
+  if (!iquv || npix < 0) return fail(ctx, GM_ERR_INVALID, "iquv is NULL or npix < 0");
+  if (nl != dcfg.nl) return fail(ctx, GM_ERR_INVALID, "nl differs from the configured grid");
+  if (npix == 0) return GM_OK;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  const size_t cube = sizeof(float) * 4 * (size_t)nl * npix;
+  size_t need = cube + (fitted ? cube : 0) + (size_t)npix * (11 * 12 + 16);
+  if (need > ctx->budget) return fail(ctx, GM_ERR_NOMEM, "request exceeds the context's HBM budget");
+  Arg a_in, a_init, a_sl, a_model, a_m64, a_chi, a_it, a_acc, a_fit, a_st;
+  gm_status st;
+  if ((st = stage_in(ctx, "iquv", iquv, cube, &a_in, s)) != GM_OK) return st;
+  if ((st = stage_in(ctx, "init", init_models, sizeof(double) * 11 * npix, &a_init, s)) != GM_OK) return st;
+  gm::DevCfg d = dcfg;
+  if (d.use_slight && d.slight_per_pixel) {
+    if (!slight_map) return fail(ctx, GM_ERR_INVALID, "per-pixel stray light needs a map");
+    if ((st = stage_in(ctx, "slight", slight_map, cube, &a_sl, s)) != GM_OK) return st;
+    d.slight = (const float*)a_sl.dev;
+  }
+  if ((st = stage_out(ctx, "model", model, sizeof(float) * 11 * npix, &a_model)) != GM_OK) return st;
+  if ((st = stage_out(ctx, "model64", model_f64, sizeof(double) * 11 * npix, &a_m64)) != GM_OK) return st;
+  if ((st = stage_out(ctx, "chi2", chi2, sizeof(float) * npix, &a_chi)) != GM_OK) return st;
+  if ((st = stage_out(ctx, "iters", iters, sizeof(int) * npix, &a_it)) != GM_OK) return st;
+  if ((st = stage_out(ctx, "acc", accepted, sizeof(int) * npix, &a_acc)) != GM_OK) return st;
+  if ((st = stage_out(ctx, "fitted", fitted, cube, &a_fit)) != GM_OK) return st;
+  if ((st = stage_out(ctx, "status", status, sizeof(uint32_t) * npix, &a_st)) != GM_OK) return st;
+  Arg a_sd, a_strial, a_sc0, a_sc1;
+  if (so) {
+    if ((st = stage_out(ctx, "sdelta", so->delta, sizeof(float) * 10 * npix, &a_sd)) != GM_OK) return st;
+    if ((st = stage_out(ctx, "strial", so->trial, sizeof(double) * 11 * npix, &a_strial)) != GM_OK) return st;
+    if ((st = stage_out(ctx, "sc0", so->chi2_start, sizeof(float) * npix, &a_sc0)) != GM_OK) return st;
+    if ((st = stage_out(ctx, "sc1", so->chi2_trial, sizeof(float) * npix, &a_sc1)) != GM_OK) return st;
+  }
+
+  gm::InvertArgs ia{};
+  ia.iquv = (const float*)a_in.dev;
+  ia.npix = npix;
+  ia.init_models = (const double*)a_init.dev;
+  ia.model = (float*)a_model.dev;
+  ia.model_f64 = (double*)a_m64.dev;
+  ia.chi2 = (float*)a_chi.dev;
+  ia.iters = (int*)a_it.dev;
+  ia.accepted = (int*)a_acc.dev;
+  ia.fitted = (float*)a_fit.dev;
+  ia.status = (uint32_t*)a_st.dev;
+  ia.step_delta = (float*)a_sd.dev;
+  ia.step_trial = (double*)a_strial.dev;
+  ia.step_chi2_start = (float*)a_sc0.dev;
+  ia.step_chi2_trial = (float*)a_sc1.dev;
+  ia.work = ctx->work;
+  cudaError_t e = cudaMemsetAsync(ctx->work, 0, sizeof(gm::WorkCounters), s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "work counter reset");
+  const int per_sm = std::max(1, gm::invert_blocks_per_sm(nl));
+  int64_t grid = (int64_t)per_sm * ctx->sms;
+  const int64_t needed = (npix + gm::kWarpsPerBlock - 1) / gm::kWarpsPerBlock;
+  if (grid > needed) grid = needed;
+  cudaEventRecord(ctx->ev0, s);
+  e = gm::launch_invert(d, ia, (int)grid, s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "inversion kernel launch");
+  cudaEventRecord(ctx->ev1, s);
+  ctx->stats.grid_blocks = (int)grid;
+  ctx->stats.block_threads = gm::kWarpsPerBlock * 32;
+  ctx->stats.warps_per_block = gm::kWarpsPerBlock;
+  ctx->stats.kernel_launches = 1;
+  ctx->stats.pixels = npix;
+  const Arg* outs[] = {&a_model, &a_m64, &a_chi, &a_it, &a_acc, &a_fit, &a_st,
+                       &a_sd, &a_strial, &a_sc0, &a_sc1};
+  bool any_host = false;
+  for (const Arg* o : outs) {
+    if ((st = copy_back(ctx, *o, s)) != GM_OK) return st;
+    any_host |= (o->host != nullptr);
+  }
+  any_host |= (a_in.dev != (void*)iquv);
+  if (any_host || !stream) {
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "inversion");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->stats.kernel_ms = ms;
+    gm::WorkCounters wc{};
+    cudaMemcpy(&wc, ctx->work, sizeof(wc), cudaMemcpyDeviceToHost);
+    ctx->stats.iterations = (int64_t)wc.iterations;
+    ctx->stats.accepted = (int64_t)wc.accepted;
+  }
+  return GM_OK;
+}
+
+gm_status gm_invert_ex(gm_ctx* ctx, const float* iquv, int64_t npix, int nl,
+                       const double* init_models, float* model, double* model_f64, float* chi2,
+                       int* iters, int* accepted, float* fitted, uint32_t* status, void* stream) {
+  if (!ctx) return GM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->call_mu);
+  gm::DevCfg d = ctx->dev;
+  if (init_models) d.init_mode = 1;
+  const float* map = (ctx->cfg.use_slight && ctx->cfg.slight_per_pixel) ? ctx->cfg.slight : nullptr;
+  return invert_impl(ctx, d, iquv, npix, nl, init_models, map, model, model_f64, chi2, iters,
+                     accepted, fitted, status, stream);
+}
+
+gm_status gm_invert(gm_ctx* ctx, const float* iquv, int64_t npix, int nl, float* model,
+                    float* chi2, int* iters, float* fitted, uint32_t* status, void* stream) {
+  return gm_invert_ex(ctx, iquv, npix, nl, nullptr, model, nullptr, chi2, iters, nullptr, fitted,
+                      status, stream);
+}
+
+gm_status gm_lm_step(gm_ctx* ctx, const float* iquv, int64_t npix, int nl, const double* models,
+                     float flambda, float* delta, double* trial, float* chi2_start,
+                     float* chi2_trial, void* stream) {
+  if (!ctx) return GM_ERR_INVALID;
+  if (!models) return fail(ctx, GM_ERR_INVALID, "gm_lm_step needs the starting models");
+  std::lock_guard<std::mutex> lk(ctx->call_mu);
+  gm::DevCfg d = ctx->dev;
+  d.init_mode = 1;
+  d.miter = 1;
+  d.ilambda = flambda;
+  StepOut so;
+  so.delta = delta;
+  so.trial = trial;
+  so.chi2_start = chi2_start;
+  so.chi2_trial = chi2_trial;
+  const float* map = (ctx->cfg.use_slight && ctx->cfg.slight_per_pixel) ? ctx->cfg.slight : nullptr;
+  return invert_impl(ctx, d, iquv, npix, nl, models, map, nullptr, nullptr, nullptr, nullptr, nullptr,
+                     nullptr, nullptr, stream, &so);
+}
+
+static gm_status synth_impl(gm_ctx* ctx, const float* m32, const double* m64, int64_t npix,
+                            float* iquv, float* rf, void* stream) {
+  if (!ctx) return GM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->call_mu);
+  if (!ctx->configured) return fail(ctx, GM_ERR_NOT_CONFIGURED, "gm_configure first");
+  if ((!m32 && !m64) || !iquv || npix < 0) return fail(ctx, GM_ERR_INVALID, "null argument");
+  if (npix == 0) return GM_OK;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  const int nl = ctx->dev.nl, nt = ctx->dev.nterms;
+  Arg a_m, a_out, a_rf, a_sl;
+  gm_status st;
+  if (m32) st = stage_in(ctx, "smodels", m32, sizeof(float) * 11 * npix, &a_m, s);
+  else st = stage_in(ctx, "smodels", m64, sizeof(double) * 11 * npix, &a_m, s);
+  if (st != GM_OK) return st;
+  if ((st = stage_out(ctx, "siquv", iquv, sizeof(float) * 4 * nl * npix, &a_out)) != GM_OK) return st;
+  if ((st = stage_out(ctx, "srf", rf, sizeof(float) * 4 * nt * nl * npix, &a_rf)) != GM_OK) return st;
+  gm::DevCfg d = ctx->dev;
+  // the synthesis path returns every response function (kernel_synthesis
+  // calls me_der without zeroing fixed parameters, gmilos.cu:71-84)
+  for (int i = 0; i < GM_NPAR; ++i) d.fix[i] = 1;
+  if (d.use_slight && d.slight_per_pixel) {
+    if ((st = stage_in(ctx, "sslight", ctx->cfg.slight, sizeof(float) * 4 * nl * npix, &a_sl, s)) != GM_OK) return st;
+    d.slight = (const float*)a_sl.dev;
+  }
+  gm::SynthArgs sa{};
+  sa.models_f32 = m32 ? (const float*)a_m.dev : nullptr;
+  sa.models_f64 = m64 ? (const double*)a_m.dev : nullptr;
+  sa.npix = npix;
+  sa.iquv = (float*)a_out.dev;
+  sa.rf = (float*)a_rf.dev;
+  cudaError_t e = gm::launch_synth(d, sa, s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "synthesis kernel launch");
+  if ((st = copy_back(ctx, a_out, s)) != GM_OK) return st;
+  if ((st = copy_back(ctx, a_rf, s)) != GM_OK) return st;
+  if (a_out.host || a_rf.host || a_m.dev != (m32 ? (const void*)m32 : (const void*)m64) || !stream) {
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "synthesis");
+  }
+  return GM_OK;
+}
+
+gm_status gm_synthesize(gm_ctx* ctx, const float* models, int64_t npix, float* iquv, float* rf,
+                        void* stream) {
+  return synth_impl(ctx, models, nullptr, npix, iquv, rf, stream);
+}
+
+gm_status gm_synthesize_f64(gm_ctx* ctx, const double* models, int64_t npix, float* iquv, float* rf,
+                            void* stream) {
+  return synth_impl(ctx, nullptr, models, npix, iquv, rf, stream);
+}
+
+gm_status gm_synthesize_grid(gm_ctx* ctx, const double* models, int64_t npix, const double* offsets,
+                             int ngrid, float* iquv, void* stream) {
+  if (!ctx) return GM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->call_mu);
+  if (!ctx->configured) return fail(ctx, GM_ERR_NOT_CONFIGURED, "gm_configure first");
+  if (!models || !offsets || !iquv || npix < 0 || ngrid < 1) return fail(ctx, GM_ERR_INVALID, "bad argument");
+  if (npix == 0) return GM_OK;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  Arg a_m, a_o, a_out;
+  gm_status st;
+  if ((st = stage_in(ctx, "gmodels", models, sizeof(double) * 11 * npix, &a_m, s)) != GM_OK) return st;
+  if ((st = stage_in(ctx, "goffs", offsets, sizeof(double) * ngrid, &a_o, s)) != GM_OK) return st;
+  if ((st = stage_out(ctx, "giquv", iquv, sizeof(float) * 4 * (size_t)ngrid * npix, &a_out)) != GM_OK) return st;
+  cudaError_t e = gm::launch_synth_grid(ctx->dev, (const double*)a_m.dev, npix, (const double*)a_o.dev,
+                                        ngrid, (float*)a_out.dev, s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "grid synthesis launch");
+  if ((st = copy_back(ctx, a_out, s)) != GM_OK) return st;
+  if (a_out.host || a_m.dev != (const void*)models || !stream) {
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "grid synthesis");
+  }
+  return GM_OK;
+}
+
+gm_status gm_get_stats(gm_ctx* ctx, gm_stats* out) {
+  if (!ctx || !out) return GM_ERR_INVALID;
+  *out = ctx->stats;
+  return GM_OK;
+}
+
+gm_status gm_measure_peaks(gm_ctx* ctx, double* fp32_tflops, double* fp64_tflops) {
+  if (!ctx) return GM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->call_mu);
+  cudaSetDevice(ctx->device);
+  void* sink = nullptr;
+  gm_status st = ensure_buf(ctx, "peaksink", sizeof(double) * 1024 * 1024, &sink);
+  if (st != GM_OK) return st;
+  const int blocks = ctx->sms * 8, threads = 256;
+  double best32 = 0, best64 = 0;
+  for (int rep = 0; rep < 4; ++rep) {
+    for (int kind = 0; kind < 2; ++kind) {
+      const int iters = kind == 0 ? 4096 : 1024;
+      cudaEventRecord(ctx->ev0, ctx->stream);
+      cudaError_t e = gm::launch_peak(kind, blocks, threads, iters, sink, ctx->stream);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "peak kernel");
+      cudaEventRecord(ctx->ev1, ctx->stream);
+      e = cudaEventSynchronize(ctx->ev1);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "peak kernel");
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+      const double flops = 2.0 * gm::kPeakChains * (double)iters * blocks * threads;
+      const double tf = flops / (ms * 1e-3) / 1e12;
+      if (kind == 0) best32 = std::max(best32, tf); else best64 = std::max(best64, tf);
+    }
+  }
+  if (fp32_tflops) *fp32_tflops = best32;
+  if (fp64_tflops) *fp64_tflops = best64;
+  return GM_OK;
+}
+
+// ---------------------------------------------------------------- serving
+// Requests are queued and run by one worker thread in arrival order; each
+// runs as its own persistent launch on the context stream.
+gm_status gm_submit(gm_ctx* ctx, const gm_request* req, gm_ticket* ticket) {
+  if (!ctx || !req || !ticket) return GM_ERR_INVALID;
+  if (!ctx->configured) return fail(ctx, GM_ERR_NOT_CONFIGURED, "gm_configure first");
+  if (!req->iquv || !req->model || req->npix < 0 || req->nl != ctx->dev.nl)
+    return fail(ctx, GM_ERR_INVALID, "bad request");
+  auto r = std::make_shared<Request>();
+  r->req = *req;
+  if (req->fix) r->fix.assign(req->fix, req->fix + GM_NPAR);
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!ctx->worker.joinable()) ctx->worker = std::thread(serve_loop, ctx);
+  const gm_ticket t = ctx->next_ticket++;
+  ctx->reqs[t] = r;
+  ctx->queue.push_back(t);
+  *ticket = t;
+  ctx->cv.notify_all();
+  return GM_OK;
+}
+
+gm_status gm_poll(gm_ctx* ctx, gm_ticket ticket, int timeout_us) {
+  if (!ctx) return GM_ERR_INVALID;
+  std::unique_lock<std::mutex> lk(ctx->mu);
+  auto it = ctx->reqs.find(ticket);
+  if (it == ctx->reqs.end()) return fail(ctx, GM_ERR_INVALID, "unknown ticket");
+  auto r = it->second;
+  auto pred = [&] { return r->done; };
+  if (timeout_us < 0) ctx->done_cv.wait(lk, pred);
+  else if (!ctx->done_cv.wait_for(lk, std::chrono::microseconds(timeout_us), pred)) return GM_ERR_TIMEOUT;
+  ctx->reqs.erase(ticket);
+  return r->cancelled ? GM_ERR_CANCELLED : r->result;
+}
+
+gm_status gm_cancel(gm_ctx* ctx, gm_ticket ticket) {
+  if (!ctx) return GM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto it = ctx->reqs.find(ticket);
+  if (it == ctx->reqs.end()) return fail(ctx, GM_ERR_INVALID, "unknown ticket");
+  auto q = std::find(ctx->queue.begin(), ctx->queue.end(), ticket);
+  if (q != ctx->queue.end()) {
+    ctx->queue.erase(q);
+    it->second->cancelled = true;
+    it->second->done = true;
+    ctx->done_cv.notify_all();
+  }
+  return GM_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+void serve_loop(gm_ctx* ctx) {
+  cudaSetDevice(ctx->device);
+  for (;;) {
+    std::shared_ptr<Request> r;
+    {
+      std::unique_lock<std::mutex> lk(ctx->mu);
+      ctx->cv.wait(lk, [&] { return ctx->stopping || !ctx->queue.empty(); });
+      if (ctx->stopping && ctx->queue.empty()) return;
+      const gm_ticket t = ctx->queue.front();
+      ctx->queue.pop_front();
+      r = ctx->reqs[t];
+    }
+    gm_status st;
+    {
+      std::lock_guard<std::mutex> lk(ctx->call_mu);
+      gm::DevCfg d = ctx->dev;
+      if (!r->fix.empty())
+        for (int i = 0; i < GM_NPAR; ++i) d.fix[i] = r->fix[i] ? 1 : 0;
+      const gm_request& q = r->req;
+      st = invert_impl(ctx, d, q.iquv, q.npix, q.nl, nullptr, nullptr, q.model, nullptr, q.chi2,
+                       q.iters, nullptr, nullptr, q.status, nullptr);
+    }
+    {
+      std::lock_guard<std::mutex> lk(ctx->mu);
+      r->result = st;
+      r->done = true;
+    }
+    ctx->done_cv.notify_all();
+  }
+}
+
+}  // namespace

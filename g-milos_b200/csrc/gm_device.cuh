@@ -1,0 +1,836 @@
+// gm_device.cuh -- device building blocks of the Milne-Eddington engine.
+//
+// Mapping: one warp inverts one pixel; lane l owns wavelength samples
+// l, l+32 (LPL = samples per lane, 1 for nl <= 32, 2 for nl <= 64).  All
+// per-pixel scalars (model, LM state) are warp-uniform.  The arithmetic
+// follows the reference's precision choices: FP32 with the same fast
+// intrinsics (__fdividef, __sincosf), FP64 for the Voigt polynomials and
+// wherever the reference keeps PRECISION=double (model parameters,
+// classical estimates).  file:line citations name the reference code each
+// piece reproduces.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gmilos.h"
+
+namespace gm {
+
+constexpr int kMaxNl = 64;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr double kPi = 3.14159265358979323846264338327950288419716939937510;
+constexpr double kVlight = 2.99792458e+5;      // km/s
+constexpr double kLarmor = 4.6686411e-13;      // A^-1 G^-1
+constexpr double kRR = 0.5641895836;           // 1/sqrt(pi) as the reference rounds it
+
+enum { ETA0 = 0, BFLD, VLOS, DOPP, AA, GM, AZ, S0, S1, MAC, ALFA };
+
+// Per-configuration constants, passed by value as a kernel parameter (lives
+// in the constant bank: uniform reads are free).
+struct DevCfg {
+  int nl, nterms;
+  int use_psf, use_slight, slight_per_pixel;
+  int init_mode, miter, logclambda, quirks;
+  int numerics;          // 0: reference intrinsics, 1: accurate trigonometry
+  int n_pi, n_sig;
+  int fix[11];
+  float dl[kMaxNl];      // (float)(lambda - lambda0), the reference's sub_aux
+  double dld[kMaxNl];    // lambda - lambda0 in double (classical estimates)
+  float psf[kMaxNl];     // PSF taps
+  float nup[10], nub[10], wep[10], web[10], wer[10];
+  float geff, fo, mu, ilambda, noise;
+  float weight[4];
+  float wsig[4];         // weight / noise (gmilos.cu:1126-1129)
+  double lambda0, toplim, stop_dchi2;
+  double init[11];
+  const float* slight;   // device [4][nl] or [P][4][nl]
+};
+
+// --------------------------------------------------------------- warp utils
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// Reduce-scatter of N = 32*r per-lane partial sums by recursive halving:
+// every step each lane keeps half of its vector and adds the partner's copy
+// of that half.  After five steps lane L holds the warp-wide sums of entries
+// [r*L, r*L + r).  Cost: N - r shuffles instead of 5 N for N butterflies.
+template <int N>
+__device__ __forceinline__ void warp_reduce_scatter(float (&v)[N], int lane) {
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    const int w = N >> s;        // live entries per lane
+    const int h = w >> 1;
+    const int bit = 16 >> s;
+    const bool up = (lane & bit) != 0;
+#pragma unroll
+    for (int i = 0; i < h; ++i) {
+      const float send = up ? v[i] : v[i + h];
+      const float keep = up ? v[i + h] : v[i];
+      v[i] = keep + __shfl_xor_sync(kFull, send, bit);
+    }
+  }
+}
+
+// sin and cos as the reference takes them (__sincosf, absolute error of a few
+// 1e-7) or correctly rounded (accurate numerics)
+__device__ __forceinline__ void sincos_mode(float x, float* s, float* c, bool accurate) {
+  if (accurate) sincosf(x, s, c);
+  else __sincosf(x, s, c);
+}
+
+// --------------------------------------------------------------- Voigt
+// Hui, Armstrong & Wray (1978) rational approximation of the complex
+// probability function w = P(z)/Q(z), z = a + i v, evaluated by Horner's rule
+// in double; H = Re w and F = -Im w / 2 are formed in float with the
+// reference's fast division (d_fvoigt, mil_sinrf.cu:172-332).
+__device__ __forceinline__ void voigt(double a, float v, float& H, float& F) {
+  const double zr = a, zi = (double)v;
+  double nr = -0.564189583562615, ni = 0.0;
+  const double p[6] = {122.607931777104326, 214.382388694706425, 181.928533092181549,
+                       93.155580458138441, 30.180142196210589, 5.912626209773153};
+#pragma unroll
+  for (int k = 5; k >= 0; --k) {
+    const double t = nr * zr - ni * zi - p[k];
+    ni = nr * zi + ni * zr;
+    nr = t;
+  }
+  const double q[7] = {122.60793177387535, 352.730625110963558, 457.334478783897737,
+                       348.703917719495792, 170.354001821091472, 53.992906912940207,
+                       10.479857114260399};
+  double dr = 1.0, di = 0.0;
+#pragma unroll
+  for (int k = 6; k >= 0; --k) {
+    const double t = dr * zr - di * zi + q[k];
+    di = dr * zi + di * zr;
+    dr = t;
+  }
+  const float den = (float)(dr * dr + di * di);
+  const float re = (float)(nr * dr + ni * di);
+  const float im = (float)(ni * dr - nr * di);
+  H = -__fdividef(re, den);
+  F = __fdividef(im, den) * 0.5f;
+}
+
+// --------------------------------------------------------------- state
+struct Angles {
+  float cosi, sinis, sina, cosa, sinda, cosda, sindi, cosdi, cosis_2;
+};
+
+// Per-lane results of a synthesis that the response functions reuse:
+// absorption / dispersion profiles of the pi, blue and red groups and the
+// last component's H, F, v of each group (the reference's profile
+// derivatives keep only the last component of a group, me_der.cu:66-74).
+template <int LPL>
+struct Lane {
+  float fi[LPL][3], shi[LPL][3];
+  float lh[LPL][3], lf[LPL][3], lu[LPL][3];
+};
+
+// Warp-private shared memory.
+template <int LPL>
+struct WarpSmem {
+  double m[11];          // current (last accepted) model: the reference's initModel
+  double t[11];          // trial model, persistent like the reference's `model`
+  float A[10][11];       // Jacobi working matrix (upper triangle)
+  float alpha[56];       // undamped normal matrix, packed upper triangle
+  float beta[12];
+  float vec[12];
+  float cs[18][5], sn[18][5];
+  float red[96];
+  float stg[96 * LPL];   // zero-padded PSF staging row
+};
+
+// Rotation pairs of the parallel Jacobi: lane b < 5 owns diagonal block
+// (b, b); lanes 5..14 own the off-diagonal blocks (p, q), p < q.
+__device__ __forceinline__ void block_of_lane(int lane, int& p, int& q) {
+  const int bp[15] = {0, 1, 2, 3, 4, 0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
+  const int bq[15] = {0, 1, 2, 3, 4, 1, 2, 3, 4, 2, 3, 4, 3, 4, 4};
+  if (lane < 15) { p = bp[lane]; q = bq[lane]; } else { p = 0; q = 0; }
+}
+// index i moves to rr_perm(i) after every step (gmilos.cu:108-128)
+__device__ __forceinline__ int rr_perm(int i) {
+  const int t[10] = {0, 2, 4, 1, 6, 3, 8, 5, 9, 7};
+  return t[i];
+}
+
+// --------------------------------------------------------------- PSF
+// Same-size correlation of one row (LPL samples per lane) with the nl-tap
+// PSF centred at nl/2, zero padded; with use_ic the row is reflected about
+// max(first, last) before and after (direct_convolution{,_ic},
+// convolution.cu:153-241).  stg is this warp's staging row: samples live at
+// [32*LPL, 64*LPL), the rest stays zero.
+template <int LPL>
+__device__ __forceinline__ void psf_row(float (&x)[LPL], float* stg, const DevCfg& c,
+                                        int lane, bool use_ic) {
+  const int nl = c.nl;
+  float ic = 0.f;
+  if (use_ic) {
+    const float first = __shfl_sync(kFull, x[0], 0);
+    const int kl = (nl - 1) >> 5, ll = (nl - 1) & 31;
+    float lastv = x[0];
+#pragma unroll
+    for (int k = 1; k < LPL; ++k)
+      if (k == kl) lastv = x[k];
+    const float last = __shfl_sync(kFull, lastv, ll);
+    ic = first > last ? first : last;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+    stg[32 * LPL + l] = (l < nl) ? (use_ic ? ic - x[k] : x[k]) : 0.f;
+  }
+  __syncwarp();
+  const int half = nl >> 1;
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const float* base = stg + 32 * LPL + lane + 32 * k - half;
+    float a0 = 0.f, a1 = 0.f;
+    int j = 0;
+    for (; j + 1 < nl; j += 2) {
+      a0 = fmaf(c.psf[j], base[j], a0);
+      a1 = fmaf(c.psf[j + 1], base[j + 1], a1);
+    }
+    if (j < nl) a0 = fmaf(c.psf[j], base[j], a0);
+    const float r = a0 + a1;
+    x[k] = use_ic ? ic - r : r;
+  }
+}
+
+// --------------------------------------------------------------- synthesis
+// ME synthesis of this lane's samples (mil_sinrf.cu:27-142 with
+// mil_sinrf_kernel :334-433): Zeeman components through the Voigt
+// profiles, Unno-Rachkovsky solution, PSF, stray-light mix.
+template <int LPL>
+__device__ __forceinline__ void synth_lane(const DevCfg& c, const double* m, const float (&dlv)[LPL],
+                                           int lane, Lane<LPL>& st, Angles& an,
+                                           float (&spec)[LPL][4], float (&pure)[LPL][4],
+                                           const float (&sl)[LPL][4], float* stg) {
+  const float CC = (float)(kPi / 180.0), CC2 = (float)((kPi / 180.0) * 2);
+  const double azi = m[AZ] * (double)CC, gmr = m[GM] * (double)CC;
+  float sgm, cgm;
+  const bool acc = c.numerics != 0;
+  sincos_mode((float)gmr, &sgm, &cgm, acc);
+  an.cosi = cgm;
+  an.sinis = sgm * sgm;
+  const float cosis = cgm * cgm;
+  an.cosis_2 = __fdividef(1.f + cosis, 2.f);
+  sincos_mode((float)(2 * azi), &an.sina, &an.cosa, acc);
+  an.sinda = an.cosa * CC2;
+  an.cosda = -an.sina * CC2;
+  an.sindi = cgm * sgm * CC2;
+  an.cosdi = -sgm * CC;
+  const float sinis_cosa = an.sinis * an.cosa, sinis_sina = an.sinis * an.sina;
+  const double E0 = m[ETA0] * (double)c.fo;
+  const float ulos = __fdividef((float)(m[VLOS] * c.lambda0), (float)(kVlight * m[DOPP]));
+  const float parcial = (float)((c.lambda0 * c.lambda0 / m[DOPP]) * kLarmor);
+  const float doppf = (float)m[DOPP];
+  const double aa = m[AA];
+
+#pragma unroll
+  for (int g = 0; g < 3; ++g) {
+    const int n = (g == 0) ? c.n_pi : c.n_sig;
+    for (int kk = 0; kk < n; ++kk) {
+      float nu, wex;
+      if (g == 0) { nu = parcial * c.nup[kk]; wex = c.wep[kk]; }
+      else if (g == 1) { nu = parcial * c.nub[kk]; wex = c.web[kk]; }
+      else { nu = -(parcial * c.nub[c.n_sig - 1 - kk]); wex = c.wer[kk]; }
+      const float rnu = (float)((double)nu * m[BFLD]);
+#pragma unroll
+      for (int k = 0; k < LPL; ++k) {
+        float v = __fdividef(dlv[k], doppf);
+        v = v - ulos;
+        v = v - rnu;
+        float h, f;
+        voigt(aa, v, h, f);
+        if (kk == 0) {
+          st.fi[k][g] = wex * h;
+          st.shi[k][g] = wex * f * 2.f;
+        } else {
+          st.fi[k][g] = st.fi[k][g] + wex * h;
+          st.shi[k][g] = st.shi[k][g] + wex * f * 2.f;
+        }
+        st.lh[k][g] = h;
+        st.lf[k][g] = f;
+        st.lu[k][g] = v;
+      }
+    }
+  }
+
+  const float E0_2 = __fdividef((float)E0, 2.f);
+  const double s1mu = -(m[S1] * (double)c.mu);
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const float fp = st.fi[k][0], fb = st.fi[k][1], fr = st.fi[k][2];
+    const float sp = st.shi[k][0], sb = st.shi[k][1], sr = st.shi[k][2];
+    const float p1 = fb + fr;
+    const float p2 = E0_2 * (fp - __fdividef(p1, 2.f));
+    const float p3 = E0_2 * (sp - __fdividef(sb + sr, 2.f));
+    const float ein = E0_2 * (fp * an.sinis + p1 * an.cosis_2);
+    const float eq = p2 * sinis_cosa, eu = p2 * sinis_sina, ev = (fr - fb) * (E0_2 * an.cosi);
+    const float rq = p3 * sinis_cosa, ru = p3 * sinis_sina, rv = (sr - sb) * (E0_2 * an.cosi);
+    const float ei = 1.f + ein;
+    const float ei2 = ei * ei;
+    const float q2 = rq * rq, u2 = ru * ru, v2 = rv * rv;
+    const float gp1 = ei2 - eq * eq - eu * eu - ev * ev + q2 + u2 + v2;
+    const float gp3 = ei2 + q2 + u2 + v2;
+    const float gp2 = eq * rq + eu * ru + ev * rv;
+    const float dt = ei2 * gp1 - gp2 * gp2;
+    const float dti = __fdividef(1.f, dt);
+    const float gp4 = ei2 * eq + ei * (ev * ru - eu * rv);
+    const float gp5 = ei2 * eu + ei * (eq * rv - ev * rq);
+    const float gp6 = ei2 * ev + ei * (eu * rq - eq * ru);
+    const float dtiaux = (float)((double)dti * s1mu);
+    spec[k][0] = (float)(m[S0] - (double)(dtiaux * ei * gp3));
+    spec[k][1] = dtiaux * (gp4 + rq * gp2);
+    spec[k][2] = dtiaux * (gp5 + ru * gp2);
+    spec[k][3] = dtiaux * (gp6 + rv * gp2);
+  }
+
+  if (c.use_psf) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      float row[LPL];
+#pragma unroll
+      for (int k = 0; k < LPL; ++k) row[k] = spec[k][s];
+      psf_row<LPL>(row, stg, c, lane, s == 0);
+#pragma unroll
+      for (int k = 0; k < LPL; ++k) spec[k][s] = row[k];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < LPL; ++k)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) pure[k][s] = spec[k][s];
+  if (c.use_slight) {
+    const double a = m[ALFA];
+#pragma unroll
+    for (int k = 0; k < LPL; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+        spec[k][s] = (float)((double)spec[k][s] * a + (double)sl[k][s] * (1.0 - a));
+  }
+}
+
+// --------------------------------------------------------------- response functions
+// Analytic derivatives of the last synthesis (me_der.cu:81-376): profile
+// derivatives of each group's last component (d_funcionComponentFor
+// :53-77), their Zeeman combination and the RTE derivative (me_der_kernel
+// :218-376), PSF of every free RF except S0's, stray-light scaling
+// (:191-211).  Rows of fixed parameters are left zero
+// (FijaACeroDerivadasNoNecesarias, milosUtils.cu:243-271).  J[k][s][t]:
+// sample k, Stokes s, parameter slot t (10-term layout: slot 9 = alpha).
+template <int LPL>
+__device__ __forceinline__ void rf_lane(const DevCfg& c, const double* m, const Lane<LPL>& st,
+                                        const Angles& an, const float (&asrc)[LPL][4],
+                                        const float (&sl)[LPL][4], int lane, float* stg,
+                                        float (&J)[LPL][4][10]) {
+  const float auxCte = __fdividef((float)(-c.lambda0), (float)(kVlight * m[DOPP]));
+  const double aa = m[AA], dopp = m[DOPP];
+  // last component of each group: its scaled splitting and strength
+  const float parcial = (float)((c.lambda0 * c.lambda0 / m[DOPP]) * kLarmor);
+  float nul[3], wel[3];
+  nul[0] = parcial * c.nup[c.n_pi - 1];
+  wel[0] = c.wep[c.n_pi - 1];
+  nul[1] = parcial * c.nub[c.n_sig - 1];
+  wel[1] = c.web[c.n_sig - 1];
+  nul[2] = -(parcial * c.nub[0]);
+  wel[2] = c.wer[c.n_sig - 1];
+
+  const float E0f = (float)(m[ETA0] * (double)c.fo);
+  const float E0d = (float)(m[ETA0] * (double)c.fo);
+  const double E0dd = m[ETA0] * (double)c.fo;
+  const float sc = __fdividef(E0f * (an.sinis * an.cosa), 2.f);
+  const float ss = __fdividef(E0f * (an.sinis * an.sina), 2.f);
+  const float E0_2 = __fdividef(E0f, 2.f);
+  const float sindi_cosa = an.sindi * an.cosa, sindi_sina = an.sindi * an.sina;
+  const float cosdi_E0_2 = E0_2 * an.cosdi;
+  const float cosi_2_E0 = __fdividef(E0f * an.cosi, 2.f);
+  const float cosis_2_E0_2 = an.cosis_2 * E0_2;
+  const float sinis_E0_2 = an.sinis * E0_2;
+  const float cosi_cosdi = an.cosi * an.cosdi * E0_2, sindi_E0_2 = an.sindi * E0_2;
+  const float sinis_cosda = an.sinis * an.cosda, sinis_sinda = an.sinis * an.sinda;
+  const float sinis_cosa = an.sinis * an.cosa, sinis_sina = an.sinis * an.sina;
+  const float E0s_2 = __fdividef((float)(m[ETA0] * (double)c.fo), 2.f);
+  const float s1mu_f = (float)(-(m[S1] * (double)c.mu));
+  const float muf = c.mu;
+
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    float dfi[3][4], dshi[3][4];
+#pragma unroll
+    for (int g = 0; g < 3; ++g) {
+      const float u = st.lu[k][g], h = st.lh[k][g], f = st.lf[k][g];
+      const float dH = (float)((4 * aa * (double)f - (double)(2.f * u * h)) * (double)wel[g]);
+      const float dF = (float)((kRR - aa * (double)h - (double)(2.f * u * f)) * (double)wel[g]);
+      const float su = (float)(-(double)u / dopp);
+      dfi[g][0] = dH * (-nul[g]);
+      dfi[g][1] = dH * auxCte;
+      dfi[g][2] = dH * su;
+      dfi[g][3] = -2.f * dF;
+      dshi[g][0] = dF * (-nul[g]);
+      dshi[g][1] = dF * auxCte;
+      dshi[g][2] = dF * su;
+      dshi[g][3] = dH * 0.5f;
+    }
+    // RTE quantities of this sample (recomputed from the stored profiles;
+    // identical to the synthesis' values)
+    const float fp = st.fi[k][0], fb = st.fi[k][1], fr = st.fi[k][2];
+    const float sp = st.shi[k][0], sb = st.shi[k][1], sr = st.shi[k][2];
+    const float p1 = fb + fr;
+    const float p2 = E0s_2 * (fp - __fdividef(p1, 2.f));
+    const float p3 = E0s_2 * (sp - __fdividef(sb + sr, 2.f));
+    const float ein = E0s_2 * (fp * an.sinis + p1 * an.cosis_2);
+    const float eq = p2 * sinis_cosa, eu = p2 * sinis_sina, ev = (fr - fb) * (E0s_2 * an.cosi);
+    const float rq = p3 * sinis_cosa, ru = p3 * sinis_sina, rv = (sr - sb) * (E0s_2 * an.cosi);
+    const float ei = 1.f + ein;
+    const float ei2 = ei * ei;
+    const float gp1 = ei2 - eq * eq - eu * eu - ev * ev + rq * rq + ru * ru + rv * rv;
+    const float gp3 = ei2 + rq * rq + ru * ru + rv * rv;
+    const float gp2 = eq * rq + eu * ru + ev * rv;
+    const float dt = ei2 * gp1 - gp2 * gp2;
+    const float g4 = (ei2 * eq + ei * (ev * ru - eu * rv)) + rq * gp2;
+    const float g5 = (ei2 * eu + ei * (eq * rv - ev * rq)) + ru * gp2;
+    const float g6 = (ei2 * ev + ei * (eu * rq - eq * ru)) + rv * gp2;
+
+    float de[7], dq[7], du[7], dv[7], drq[7], dru[7], drv[7];
+    de[0] = (float)((double)ein / E0dd);
+    dq[0] = __fdividef(eq, E0d); du[0] = __fdividef(eu, E0d); dv[0] = __fdividef(ev, E0d);
+    drq[0] = __fdividef(rq, E0d); dru[0] = __fdividef(ru, E0d); drv[0] = __fdividef(rv, E0d);
+#pragma unroll
+    for (int j = 1; j < 5; ++j) {
+      const float dsum = dfi[1][j - 1] + dfi[2][j - 1];
+      de[j] = dfi[0][j - 1] * sinis_E0_2 + dsum * cosis_2_E0_2;
+      const float aux = dfi[0][j - 1] - __fdividef(dsum, 2.f);
+      dq[j] = aux * sc;
+      du[j] = aux * ss;
+      dv[j] = (dfi[2][j - 1] - dfi[1][j - 1]) * cosi_2_E0;
+      const float s1 = dshi[1][j - 1], s2 = dshi[2][j - 1];
+      const float aux2 = dshi[0][j - 1] - __fdividef(s1 + s2, 2.f);
+      drq[j] = aux2 * sc;
+      dru[j] = aux2 * ss;
+      drv[j] = (s2 - s1) * cosi_2_E0;
+    }
+    de[5] = fp * sindi_E0_2 + p1 * cosi_cosdi;
+    dq[5] = p2 * sindi_cosa;
+    du[5] = p2 * sindi_sina;
+    dv[5] = (fr - fb) * cosdi_E0_2;
+    drq[5] = p3 * sindi_cosa;
+    dru[5] = p3 * sindi_sina;
+    drv[5] = (sr - sb) * cosdi_E0_2;
+    de[6] = 0.f;
+    dv[6] = 0.f;
+    drv[6] = 0.f;
+    dq[6] = p2 * sinis_cosda;
+    du[6] = p2 * sinis_sinda;
+    drq[6] = p3 * sinis_cosda;
+    dru[6] = p3 * sinis_sinda;
+
+    const float dtaux = __fdividef(s1mu_f, dt * dt);
+    const float eigp3 = ei * gp3;
+    const float a2 = 2.f * ei;
+    const float ext1 = a2 * eq + ev * ru - eu * rv;
+    const float ext2 = a2 * eu + eq * rv - ev * rq;
+    const float ext3 = a2 * ev + eu * rq - eq * ru;
+    const float ext4 = a2 * gp1;
+#pragma unroll
+    for (int il = 0; il < 7; ++il) {
+      const float dgp1 = 2.f * (ei * de[il] - eq * dq[il] - eu * du[il] - ev * dv[il] +
+                               rq * drq[il] + ru * dru[il] + rv * drv[il]);
+      const float dgp2 = rq * dq[il] + eq * drq[il] + ru * du[il] + eu * dru[il] +
+                         rv * dv[il] + ev * drv[il];
+      const float ddt = ext4 * de[il] + ei2 * dgp1 - 2.f * gp2 * dgp2;
+      const float dgp3 = 2.f * (ei * de[il] + rq * drq[il] + ru * dru[il] + rv * drv[il]);
+      const float dgp4 = de[il] * ext1 + ei2 * dq[il] +
+                         ei * (ru * dv[il] + ev * dru[il] - rv * du[il] - eu * drv[il]);
+      const float dgp5 = de[il] * ext2 + ei2 * du[il] +
+                         ei * (rv * dq[il] + eq * drv[il] - rq * dv[il] - ev * drq[il]);
+      const float dgp6 = de[il] * ext3 + ei2 * dv[il] +
+                         ei * (rq * du[il] + eu * drq[il] - ru * dq[il] - eq * dru[il]);
+      J[k][0][il] = -(((de[il] * gp3 + ei * dgp3) * dt - ddt * eigp3) * dtaux);
+      J[k][1][il] = ((dgp4 + drq[il] * gp2 + rq * dgp2) * dt - ddt * g4) * dtaux;
+      J[k][2][il] = ((dgp5 + dru[il] * gp2 + ru * dgp2) * dt - ddt * g5) * dtaux;
+      J[k][3][il] = ((dgp6 + drv[il] * gp2 + rv * dgp2) * dt - ddt * g6) * dtaux;
+    }
+    const float dti = -(__fdividef(1.f, dt) * muf);
+    J[k][0][8] = -dti * eigp3;
+    J[k][1][8] = dti * g4;
+    J[k][2][8] = dti * g5;
+    J[k][3][8] = dti * g6;
+    J[k][0][7] = 1.f;
+    J[k][1][7] = 0.f;
+    J[k][2][7] = 0.f;
+    J[k][3][7] = 0.f;
+    J[k][0][6] = 0.f;
+    J[k][3][6] = 0.f;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) J[k][s][9] = 0.f;
+  }
+
+  if (c.use_psf) {
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+      if (t == 7 || !c.fix[t]) continue;
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        float row[LPL];
+#pragma unroll
+        for (int k = 0; k < LPL; ++k) row[k] = J[k][s][t];
+        psf_row<LPL>(row, stg, c, lane, s == 0);
+#pragma unroll
+        for (int k = 0; k < LPL; ++k) J[k][s][t] = row[k];
+      }
+    }
+  }
+  if (c.use_slight) {
+    const double a = m[ALFA];
+#pragma unroll
+    for (int k = 0; k < LPL; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+#pragma unroll
+        for (int t = 0; t < 9; ++t) J[k][s][t] = (float)((double)J[k][s][t] * a);
+        J[k][s][9] = asrc[k][s] - sl[k][s];
+      }
+  }
+#pragma unroll
+  for (int t = 0; t < 10; ++t) {
+    const int key = (t == 9) ? 10 : t;
+    if (!c.fix[key]) {
+#pragma unroll
+      for (int k = 0; k < LPL; ++k)
+#pragma unroll
+        for (int s = 0; s < 4; ++s) J[k][s][t] = 0.f;
+    }
+  }
+}
+
+// packed index of (i <= h) in the upper triangle of a 10x10 matrix
+__host__ __device__ constexpr int upk(int i, int h) { return i * 10 - (i * (i - 1)) / 2 + (h - i); }
+
+// Normal equations alpha = sum_s w_s/sigma^2 J^T J and beta = sum_s w_s J^T
+// (syn - obs) / sigma^2 (covarmf, lib.cu:65-118) reduced across the warp;
+// results land in sm.alpha (packed) and sm.beta.
+template <int LPL>
+__device__ __forceinline__ void normal_eq(const DevCfg& c, const float (&J)[LPL][4][10],
+                                          const float (&syn)[LPL][4], const float (&ob)[LPL][4],
+                                          const bool (&valid)[LPL], int lane, WarpSmem<LPL>& sm) {
+  float v[96];
+#pragma unroll
+  for (int i = 0; i < 96; ++i) v[i] = 0.f;
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    if (!valid[k]) continue;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const float wd = c.wsig[s];
+      const float r = c.weight[s] * (syn[k][s] - ob[k][s]);
+#pragma unroll
+      for (int i = 0; i < 10; ++i) {
+        const float ji = J[k][s][i];
+#pragma unroll
+        for (int h = i; h < 10; ++h) v[upk(i, h)] = fmaf(wd * ji, J[k][s][h], v[upk(i, h)]);
+        v[55 + i] = fmaf(r, ji, v[55 + i]);
+      }
+    }
+  }
+  warp_reduce_scatter<96>(v, lane);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) sm.red[3 * lane + i] = v[i];
+  __syncwarp();
+  for (int i = lane; i < 55; i += 32) sm.alpha[i] = sm.red[i];
+  if (lane < 10) sm.beta[lane] = __fdividef(sm.red[55 + lane], c.noise);
+  __syncwarp();
+}
+
+template <int LPL>
+__device__ __forceinline__ float chisq(const DevCfg& c, const float (&syn)[LPL][4],
+                                       const float (&ob)[LPL][4], const bool (&valid)[LPL]) {
+  float acc = 0.f;
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    if (!valid[k]) continue;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const float d = syn[k][s] - ob[k][s];
+      acc += __fdividef((d * d) * c.weight[s], c.noise);
+    }
+  }
+  const float nfree = (float)(c.nl * 4 - c.nterms);
+  return warp_sum(acc) / nfree;
+}
+
+// --------------------------------------------------------------- 10x10 solve
+// delta = V diag(1/w) V^T beta where (w, V) come from 18 steps of the
+// reference's parallel Jacobi (svdcordicf, svdcordic.cu:423-536; mil_svdf,
+// milosUtils.cu:328-365).  Lanes 0..14 own the 15 2x2 blocks of the upper
+// triangle; after every step the rotated blocks are written to the
+// round-robin relabelled positions.  V is never formed: the step rotations
+// are applied to beta on the way in and replayed transposed, in reverse, on
+// the way out.  Input: sm.alpha (packed), damping flambda; output sm.vec.
+template <int LPL>
+__device__ __forceinline__ void solve10(WarpSmem<LPL>& sm, float flambda, int lane, bool accurate) {
+  // damped matrix into the working array (milosUtils.cu:648-652)
+  for (int i = lane; i < 55; i += 32) {
+    int r = 0, cc = i;
+    while (cc >= 10 - r) { cc -= 10 - r; ++r; }
+    const int col = r + cc;
+    float a = sm.alpha[i];
+    if (col == r) a = (float)((double)a * (1.0 + (double)flambda));
+    sm.A[r][col] = a;
+  }
+  if (lane < 10) sm.vec[lane] = sm.beta[lane];
+  __syncwarp();
+
+  int p, q;
+  block_of_lane(lane, p, q);
+  const int r0 = 2 * p, c0 = 2 * q;
+  const float quarter = (float)(kPi / 4);
+  const float qclamp = __fdividef((float)kPi, 4.f);
+  // destinations of this lane's four entries (fixed for every step)
+  const int d00r = min(rr_perm(r0), rr_perm(c0)), d00c = max(rr_perm(r0), rr_perm(c0));
+  const int d01r = min(rr_perm(r0), rr_perm(c0 + 1)), d01c = max(rr_perm(r0), rr_perm(c0 + 1));
+  const int d10r = min(rr_perm(r0 + 1), rr_perm(c0)), d10c = max(rr_perm(r0 + 1), rr_perm(c0));
+  const int d11r = min(rr_perm(r0 + 1), rr_perm(c0 + 1)), d11c = max(rr_perm(r0 + 1), rr_perm(c0 + 1));
+  const bool active = lane < 15, diag = lane < 5;
+
+  for (int step = 0; step < 18; ++step) {
+    float m00 = 0.f, m01 = 0.f, m10 = 0.f, m11 = 0.f, b0 = 0.f, b1 = 0.f;
+    if (active) {
+      m00 = sm.A[r0][c0];
+      m01 = sm.A[r0][c0 + 1];
+      m10 = diag ? m01 : sm.A[r0 + 1][c0];
+      m11 = sm.A[r0 + 1][c0 + 1];
+    }
+    float cs = 1.f, sn = 0.f;
+    if (diag) {
+      b0 = sm.vec[r0];
+      b1 = sm.vec[r0 + 1];
+      float th;
+      if (m00 == m11) {
+        th = quarter;
+      } else {
+        const float arc = accurate ? (2.f * m01) / (m11 - m00) : __fdividef(2.f * m01, m11 - m00);
+        th = accurate ? atanf(arc) / 2.f : __fdividef(atanf(arc), 2.f);
+        if (th > qclamp) th = qclamp;
+        if (th < -qclamp) th = -qclamp;
+      }
+      sincos_mode(th, &sn, &cs, accurate);
+      sm.cs[step][lane] = cs;
+      sm.sn[step][lane] = sn;
+    }
+    const float cr = __shfl_sync(kFull, cs, p), sr = __shfl_sync(kFull, sn, p);
+    const float cc = __shfl_sync(kFull, cs, q), sc = __shfl_sync(kFull, sn, q);
+    __syncwarp();
+    if (active) {
+      const float t0 = m00 * cr - m10 * sr, t1 = m00 * sr + m10 * cr;
+      const float u0 = m01 * cr - m11 * sr, u1 = m01 * sr + m11 * cr;
+      const float n00 = t0 * cc - u0 * sc, n11 = t1 * sc + u1 * cc;
+      if (diag) {
+        sm.A[d00r][d00c] = n00;
+        sm.A[d01r][d01c] = 0.f;
+        sm.A[d11r][d11c] = n11;
+        sm.vec[rr_perm(r0)] = cs * b0 - sn * b1;
+        sm.vec[rr_perm(r0 + 1)] = sn * b0 + cs * b1;
+      } else {
+        sm.A[d00r][d00c] = n00;
+        sm.A[d01r][d01c] = t0 * sc + u0 * cc;
+        sm.A[d10r][d10c] = t1 * cc - u1 * sc;
+        sm.A[d11r][d11c] = n11;
+      }
+    }
+    __syncwarp();
+  }
+  // z = (V^T beta) / w with the |w| <= 1e-12 cut
+  if (lane < 10) {
+    const float w = sm.A[lane][lane];
+    const float inv = ((double)fabsf(w) > 1e-12) ? (1.f / w) : 0.f;
+    sm.vec[lane] = sm.vec[lane] * inv;
+  }
+  __syncwarp();
+  // delta = V z: undo the steps in reverse order
+  for (int step = 17; step >= 0; --step) {
+    float y0 = 0.f, y1 = 0.f, cs = 0.f, sn = 0.f;
+    if (diag) {
+      y0 = sm.vec[rr_perm(r0)];
+      y1 = sm.vec[rr_perm(r0 + 1)];
+      cs = sm.cs[step][lane];
+      sn = sm.sn[step][lane];
+    }
+    __syncwarp();
+    if (diag) {
+      sm.vec[r0] = cs * y0 + sn * y1;
+      sm.vec[r0 + 1] = -sn * y0 + cs * y1;
+    }
+    __syncwarp();
+  }
+}
+
+// --------------------------------------------------------------- model updates
+// model -= delta on free parameters with the reference's step limits
+// (AplicaDeltaf, milosUtils.cu:93-159), then range checks (check, :160-238).
+__device__ __forceinline__ void apply_delta_check(const DevCfg& c, const double* m, const float* d,
+                                                  double* t) {
+  float aux;
+  if (c.fix[ETA0]) t[ETA0] = m[ETA0] - d[0];
+  if (c.fix[BFLD]) {
+    aux = d[1];
+    if (aux < -300) aux = -300; else if (aux > 300) aux = 300;
+    t[BFLD] = m[BFLD] - aux;
+  }
+  if (c.fix[VLOS]) t[VLOS] = m[VLOS] - d[2];
+  if (c.fix[DOPP]) t[DOPP] = m[DOPP] - d[3];
+  if (c.fix[AA]) t[AA] = m[AA] - d[4];
+  if (c.fix[GM]) {
+    aux = d[5];
+    if (aux < -30) aux = -30; else if (aux > 30) aux = 30;
+    t[GM] = m[GM] - aux;
+  }
+  if (c.fix[AZ]) {
+    aux = d[6];
+    if (aux < -30) aux = -30; else if (aux > 30) aux = 30;
+    t[AZ] = m[AZ] - aux;
+  }
+  if (c.fix[S0]) t[S0] = m[S0] - d[7];
+  if (c.fix[S1]) t[S1] = m[S1] - d[8];
+  if (c.fix[MAC]) t[MAC] = m[MAC] - d[9];
+  if (c.fix[ALFA]) t[ALFA] = m[ALFA] - d[9];
+  if (t[BFLD] < 0) { t[BFLD] = -t[BFLD]; t[GM] = 180.0 - t[GM]; }
+  if (t[BFLD] > 5000) t[BFLD] = 5000;
+  if (t[GM] < 0) t[GM] = -t[GM];
+  if (t[GM] > 180) t[GM] = 360.0 - t[GM];
+  if (t[AZ] < 0) t[AZ] = 180 + t[AZ];
+  if (t[AZ] > 180) t[AZ] = t[AZ] - 180.0;
+  if (t[ETA0] < 1) t[ETA0] = 1;
+  if (t[ETA0] > 2500) t[ETA0] = 2500;
+  if (t[VLOS] < -20) t[VLOS] = -20;
+  if (t[VLOS] > 20) t[VLOS] = 20;
+  if (t[DOPP] < 0.0001) t[DOPP] = 0.0001;
+  if (t[DOPP] > 0.6) t[DOPP] = 0.6;
+  if (t[AA] < 0.0001) t[AA] = 0.0001;
+  if (t[AA] > 10.0) t[AA] = 10.0;
+  if (t[S0] < 0.0001) t[S0] = 0.0001;
+  if (t[S0] > 2.00) t[S0] = 2.00;
+  if (t[S1] < 0.0001) t[S1] = 0.0001;
+  if (t[S1] > 2.00) t[S1] = 2.00;
+  if (t[MAC] < 0) t[MAC] = 0;
+  if (t[MAC] > 4) t[MAC] = 4;
+  if (t[ALFA] < 0) t[ALFA] = 0.0;
+  if (t[ALFA] > 1.0) t[ALFA] = 1.0;
+}
+
+// Weak-field and centre-of-gravity estimates of B, vlos, gamma, phi
+// (estimacionesClasicas, milosUtils.cu:386-563) with the NaN fallbacks of
+// lm_mils (:621-628).  Sums are warp reductions in double.  Lane 0 writes m.
+template <int LPL>
+__device__ __forceinline__ uint32_t classical_warp(const DevCfg& c, const float (&ob)[LPL][4],
+                                                   const double (&dld)[LPL], const bool (&valid)[LPL],
+                                                   int lane, double* m) {
+  const int nl = c.nl;
+  int bmin = nl, emax = 0;
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+    if (valid[k] && !(ob[k][0] < 0.f)) {
+      bmin = min(bmin, l);
+      emax = max(emax, l + 1);
+    }
+  }
+  const int b = __reduce_min_sync(kFull, bmin);
+  const int e = __reduce_max_sync(kFull, emax);
+  uint32_t st = 0;
+  double Ic;
+  {
+    const int l = e - 1;
+    float v = 0.f;
+#pragma unroll
+    for (int k = 0; k < LPL; ++k)
+      if (l >= 0 && (l >> 5) == k) v = ob[k][0];
+    const float icf = __shfl_sync(kFull, v, l >= 0 ? (l & 31) : 0);
+    Ic = (e > 0) ? (double)icf : __longlong_as_double(0x7ff8000000000000ll);
+    if (e <= 0) st |= 0x20u;
+  }
+  double x = 0, y = 0, xv = 0, yv = 0, x2 = 0, y2 = 0, x3 = 0, y3 = 0, su = 0, sq = 0;
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    if (!valid[k]) continue;
+    const int l = lane + 32 * k;
+    const float I = ob[k][0], Q = ob[k][1], U = ob[k][2], V = ob[k][3];
+    const double d = dld[k];
+    if (l >= b && l < e - 1) {
+      if (I > -1 && V > -1) {
+        const double aux = Ic - (double)(I + V);
+        const double avl = Ic - (double)I;
+        x += aux * d;
+        xv += avl * d;
+        y += aux;
+        yv += avl;
+        const double aux2 = Ic - (double)(I - V);
+        x2 += aux2 * d;
+        y2 += aux2;
+      }
+      if (Q > -1 && U > -1 && V > -1) {
+        const double L = (double)fabsf(sqrtf(Q * Q + U * U));
+        const double mm = fabs((4 * d * L));
+        x3 += (double)fabsf(V) * mm;
+        y3 += (double)(fabsf(V) * fabsf(V));
+      }
+    }
+    if (U > -1 && Q > -1) {
+      if (fabs((double)U) > 0.0001 || fabs((double)Q) > 0.0001) {
+        su += U;
+        sq += Q;
+      }
+    }
+  }
+  x = warp_sum_d(x); y = warp_sum_d(y); xv = warp_sum_d(xv); yv = warp_sum_d(yv);
+  x2 = warp_sum_d(x2); y2 = warp_sum_d(y2); x3 = warp_sum_d(x3); y3 = warp_sum_d(y3);
+  su = warp_sum_d(su); sq = warp_sum_d(sq);
+  const double lp = (fabs(y) > 1e-15) ? x / y : 0;
+  const double lmn = (fabs(y2) > 1e-15) ? x2 / y2 : 0;
+  const double C = (kLarmor * (c.lambda0 * c.lambda0) * (double)c.geff);
+  const double Blos = (1 / C) * ((lp - lmn) / 2);
+  double Vlos = (kVlight / (c.lambda0)) * ((xv / yv) / 2);
+  y3 = y3 * fabs((3 * C * Blos));
+  const double tg = fabs(sqrt(x3 / y3));
+  double grad = atan(tg);
+  double gamma = grad * (180 / kPi);
+  if (gamma >= 85 && gamma <= 90) grad = 85 * (kPi / 180);
+  if (gamma > 90 && gamma <= 95) grad = 95 * (kPi / 180);
+  if (Blos < 0) gamma = (180) - gamma;
+  double phi = (atan(su / sq) * 180 / kPi) / 2;
+  if (su > 0 && sq > 0) {
+  } else if (su < 0 && sq > 0) {
+    phi = phi + 180;
+  } else if (su < 0 && sq < 0) {
+    phi = phi + 90;
+  } else if (su > 0 && sq < 0) {
+    phi = phi + 90;
+  }
+  const double Baux = fabs(Blos / cos(grad));
+  if (Vlos < -4) Vlos = -4;
+  if (Vlos > 4) Vlos = 4;
+  double B = (Baux > 4000 ? 4000 : Baux);
+  if (isnan(B)) { B = 1; st |= 0x01u; }
+  if (isnan(Vlos)) { Vlos = 1e-3; st |= 0x01u; }
+  if (isnan(gamma)) { gamma = 1; st |= 0x01u; }
+  if (isnan(phi)) { phi = 1; st |= 0x01u; }
+  if (lane == 0) {
+    m[BFLD] = B;
+    m[VLOS] = Vlos;
+    m[GM] = gamma;
+    m[AZ] = phi;
+  }
+  return st;
+}
+
+}  // namespace gm

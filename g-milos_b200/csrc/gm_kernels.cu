@@ -1,0 +1,327 @@
+// gm_kernels.cu -- persistent LM inversion kernel, synthesis kernels.
+#include "gm_kernels.cuh"
+
+namespace gm {
+
+// Load this lane's observed samples (zero past nl).
+template <int LPL>
+__device__ __forceinline__ void load_pixel(const float* __restrict__ p, int nl, int lane,
+                                           float (&ob)[LPL][4]) {
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) ob[k][s] = (l < nl) ? __ldg(p + s * nl + l) : 0.f;
+  }
+}
+
+// One warp per pixel, pixels taken from a global cursor until the cube is
+// done (lm_mils, milosUtils.cu:574-710, with its per-thread contiguous pixel
+// slice replaced by work stealing).
+template <int LPL>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+invert_kernel(const DevCfg c, const InvertArgs a) {
+  __shared__ WarpSmem<LPL> smem[kWarpsPerBlock];
+  const int lane = threadIdx.x & 31;
+  WarpSmem<LPL>& sm = smem[threadIdx.x >> 5];
+  for (int i = lane; i < 96 * LPL; i += 32) sm.stg[i] = 0.f;
+
+  const int nl = c.nl;
+  float dlv[LPL];
+  double dld[LPL];
+  bool valid[LPL];
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+    valid[k] = l < nl;
+    dlv[k] = valid[k] ? c.dl[l] : 0.f;
+    dld[k] = valid[k] ? c.dld[l] : 0.0;
+  }
+  float slg[LPL][4];
+  if (c.use_slight && !c.slight_per_pixel) load_pixel<LPL>(c.slight, nl, lane, slg);
+  else {
+#pragma unroll
+    for (int k = 0; k < LPL; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
+  }
+  __syncwarp();
+
+  unsigned long long my_iter = 0, my_acc = 0;
+  while (true) {
+    unsigned long long pix = 0;
+    if (lane == 0) pix = atomicAdd(&a.work->next_pixel, 1ull);
+    pix = __shfl_sync(kFull, pix, 0);
+    if (pix >= (unsigned long long)a.npix) break;
+    const size_t off = (size_t)pix * 4 * nl;
+
+    float ob[LPL][4];
+    load_pixel<LPL>(a.iquv + off, nl, lane, ob);
+    if (c.use_slight && c.slight_per_pixel) load_pixel<LPL>(c.slight + off, nl, lane, slg);
+
+    // initial model
+    if (lane < 11) {
+      const double v = a.init_models ? a.init_models[pix * 11 + lane] : c.init[lane];
+      sm.m[lane] = v;
+    }
+    __syncwarp();
+    uint32_t st = 0;
+    if (c.init_mode == 0) st |= classical_warp<LPL>(c, ob, dld, valid, lane, sm.m);
+    __syncwarp();
+
+    Lane<LPL> ln;
+    Angles an;
+    float syn[LPL][4], pure[LPL][4];
+    float J[LPL][4][10];
+    synth_lane<LPL>(c, sm.m, dlv, lane, ln, an, syn, pure, slg, sm.stg);
+    rf_lane<LPL>(c, sm.m, ln, an, pure, slg, lane, sm.stg, J);
+    normal_eq<LPL>(c, J, syn, ob, valid, lane, sm);
+    float ochisqr = chisq<LPL>(c, syn, ob, valid);
+    const float chisqr0 = ochisqr;
+    if (lane < 11) sm.t[lane] = sm.m[lane];
+    __syncwarp();
+
+    float flambda = c.ilambda, pbf = 1.f;
+    int iter = 0, acc = 0;
+    bool stop = false;
+    do {
+      solve10<LPL>(sm, flambda, lane, c.numerics != 0);
+      if (lane == 0) apply_delta_check(c, sm.m, sm.vec, sm.t);
+      __syncwarp();
+      synth_lane<LPL>(c, sm.t, dlv, lane, ln, an, syn, pure, slg, sm.stg);
+      const float chisqr = chisq<LPL>(c, syn, ob, valid);
+      if (iter == 0) {
+        if (a.step_delta && lane < 10) a.step_delta[pix * 10 + lane] = sm.vec[lane];
+        if (a.step_trial && lane < 11) a.step_trial[pix * 11 + lane] = sm.t[lane];
+        if (lane == 0 && a.step_chi2_start) a.step_chi2_start[pix] = chisqr0;
+        if (lane == 0 && a.step_chi2_trial) a.step_chi2_trial[pix] = chisqr;
+      }
+      if ((double)fabsf(((ochisqr) - (chisqr)) * 100 / (chisqr)) < c.toplim || (chisqr) < 0.0001f) {
+        stop = true;
+        st |= GM_PIX_CHI2_EXIT;
+      }
+      if ((chisqr) - (ochisqr) < 0.f) {
+        flambda = flambda / (5.f * pbf);
+        if (lane < 11) sm.m[lane] = sm.t[lane];
+        __syncwarp();
+        if (c.quirks) rf_lane<LPL>(c, sm.m, ln, an, syn, slg, lane, sm.stg, J);
+        else rf_lane<LPL>(c, sm.m, ln, an, pure, slg, lane, sm.stg, J);
+        normal_eq<LPL>(c, J, syn, ob, valid, lane, sm);
+        if (c.stop_dchi2 > 0.0 && (double)(ochisqr - chisqr) < c.stop_dchi2) stop = true;
+        ochisqr = chisqr;
+        ++acc;
+      } else {
+        flambda = flambda * 10.f * pbf;
+      }
+      if (flambda > 1e+7f || flambda < 1e-25f) {
+        stop = true;
+        st |= GM_PIX_LAMBDA_EXIT;
+      }
+      ++iter;
+      if (c.logclambda) pbf = log10f(chisqr) / log10f(chisqr0);
+    } while (iter < c.miter && !stop);
+    if (!stop) st |= GM_PIX_MAXITER;
+    if (!isfinite(ochisqr)) st |= GM_PIX_NONFINITE;
+
+    // outputs: last accepted model and chi2, trial count, last trial synthesis
+    if (lane < 11) {
+      if (a.model) a.model[pix * 11 + lane] = (float)sm.m[lane];
+      if (a.model_f64) a.model_f64[pix * 11 + lane] = sm.m[lane];
+    }
+    if (lane == 0) {
+      if (a.chi2) a.chi2[pix] = ochisqr;
+      if (a.iters) a.iters[pix] = iter;
+      if (a.accepted) a.accepted[pix] = acc;
+      if (a.status) a.status[pix] = st;
+    }
+    if (a.fitted) {
+#pragma unroll
+      for (int k = 0; k < LPL; ++k) {
+        const int l = lane + 32 * k;
+        if (l < nl)
+#pragma unroll
+          for (int s = 0; s < 4; ++s) a.fitted[off + s * nl + l] = syn[k][s];
+      }
+    }
+    my_iter += iter;
+    my_acc += acc;
+    __syncwarp();
+  }
+  if (lane == 0 && (my_iter | my_acc)) {
+    atomicAdd(&a.work->iterations, my_iter);
+    atomicAdd(&a.work->accepted, my_acc);
+  }
+}
+
+// Synthesis (+ response functions) of one model per warp
+// (kernel_synthesis, gmilos.cu:71-84, batched).
+template <int LPL>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+synth_kernel(const DevCfg c, const SynthArgs a) {
+  __shared__ WarpSmem<LPL> smem[kWarpsPerBlock];
+  const int lane = threadIdx.x & 31;
+  WarpSmem<LPL>& sm = smem[threadIdx.x >> 5];
+  for (int i = lane; i < 96 * LPL; i += 32) sm.stg[i] = 0.f;
+  const int nl = c.nl, nt = c.nterms;
+  float dlv[LPL];
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+    dlv[k] = (l < nl) ? c.dl[l] : 0.f;
+  }
+  float slg[LPL][4];
+  if (c.use_slight && !c.slight_per_pixel) load_pixel<LPL>(c.slight, nl, lane, slg);
+  else {
+#pragma unroll
+    for (int k = 0; k < LPL; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
+  }
+  __syncwarp();
+  const int64_t wid = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
+  const int64_t nw = (int64_t)gridDim.x * kWarpsPerBlock;
+  for (int64_t pix = wid; pix < a.npix; pix += nw) {
+    const size_t off = (size_t)pix * 4 * nl;
+    if (c.use_slight && c.slight_per_pixel) load_pixel<LPL>(c.slight + off, nl, lane, slg);
+    if (lane < 11) sm.m[lane] = a.models_f64 ? a.models_f64[pix * 11 + lane] : (double)a.models_f32[pix * 11 + lane];
+    __syncwarp();
+    Lane<LPL> ln;
+    Angles an;
+    float syn[LPL][4], pure[LPL][4];
+    synth_lane<LPL>(c, sm.m, dlv, lane, ln, an, syn, pure, slg, sm.stg);
+#pragma unroll
+    for (int k = 0; k < LPL; ++k) {
+      const int l = lane + 32 * k;
+      if (l < nl)
+#pragma unroll
+        for (int s = 0; s < 4; ++s) a.iquv[off + s * nl + l] = syn[k][s];
+    }
+    if (a.rf) {
+      float J[LPL][4][10];
+      rf_lane<LPL>(c, sm.m, ln, an, pure, slg, lane, sm.stg, J);
+      const size_t roff = (size_t)pix * 4 * nt * nl;
+#pragma unroll
+      for (int k = 0; k < LPL; ++k) {
+        const int l = lane + 32 * k;
+        if (l < nl)
+#pragma unroll
+          for (int s = 0; s < 4; ++s)
+#pragma unroll
+            for (int t = 0; t < 10; ++t) a.rf[roff + ((size_t)s * nt + t) * nl + l] = J[k][s][t];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Pure ME profiles (no PSF, no stray light) on an arbitrary offset grid, one
+// thread per (pixel, sample): used to synthesise observations on fine grids.
+__global__ void synth_grid_kernel(const DevCfg c, const double* __restrict__ models, int64_t npix,
+                                  const double* __restrict__ offs, int ngrid, float* __restrict__ out) {
+  const int64_t total = npix * ngrid;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t pix = i / ngrid;
+    const int l = (int)(i - pix * ngrid);
+    const double* m = models + pix * 11;
+    const float CC = (float)(kPi / 180.0);
+    float sgm, cgm, sina, cosa;
+    __sincosf((float)(m[GM] * (double)CC), &sgm, &cgm);
+    __sincosf((float)(2 * m[AZ] * (double)CC), &sina, &cosa);
+    const float sinis = sgm * sgm, cosis_2 = __fdividef(1.f + cgm * cgm, 2.f);
+    const float ulos = __fdividef((float)(m[VLOS] * c.lambda0), (float)(kVlight * m[DOPP]));
+    const float parcial = (float)((c.lambda0 * c.lambda0 / m[DOPP]) * kLarmor);
+    const float v0 = __fdividef((float)offs[l], (float)m[DOPP]) - ulos;
+    float fi[3] = {0, 0, 0}, shi[3] = {0, 0, 0};
+    for (int g = 0; g < 3; ++g) {
+      const int n = (g == 0) ? c.n_pi : c.n_sig;
+      for (int kk = 0; kk < n; ++kk) {
+        float nu, wex;
+        if (g == 0) { nu = parcial * c.nup[kk]; wex = c.wep[kk]; }
+        else if (g == 1) { nu = parcial * c.nub[kk]; wex = c.web[kk]; }
+        else { nu = -(parcial * c.nub[c.n_sig - 1 - kk]); wex = c.wer[kk]; }
+        const float v = v0 - (float)((double)nu * m[BFLD]);
+        float h, f;
+        voigt(m[AA], v, h, f);
+        fi[g] += wex * h;
+        shi[g] += wex * f * 2.f;
+      }
+    }
+    const float E0_2 = __fdividef((float)(m[ETA0] * (double)c.fo), 2.f);
+    const float p1 = fi[1] + fi[2];
+    const float p2 = E0_2 * (fi[0] - 0.5f * p1);
+    const float p3 = E0_2 * (shi[0] - 0.5f * (shi[1] + shi[2]));
+    const float ein = E0_2 * (fi[0] * sinis + p1 * cosis_2);
+    const float eq = p2 * sinis * cosa, eu = p2 * sinis * sina, ev = (fi[2] - fi[1]) * (E0_2 * cgm);
+    const float rq = p3 * sinis * cosa, ru = p3 * sinis * sina, rv = (shi[2] - shi[1]) * (E0_2 * cgm);
+    const float ei = 1.f + ein, ei2 = ei * ei;
+    const float gp1 = ei2 - eq * eq - eu * eu - ev * ev + rq * rq + ru * ru + rv * rv;
+    const float gp3 = ei2 + rq * rq + ru * ru + rv * rv;
+    const float gp2 = eq * rq + eu * ru + ev * rv;
+    const float dt = ei2 * gp1 - gp2 * gp2;
+    const float dtiaux = (float)((double)__fdividef(1.f, dt) * (-(m[S1] * (double)c.mu)));
+    const int64_t o = pix * 4 * ngrid + l;
+    out[o] = (float)(m[S0] - (double)(dtiaux * ei * gp3));
+    out[o + ngrid] = dtiaux * (ei2 * eq + ei * (ev * ru - eu * rv) + rq * gp2);
+    out[o + 2 * ngrid] = dtiaux * (ei2 * eu + ei * (eq * rv - ev * rq) + ru * gp2);
+    out[o + 3 * ngrid] = dtiaux * (ei2 * ev + ei * (eu * rq - eq * ru) + rv * gp2);
+  }
+}
+
+template <typename T>
+__global__ void peak_kernel(int iters, T* sink) {
+  T a[kPeakChains];
+  const T x = (T)1.0000001, y = (T)1e-7;
+#pragma unroll
+  for (int c = 0; c < kPeakChains; ++c) a[c] = (T)(threadIdx.x + c);
+  for (int i = 0; i < iters; ++i)
+#pragma unroll
+    for (int c = 0; c < kPeakChains; ++c) a[c] = fma(a[c], x, y);
+  T s = 0;
+#pragma unroll
+  for (int c = 0; c < kPeakChains; ++c) s += a[c];
+  if (s == (T)-1) sink[(blockIdx.x * blockDim.x + threadIdx.x) & 1023] = s;
+}
+
+cudaError_t launch_peak(int kind, int blocks, int threads, int iters, void* sink, cudaStream_t s) {
+  if (kind == 0) peak_kernel<float><<<blocks, threads, 0, s>>>(iters, (float*)sink);
+  else peak_kernel<double><<<blocks, threads, 0, s>>>(iters, (double*)sink);
+  return cudaGetLastError();
+}
+
+int invert_blocks_per_sm(int nl) {
+  int n = 0;
+  if (nl <= 32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, invert_kernel<1>, kWarpsPerBlock * 32, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, invert_kernel<2>, kWarpsPerBlock * 32, 0);
+  return n;
+}
+
+cudaError_t launch_invert(const DevCfg& cfg, const InvertArgs& a, int grid, cudaStream_t s) {
+  if (cfg.nl <= 32) invert_kernel<1><<<grid, kWarpsPerBlock * 32, 0, s>>>(cfg, a);
+  else invert_kernel<2><<<grid, kWarpsPerBlock * 32, 0, s>>>(cfg, a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_synth(const DevCfg& cfg, const SynthArgs& a, cudaStream_t s) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int64_t need = (a.npix + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  int grid = (int)(need < (int64_t)sms * 16 ? need : (int64_t)sms * 16);
+  if (grid < 1) grid = 1;
+  if (cfg.nl <= 32) synth_kernel<1><<<grid, kWarpsPerBlock * 32, 0, s>>>(cfg, a);
+  else synth_kernel<2><<<grid, kWarpsPerBlock * 32, 0, s>>>(cfg, a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_synth_grid(const DevCfg& cfg, const double* models, int64_t npix,
+                              const double* offsets, int ngrid, float* out, cudaStream_t s) {
+  const int64_t total = npix * ngrid;
+  int64_t blocks = (total + 255) / 256;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  if (blocks < 1) blocks = 1;
+  synth_grid_kernel<<<(int)blocks, 256, 0, s>>>(cfg, models, npix, offsets, ngrid, out);
+  return cudaGetLastError();
+}
+
+}  // namespace gm

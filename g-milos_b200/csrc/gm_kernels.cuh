@@ -1,0 +1,60 @@
+// gm_kernels.cuh -- the engine's kernels and their host-side launchers.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gm_device.cuh"
+
+namespace gm {
+
+constexpr int kWarpsPerBlock = 4;
+
+// Work counters shared by the warps of one persistent launch.
+struct WorkCounters {
+  unsigned long long next_pixel;   // work-stealing cursor
+  unsigned long long iterations;   // sum of LM trials
+  unsigned long long accepted;     // sum of accepted steps
+  unsigned long long pad;
+};
+
+struct InvertArgs {
+  const float* iquv;          // [P][4][nl]
+  int64_t npix;
+  const double* init_models;  // [P][11] or null
+  float* model;               // [P][11] or null
+  double* model_f64;          // [P][11] or null
+  float* chi2;                // [P] or null
+  int* iters;                 // [P] or null
+  int* accepted;              // [P] or null
+  float* fitted;              // [P][4][nl] or null
+  uint32_t* status;           // [P] or null
+  float* step_delta;          // [P][10] first-iteration step, or null
+  double* step_trial;         // [P][11] first-iteration trial model, or null
+  float* step_chi2_start;     // [P] chi2 of the starting model, or null
+  float* step_chi2_trial;     // [P] chi2 of the first trial, or null
+  WorkCounters* work;         // zeroed before the launch
+};
+
+struct SynthArgs {
+  const float* models_f32;    // [P][11] (one of the two)
+  const double* models_f64;
+  int64_t npix;
+  float* iquv;                // [P][4][nl]
+  float* rf;                  // [P][4][nterms][nl] or null
+};
+
+// launchers (gm_kernels.cu); return the CUDA error of the launch
+cudaError_t launch_invert(const DevCfg& cfg, const InvertArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_synth(const DevCfg& cfg, const SynthArgs& a, cudaStream_t s);
+cudaError_t launch_synth_grid(const DevCfg& cfg, const double* models, int64_t npix,
+                              const double* offsets, int ngrid, float* out, cudaStream_t s);
+// resident blocks per SM of the inversion kernel for this nl
+int invert_blocks_per_sm(int nl);
+
+// FMA-issue-bound microbenchmark (kind 0: FP32, 1: FP64); each thread runs
+// kPeakChains independent FMA chains of `iters` steps.
+constexpr int kPeakChains = 8;
+cudaError_t launch_peak(int kind, int blocks, int threads, int iters, void* sink, cudaStream_t s);
+
+}  // namespace gm

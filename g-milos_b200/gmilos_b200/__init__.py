@@ -1,0 +1,381 @@
+"""Python binding of the B200 Milne-Eddington inversion engine (libgmilos.so).
+
+A thin ctypes layer over the C ABI declared in include/gmilos.h.  Arrays may
+be numpy arrays (host memory) or torch CUDA tensors (device memory); the
+engine copies host data itself.  There is no CPU fallback: every entry point
+needs the compiled library and a CUDA device, and raises otherwise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgmilos.so")
+PKG_ROOT = os.path.dirname(HERE)
+MAX_NL = 64
+NPAR = 11
+ABI_VERSION = 1
+PARAM_NAMES = ("eta0", "B", "vlos", "dopp", "aa", "gm", "az", "S0", "S1", "mac", "alfa")
+
+GM_OK = 0
+STATUS_NAMES = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory / over budget",
+                4: "not configured", 5: "unsupported", 6: "timeout", 7: "cancelled", 8: "I/O error"}
+
+PIX_INIT_NAN = 0x01
+PIX_MAXITER = 0x02
+PIX_LAMBDA_EXIT = 0x04
+PIX_CHI2_EXIT = 0x08
+PIX_NONFINITE = 0x10
+PIX_BAD_INPUT = 0x20
+
+INIT_CLASSICAL, INIT_GIVEN, INIT_PER_PIXEL = 0, 1, 2
+NUMERICS_REFERENCE, NUMERICS_ACCURATE = 0, 1
+
+# Symbols include/gmilos.h declares (checked by the tests against the .so).
+EXPORTS = ("gm_create", "gm_destroy", "gm_last_error", "gm_status_string", "gm_config_defaults",
+           "gm_configure", "gm_invert", "gm_invert_ex", "gm_synthesize", "gm_synthesize_f64",
+           "gm_synthesize_grid", "gm_lm_step", "gm_submit", "gm_poll", "gm_cancel", "gm_zeeman_from_levels",
+           "gm_psf_gaussian", "gm_psf_from_table", "gm_get_stats", "gm_measure_peaks")
+
+
+class GmError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__("gmilos: %s%s" % (STATUS_NAMES.get(status, status), (": " + msg) if msg else ""))
+
+
+class Zeeman(C.Structure):
+    _fields_ = [("n_pi", C.c_int), ("n_sig", C.c_int),
+                ("nub", C.c_float * 10), ("nup", C.c_float * 10), ("nur", C.c_float * 10),
+                ("web", C.c_float * 10), ("wep", C.c_float * 10), ("wer", C.c_float * 10),
+                ("gl", C.c_float), ("gu", C.c_float), ("geff", C.c_float), ("fo", C.c_float)]
+
+
+class Config(C.Structure):
+    _fields_ = [("abi_version", C.c_int), ("nl", C.c_int), ("lambda0", C.c_double),
+                ("lambda_", C.c_double * MAX_NL), ("zeeman", Zeeman), ("use_psf", C.c_int),
+                ("psf", C.c_double * MAX_NL), ("mu", C.c_float), ("weight", C.c_float * 4),
+                ("noise", C.c_float), ("fix", C.c_int * NPAR), ("init_model", C.c_double * NPAR),
+                ("init_mode", C.c_int), ("miter", C.c_int), ("ilambda", C.c_float),
+                ("toplim", C.c_double), ("logclambda", C.c_int), ("stop_dchi2", C.c_double),
+                ("use_slight", C.c_int), ("slight_per_pixel", C.c_int),
+                ("slight", C.POINTER(C.c_float)), ("reference_quirks", C.c_int),
+                ("numerics", C.c_int)]
+
+
+class Request(C.Structure):
+    _fields_ = [("iquv", C.c_void_p), ("npix", C.c_int64), ("nl", C.c_int),
+                ("model", C.c_void_p), ("chi2", C.c_void_p), ("iters", C.c_void_p),
+                ("status", C.c_void_p), ("fix", C.POINTER(C.c_int))]
+
+
+class Stats(C.Structure):
+    _fields_ = [("pixels", C.c_int64), ("iterations", C.c_int64), ("accepted", C.c_int64),
+                ("kernel_ms", C.c_float), ("grid_blocks", C.c_int), ("block_threads", C.c_int),
+                ("warps_per_block", C.c_int), ("kernel_launches", C.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libgmilos.so; raises if the extension was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise GmError(5, "libgmilos.so not built (run `make -C %s` or __graft_entry__.build())" % PKG_ROOT)
+        L = C.CDLL(LIB_PATH)
+        vp, i64 = C.c_void_p, C.c_int64
+        L.gm_create.argtypes = [C.c_int, C.c_size_t, C.POINTER(vp)]
+        L.gm_destroy.argtypes = [vp]
+        L.gm_last_error.argtypes = [vp]
+        L.gm_last_error.restype = C.c_char_p
+        L.gm_status_string.argtypes = [C.c_int]
+        L.gm_status_string.restype = C.c_char_p
+        L.gm_config_defaults.argtypes = [C.POINTER(Config)]
+        L.gm_config_defaults.restype = None
+        L.gm_configure.argtypes = [vp, C.POINTER(Config)]
+        L.gm_invert.argtypes = [vp, vp, i64, C.c_int, vp, vp, vp, vp, vp, vp]
+        L.gm_invert_ex.argtypes = [vp, vp, i64, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.gm_lm_step.argtypes = [vp, vp, i64, C.c_int, vp, C.c_float, vp, vp, vp, vp, vp]
+        L.gm_synthesize.argtypes = [vp, vp, i64, vp, vp, vp]
+        L.gm_synthesize_f64.argtypes = [vp, vp, i64, vp, vp, vp]
+        L.gm_synthesize_grid.argtypes = [vp, vp, i64, vp, C.c_int, vp, vp]
+        L.gm_submit.argtypes = [vp, C.POINTER(Request), C.POINTER(C.c_uint64)]
+        L.gm_poll.argtypes = [vp, C.c_uint64, C.c_int]
+        L.gm_cancel.argtypes = [vp, C.c_uint64]
+        L.gm_zeeman_from_levels.argtypes = [C.c_double] * 7 + [C.POINTER(Zeeman)]
+        L.gm_psf_gaussian.argtypes = [C.c_double, vp, C.c_int, vp]
+        L.gm_psf_from_table.argtypes = [vp, vp, C.c_int, vp, C.c_int, C.c_double, vp]
+        L.gm_get_stats.argtypes = [vp, C.POINTER(Stats)]
+        L.gm_measure_peaks.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    """Raw pointer of a numpy array or torch tensor (None -> NULL)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return C.c_void_p(a.data_ptr())
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return C.c_void_p(a.ctypes.data)
+
+
+def _check(st, ctx=None):
+    if st != GM_OK:
+        msg = lib().gm_last_error(ctx).decode() if ctx else ""
+        raise GmError(st, msg)
+
+
+# ------------------------------------------------------------------ set-up
+def zeeman_from_levels(sl, ll, jl, su, lu, ju, fos=1.0):
+    z = Zeeman()
+    _check(lib().gm_zeeman_from_levels(sl, ll, jl, su, lu, ju, fos, C.byref(z)))
+    return z
+
+
+def fe6173():
+    """Fe I 6173.3356 A (atomic-parameter entry `5P 1.0- 5D 0.0`)."""
+    return 6173.3356, zeeman_from_levels(2, 1, 1.0, 2, 2, 0.0, 1.0)
+
+
+def grid_offsets_mA(first_mA, step_mA, last_mA):
+    n = int(((last_mA - first_mA) / step_mA) + 1)
+    off = np.empty(n)
+    off[0] = first_mA
+    for i in range(1, n):
+        off[i] = off[i - 1] + step_mA
+    return off
+
+
+def grid_lambda(lambda0, first_mA, step_mA, last_mA):
+    """Absolute wavelengths of a .grid line, accumulated like gmilos.cu:184-189."""
+    n = int(((last_mA - first_mA) / step_mA) + 1)
+    lam = np.empty(n)
+    lam[0] = lambda0 + first_mA / 1000.0
+    for i in range(1, n):
+        lam[i] = lam[i - 1] + step_mA / 1000.0
+    return lam
+
+
+def psf_gaussian(fwhm_mA, lam):
+    lam = np.ascontiguousarray(lam, dtype=np.float64)
+    out = np.zeros(len(lam))
+    _check(lib().gm_psf_gaussian(fwhm_mA, _ptr(lam), len(lam), _ptr(out)))
+    return out
+
+
+def psf_from_table(x_mA, y, offsets_mA, step_mA):
+    x = np.ascontiguousarray(x_mA, dtype=np.float64)
+    yy = np.ascontiguousarray(y, dtype=np.float64)
+    off = np.ascontiguousarray(offsets_mA, dtype=np.float64)
+    out = np.zeros(len(off))
+    _check(lib().gm_psf_from_table(_ptr(x), _ptr(yy), len(x), _ptr(off), len(off), step_mA, _ptr(out)))
+    return out
+
+
+def make_config(lam, lambda0, zeeman, psf=None, mu=1.0, weight=(1, 1, 1, 1), noise=1e-6,
+                fix=(1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0), init=None, init_mode=INIT_CLASSICAL,
+                miter=50, ilambda=0.1, toplim=1e-12, logclambda=0, stop_dchi2=0.0,
+                slight=None, slight_per_pixel=False, reference_quirks=1, numerics=0):
+    c = Config()
+    lib().gm_config_defaults(C.byref(c))
+    lam = np.asarray(lam, dtype=np.float64)
+    if len(lam) > MAX_NL:
+        raise ValueError("at most %d wavelength samples" % MAX_NL)
+    c.nl = len(lam)
+    c.lambda0 = lambda0
+    for i, v in enumerate(lam):
+        c.lambda_[i] = v
+    c.zeeman = zeeman
+    c.use_psf = 0 if psf is None else 1
+    if psf is not None:
+        for i, v in enumerate(psf):
+            c.psf[i] = v
+    c.mu = mu
+    for i in range(4):
+        c.weight[i] = weight[i]
+    c.noise = noise
+    for i in range(NPAR):
+        c.fix[i] = int(fix[i])
+    if init is not None:
+        for i in range(NPAR):
+            c.init_model[i] = init[i]
+    c.init_mode = init_mode
+    c.miter = miter
+    c.ilambda = ilambda
+    c.toplim = toplim
+    c.logclambda = logclambda
+    c.stop_dchi2 = stop_dchi2
+    c.reference_quirks = reference_quirks
+    c.numerics = numerics
+    c._slight_ref = None
+    if slight is not None:
+        c.use_slight = 1
+        c.slight_per_pixel = 1 if slight_per_pixel else 0
+        if hasattr(slight, "data_ptr"):
+            c.slight = C.cast(C.c_void_p(slight.data_ptr()), C.POINTER(C.c_float))
+        else:
+            arr = np.ascontiguousarray(slight, dtype=np.float32)
+            c._slight_ref = arr
+            c.slight = arr.ctypes.data_as(C.POINTER(C.c_float))
+    return c
+
+
+# ------------------------------------------------------------------ engine
+class Engine:
+    """One engine context on one CUDA device (gm_create / gm_destroy)."""
+
+    def __init__(self, device=0, hbm_budget=0):
+        self._ctx = C.c_void_p()
+        _check(lib().gm_create(device, hbm_budget, C.byref(self._ctx)))
+        self.cfg = None
+
+    def close(self):
+        if self._ctx:
+            lib().gm_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def configure(self, cfg):
+        _check(lib().gm_configure(self._ctx, C.byref(cfg)), self._ctx)
+        self.cfg = cfg
+
+    @property
+    def nl(self):
+        return self.cfg.nl
+
+    def invert(self, iquv, init_models=None, fitted=False, out=None, stream=None):
+        """Invert a cube iquv [P][4][nl] (numpy: host; torch CUDA tensor: device).
+
+        Returns dict(model [P][11] f32, model64 [P][11] f64, chi2, iters, accepted,
+        status, fitted [P][4][nl] or None) in the same memory space as the input."""
+        P = int(iquv.shape[0])
+        nl = self.nl
+        if tuple(iquv.shape[1:]) != (4, nl):
+            raise ValueError("iquv must be [P][4][%d]" % nl)
+        if out is None:
+            out = self._alloc_outputs(iquv, P, nl, fitted)
+        st = lib().gm_invert_ex(self._ctx, _ptr(iquv), P, nl, _ptr(init_models), _ptr(out["model"]),
+                                _ptr(out["model64"]), _ptr(out["chi2"]), _ptr(out["iters"]),
+                                _ptr(out["accepted"]), _ptr(out["fitted"]), _ptr(out["status"]),
+                                C.c_void_p(stream) if stream else None)
+        _check(st, self._ctx)
+        return out
+
+    def invert_plain(self, iquv, model, chi2=None, iters=None, fitted=None, status=None, stream=None):
+        """gm_invert: the reference-facing call with caller-owned buffers."""
+        P = int(iquv.shape[0])
+        st = lib().gm_invert(self._ctx, _ptr(iquv), P, self.nl, _ptr(model), _ptr(chi2), _ptr(iters),
+                             _ptr(fitted), _ptr(status), C.c_void_p(stream) if stream else None)
+        _check(st, self._ctx)
+
+    @staticmethod
+    def _alloc_outputs(like, P, nl, fitted):
+        if hasattr(like, "data_ptr"):
+            import torch
+            dev = like.device
+            mk = lambda shape, dt: torch.empty(shape, dtype=dt, device=dev)
+            f32, f64, i32 = torch.float32, torch.float64, torch.int32
+        else:
+            mk = lambda shape, dt: np.empty(shape, dtype=dt)
+            f32, f64, i32 = np.float32, np.float64, np.int32
+        o = {"model": mk((P, NPAR), f32), "model64": mk((P, NPAR), f64), "chi2": mk((P,), f32),
+             "iters": mk((P,), i32), "accepted": mk((P,), i32), "status": mk((P,), i32),
+             "fitted": mk((P, 4, nl), f32) if fitted else None}
+        return o
+
+    def lm_step(self, iquv, models, flambda):
+        """One LM iteration from explicit states: (delta [P][10], trial [P][11],
+        chi2_start [P], chi2_trial [P]) as host numpy arrays."""
+        P = int(iquv.shape[0])
+        models = np.ascontiguousarray(models, dtype=np.float64)
+        d = np.empty((P, 10), dtype=np.float32)
+        t = np.empty((P, NPAR), dtype=np.float64)
+        c0 = np.empty(P, dtype=np.float32)
+        c1 = np.empty(P, dtype=np.float32)
+        _check(lib().gm_lm_step(self._ctx, _ptr(iquv), P, self.nl, _ptr(models), float(flambda),
+                                _ptr(d), _ptr(t), _ptr(c0), _ptr(c1), None), self._ctx)
+        return d, t, c0, c1
+
+    def synthesize(self, models, rf=False, stream=None):
+        """Synthesis (+ response functions [P][4][10][nl]) of models [P][11] (float64 or float32)."""
+        P = int(models.shape[0])
+        nl = self.nl
+        is_t = hasattr(models, "data_ptr")
+        if is_t:
+            import torch
+            spec = torch.empty((P, 4, nl), dtype=torch.float32, device=models.device)
+            r = torch.empty((P, 4, 10, nl), dtype=torch.float32, device=models.device) if rf else None
+            f64 = models.dtype == torch.float64
+        else:
+            spec = np.empty((P, 4, nl), dtype=np.float32)
+            r = np.empty((P, 4, 10, nl), dtype=np.float32) if rf else None
+            f64 = models.dtype == np.float64
+        fn = lib().gm_synthesize_f64 if f64 else lib().gm_synthesize
+        _check(fn(self._ctx, _ptr(models), P, _ptr(spec), _ptr(r), C.c_void_p(stream) if stream else None),
+               self._ctx)
+        return (spec, r) if rf else spec
+
+    def synthesize_grid(self, models, offsets_A, stream=None):
+        """Pure ME profiles (no PSF / stray light) of models [P][11] f64 on offsets [A]."""
+        P = int(models.shape[0])
+        n = int(offsets_A.shape[0])
+        if hasattr(models, "data_ptr"):
+            import torch
+            out = torch.empty((P, 4, n), dtype=torch.float32, device=models.device)
+        else:
+            out = np.empty((P, 4, n), dtype=np.float32)
+        _check(lib().gm_synthesize_grid(self._ctx, _ptr(models), P, _ptr(offsets_A), n, _ptr(out),
+                                        C.c_void_p(stream) if stream else None), self._ctx)
+        return out
+
+    def submit(self, iquv, model, chi2=None, iters=None, status=None, fix=None):
+        r = Request()
+        r.iquv = _ptr(iquv)
+        r.npix = int(iquv.shape[0])
+        r.nl = self.nl
+        r.model = _ptr(model)
+        r.chi2 = _ptr(chi2)
+        r.iters = _ptr(iters)
+        r.status = _ptr(status)
+        if fix is not None:
+            arr = (C.c_int * NPAR)(*[int(x) for x in fix])
+            r.fix = C.cast(arr, C.POINTER(C.c_int))
+        t = C.c_uint64()
+        _check(lib().gm_submit(self._ctx, C.byref(r), C.byref(t)), self._ctx)
+        return t.value
+
+    def poll(self, ticket, timeout_us=-1):
+        return lib().gm_poll(self._ctx, ticket, timeout_us)
+
+    def cancel(self, ticket):
+        _check(lib().gm_cancel(self._ctx, ticket), self._ctx)
+
+    def measure_peaks(self):
+        """(fp32, fp64) FMA peaks of this device in TFLOP/s."""
+        a, b = C.c_double(), C.c_double()
+        _check(lib().gm_measure_peaks(self._ctx, C.byref(a), C.byref(b)), self._ctx)
+        return a.value, b.value
+
+    def stats(self):
+        s = Stats()
+        _check(lib().gm_get_stats(self._ctx, C.byref(s)), self._ctx)
+        return {k: getattr(s, k) for k, _ in Stats._fields_}

@@ -1,0 +1,221 @@
+/*
+ * gmilos.h -- C ABI of the B200 Milne-Eddington inversion engine.
+ *
+ * The engine is a drop-in for the two device paths of G-MILOS: the per-pixel
+ * Levenberg-Marquardt inversion (the __global__ lm_mils / lm_mils_11 kernels,
+ * milosUtils.cuh:54-60, launched at gmilos.cu:1233-1240) and the single-model
+ * synthesis with response functions (kernel_synthesis, gmilos.cu:71-84,
+ * launched at gmilos.cu:557-562).  The reference passes its configuration
+ * through ~20 __constant__ symbols uploaded at gmilos.cu:1184-1198; here it is
+ * one gm_config struct handed to gm_configure.
+ *
+ * Conventions
+ *  - every call returns a gm_status and never exits the process;
+ *  - handles are opaque; the caller owns every buffer it passes;
+ *  - pointers may be host (pageable or pinned) or device memory: the engine
+ *    checks with cudaPointerGetAttributes and copies host data itself;
+ *  - `stream` is a cudaStream_t passed as void* (NULL = the context's stream);
+ *    calls on host buffers return after the results are in host memory,
+ *    calls on device buffers are stream-ordered and return after launch;
+ *  - one context per host thread, or serialise calls on a shared context
+ *    (the serving entry points gm_submit / gm_poll / gm_cancel are
+ *    internally locked and may be called from any thread).
+ *
+ * Layouts (all float32 unless stated; pixel-major like the reference's
+ * spectroImagen, gmilos.cu:1200):
+ *   Stokes cube  iquv [P][4][nl]     (I, Q, U, V rows per pixel)
+ *   model        [P][11]             eta0, B [G], vlos [km/s], dopp [A],
+ *                                    damping, gamma [deg], phi [deg], S0, S1,
+ *                                    vmac [km/s], alpha (filling factor)
+ *   response fn  rf [P][4][nterms][nl]
+ */
+#ifndef GMILOS_H
+#define GMILOS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GM_MAX_NL 64          /* wavelength samples per pixel (reference: MAX_LAMBDA 50) */
+#define GM_NPAR 11
+#define GM_ABI_VERSION 1
+
+typedef enum {
+    GM_OK = 0,
+    GM_ERR_INVALID = 1,       /* bad argument or configuration */
+    GM_ERR_CUDA = 2,          /* CUDA runtime error (see gm_last_error) */
+    GM_ERR_NOMEM = 3,         /* allocation failed or request exceeds the HBM budget */
+    GM_ERR_NOT_CONFIGURED = 4,
+    GM_ERR_UNSUPPORTED = 5,   /* feature not available in this build / configuration */
+    GM_ERR_TIMEOUT = 6,       /* gm_poll waited its full timeout */
+    GM_ERR_CANCELLED = 7,
+    GM_ERR_IO = 8             /* file could not be read or written */
+} gm_status;
+
+/* per-pixel status bits written by gm_invert */
+#define GM_PIX_INIT_NAN      0x01u  /* a classical estimate was NaN and was replaced
+                                       (milosUtils.cu:621-628) */
+#define GM_PIX_MAXITER       0x02u  /* stopped at the iteration limit */
+#define GM_PIX_LAMBDA_EXIT   0x04u  /* stopped because lambda_LM left [1e-25, 1e7] */
+#define GM_PIX_CHI2_EXIT     0x08u  /* stopped by the relative-chi2 or chi2 < 1e-4 rule */
+#define GM_PIX_NONFINITE     0x10u  /* final chi2 not finite */
+#define GM_PIX_BAD_INPUT     0x20u  /* no valid continuum sample in Stokes I */
+
+typedef enum {
+    GM_INIT_CLASSICAL = 0,    /* reference: guess model + classical estimates of B, vlos,
+                                 gamma, phi (milosUtils.cu:616-628) */
+    GM_INIT_GIVEN = 1,        /* guess model as given, no estimates */
+    GM_INIT_PER_PIXEL = 2     /* caller supplies init_models [P][11] to gm_invert_ex */
+} gm_init_mode;
+
+/* Zeeman pattern of the line (Cuantic, defines.h:108-123) */
+typedef struct {
+    int n_pi, n_sig;
+    float nub[10], nup[10], nur[10];
+    float web[10], wep[10], wer[10];
+    float gl, gu, geff, fo;
+} gm_zeeman;
+
+/* Everything the reference's __constant__ symbols carry (gmilos.cu:46-68). */
+typedef struct {
+    int abi_version;              /* GM_ABI_VERSION */
+    int nl;                       /* wavelength samples, 1..GM_MAX_NL */
+    double lambda0;               /* line centre [A] (d_wlines_const[1]) */
+    double lambda[GM_MAX_NL];     /* absolute wavelengths [A] (d_lambda_const) */
+    gm_zeeman zeeman;             /* d_cuantic_const */
+    int use_psf;                  /* d_use_convolution_const */
+    double psf[GM_MAX_NL];        /* nl taps centred at nl/2 (d_psfFunction_const) */
+    float mu;                     /* d_ah_const */
+    float weight[4];              /* d_weight_const */
+    float noise;                  /* sigma^2, d_sigma_const */
+    int fix[GM_NPAR];             /* 1 = free (d_fix_const) */
+    double init_model[GM_NPAR];   /* d_initModel_const */
+    int init_mode;                /* gm_init_mode */
+    int miter;                    /* d_miter_const */
+    float ilambda;                /* d_ilambda_const */
+    double toplim;                /* d_toplim_const */
+    int logclambda;               /* d_logclambda_const */
+    double stop_dchi2;            /* >0: extra per-pixel stop when the accepted
+                                     chi2 improves by less than this (absolute);
+                                     0 = reference stop rule only */
+    int use_slight;               /* stray-light mixing on */
+    int slight_per_pixel;         /* 0: one profile slight[4][nl]; 1: map [P][4][nl] */
+    const float *slight;          /* profile (copied at gm_configure when global) */
+    int reference_quirks;         /* 1 (default): reproduce the reference's numerics
+                                     exactly where it deviates from the textbook
+                                     derivative (alpha RF of the mixed profile after
+                                     an accepted step, milosUtils.cu:675) */
+    int numerics;                 /* GM_NUMERICS_REFERENCE (default) or
+                                     GM_NUMERICS_ACCURATE */
+} gm_config;
+
+/* Trigonometry of the 10x10 Jacobi solve and of the field angles.
+ * REFERENCE uses the hardware approximations the reference uses
+ * (__sincosf, __fdividef; svdcordic.cu:38,97); their absolute error of a few
+ * 1e-7 is amplified by the badly scaled normal matrix into step differences
+ * of ~1e-3, so only this mode follows the reference's LM trajectories.
+ * ACCURATE uses correctly rounded sincosf/atanf and IEEE division there. */
+#define GM_NUMERICS_REFERENCE 0
+#define GM_NUMERICS_ACCURATE 1
+
+typedef struct gm_ctx gm_ctx;
+
+/* ---------------- lifecycle ---------------------------------------------- */
+gm_status gm_create(int device, size_t hbm_budget, gm_ctx **out);
+gm_status gm_destroy(gm_ctx *ctx);
+const char *gm_last_error(gm_ctx *ctx);
+const char *gm_status_string(gm_status s);
+void gm_config_defaults(gm_config *cfg);
+
+/* ---------------- configuration ------------------------------------------ */
+gm_status gm_configure(gm_ctx *ctx, const gm_config *cfg);
+
+/* ---------------- the two reference paths -------------------------------- */
+/* Invert P pixels (replaces lm_mils / lm_mils_11).  fitted (optional) receives
+ * the last trial synthesis per pixel, as the reference's spectraAdjusted
+ * (milosUtils.cu:658).  status (optional) receives GM_PIX_* bits. */
+gm_status gm_invert(gm_ctx *ctx, const float *iquv, int64_t npix, int nl,
+                    float *model, float *chi2, int *iters, float *fitted,
+                    uint32_t *status, void *stream);
+
+/* Extended form: per-pixel initial models, FP64 model output in the
+ * reference's Init_Model layout, accepted-step counts. Any pointer may be NULL. */
+gm_status gm_invert_ex(gm_ctx *ctx, const float *iquv, int64_t npix, int nl,
+                       const double *init_models, float *model, double *model_f64,
+                       float *chi2, int *iters, int *accepted, float *fitted,
+                       uint32_t *status, void *stream);
+
+/* One Levenberg-Marquardt iteration from explicit per-pixel states
+ * (models [P][11], damping flambda): the step delta [P][10] from the damped
+ * normal equations, the trial model [P][11] after step limits and range
+ * checks, and chi2 of the start and trial models (milosUtils.cu:645-660).
+ * Any output may be NULL. */
+gm_status gm_lm_step(gm_ctx *ctx, const float *iquv, int64_t npix, int nl,
+                     const double *models, float flambda, float *delta, double *trial,
+                     float *chi2_start, float *chi2_trial, void *stream);
+
+/* Synthesis with optional response functions for P models [P][11] (float or
+ * the FP64 Init_Model layout via gm_synthesize_f64); rf [P][4][nterms][nl]
+ * with nterms = 10 (11 when both vmac and alpha are free). */
+gm_status gm_synthesize(gm_ctx *ctx, const float *models, int64_t npix, float *iquv,
+                        float *rf, void *stream);
+gm_status gm_synthesize_f64(gm_ctx *ctx, const double *models, int64_t npix, float *iquv,
+                            float *rf, void *stream);
+
+/* ME profiles without PSF or stray light on an arbitrary grid of offsets from
+ * lambda0 (any length); used for data generation on fine grids. */
+gm_status gm_synthesize_grid(gm_ctx *ctx, const double *models, int64_t npix,
+                             const double *offsets_A, int ngrid, float *iquv, void *stream);
+
+/* ---------------- serving (continuous batching) --------------------------- */
+typedef uint64_t gm_ticket;
+typedef struct {
+    const float *iquv;            /* [P][4][nl] host or device */
+    int64_t npix;
+    int nl;
+    float *model;                 /* [P][11] */
+    float *chi2;                  /* [P] (optional) */
+    int *iters;                   /* [P] (optional) */
+    uint32_t *status;             /* [P] (optional) */
+    const int *fix;               /* optional per-request free mask [11] */
+} gm_request;
+
+gm_status gm_submit(gm_ctx *ctx, const gm_request *req, gm_ticket *ticket);
+gm_status gm_poll(gm_ctx *ctx, gm_ticket ticket, int timeout_us);
+gm_status gm_cancel(gm_ctx *ctx, gm_ticket ticket);
+
+/* ---------------- host helpers mirroring the reference's set-up ---------- */
+/* Zeeman pattern from LS quantum numbers (create_cuantic.c:31-215) */
+gm_status gm_zeeman_from_levels(double sl, double ll, double jl, double su, double lu,
+                                double ju, double fos, gm_zeeman *out);
+/* Gaussian PSF of FWHM [mA] on the grid, centred at lambda[nl/2] (fgaussC.c:14-87) */
+gm_status gm_psf_gaussian(double fwhm_mA, const double *lambda, int nl, double *psf);
+/* Tabulated PSF (offsets [mA], values) linearly interpolated at the grid
+ * offsets [mA] and centred at nl/2 (gmilos.cu:246-296, interpolLineal.c:46-98) */
+gm_status gm_psf_from_table(const double *x_mA, const double *y, int ntab,
+                            const double *offsets_mA, int nl, double step_mA, double *psf);
+
+/* ---------------- introspection ------------------------------------------ */
+typedef struct {
+    int64_t pixels;               /* pixels of the last gm_invert */
+    int64_t iterations;           /* sum of LM trials */
+    int64_t accepted;             /* sum of accepted steps */
+    float kernel_ms;              /* device time of the last inversion kernel */
+    int grid_blocks, block_threads, warps_per_block;
+    int kernel_launches;          /* engine kernels launched by the last call */
+} gm_stats;
+gm_status gm_get_stats(gm_ctx *ctx, gm_stats *out);
+
+/* Measured arithmetic peaks of this device (FFMA and DFMA issue-bound
+ * microbenchmarks, TFLOP/s counting an FMA as 2 flops) -- the denominators of
+ * the engine's roofline fraction.  Measurement helper, no reference
+ * counterpart. */
+gm_status gm_measure_peaks(gm_ctx *ctx, double *fp32_tflops, double *fp64_tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
