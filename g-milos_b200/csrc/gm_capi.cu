@@ -645,3 +645,92 @@ void serve_loop(gm_ctx* ctx) {
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------- no-alloc inversion
+// Scratch of gm_invert_noalloc: the work-stealing counters at offset 0 and the
+// global stray-light profile [4][nl] at offset 256.  A file-scope device array
+// of fixed size, resident on every device that loads the library.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[GM_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kNoallocMaxDevices = 64;
+constexpr size_t kNoallocSlightOffset = 256;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoallocMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  The first call
+// per device (with that device current) looks it up and loads the inversion
+// kernel, so later calls do neither.
+gm_status noalloc_scratch(int dev, void** out) {
+  if (dev < 0 || dev >= kNoallocMaxDevices) return GM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      return GM_ERR_CUDA;
+    }
+    if (gm::invert_blocks_per_sm(32) < 1 || gm::invert_blocks_per_sm(64) < 1) {
+      cudaGetLastError();
+      return GM_ERR_CUDA;
+    }
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return GM_OK;
+}
+
+}  // namespace
+
+extern "C" gm_status gm_invert_noalloc(const gm_config* cfg, const float* iquv, int64_t npix, int nl,
+                                       float* model, float* chi2, int* iters, float* fitted,
+                                       uint32_t* status, void* stream) {
+  if (!cfg || !iquv || !model || npix < 0) return GM_ERR_INVALID;
+  gm::DevCfg d;
+  gm_status st = build_devcfg(nullptr, *cfg, &d);
+  if (st != GM_OK) return st;
+  if (nl != d.nl) return GM_ERR_INVALID;
+  const bool global_slight = d.use_slight && !d.slight_per_pixel;
+  const size_t need = kNoallocSlightOffset + (global_slight ? sizeof(float) * 4 * (size_t)nl : 0);
+  if (need > GM_NOALLOC_SCRATCH_BYTES) return GM_ERR_INVALID;
+  if (d.use_slight && !cfg->slight) return GM_ERR_INVALID;
+  // every array the kernel touches must already be device memory
+  const void* dev_ptrs[] = {iquv, model, chi2, iters, fitted, status,
+                            (d.use_slight && d.slight_per_pixel) ? (const void*)cfg->slight : nullptr};
+  for (const void* p : dev_ptrs)
+    if (p && !is_device_ptr(p)) return GM_ERR_INVALID;
+  if (npix == 0) return GM_OK;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return GM_ERR_CUDA;
+  void* scratch = nullptr;
+  if ((st = noalloc_scratch(dev, &scratch)) != GM_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  // the counters must start at zero; the array keeps the previous call's values
+  cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(gm::WorkCounters), s);
+  if (e == cudaSuccess && global_slight) {
+    float* dst = (float*)((unsigned char*)scratch + kNoallocSlightOffset);
+    e = cudaMemcpyAsync(dst, cfg->slight, sizeof(float) * 4 * nl, cudaMemcpyDefault, s);
+    d.slight = dst;
+  } else if (d.use_slight) {
+    d.slight = cfg->slight;
+  }
+  if (e != cudaSuccess) return GM_ERR_CUDA;
+  gm::InvertArgs ia{};
+  ia.iquv = iquv;
+  ia.npix = npix;
+  ia.model = model;
+  ia.chi2 = chi2;
+  ia.iters = iters;
+  ia.fitted = fitted;
+  ia.status = status;
+  ia.work = (gm::WorkCounters*)scratch;
+  const int per_sm = std::max(1, gm::invert_blocks_per_sm(nl));
+  int64_t grid = (int64_t)per_sm * sms;
+  const int64_t needed = (npix + gm::kWarpsPerBlock - 1) / gm::kWarpsPerBlock;
+  if (grid > needed) grid = needed;
+  e = gm::launch_invert(d, ia, (int)grid, s);
+  return e == cudaSuccess ? GM_OK : GM_ERR_CUDA;
+}

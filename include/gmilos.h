@@ -148,6 +148,27 @@ gm_status gm_invert_ex(gm_ctx *ctx, const float *iquv, int64_t npix, int nl,
                        float *chi2, int *iters, int *accepted, float *fitted,
                        uint32_t *status, void *stream);
 
+/* Inversion for callers that cannot allocate device memory.  No counterpart
+ * in the reference.  Some callers cannot call cudaMalloc while they run: code
+ * inside a CUDA-graph capture or a real-time pipeline that must not block on
+ * the allocator, or a host framework that owns every device byte itself.
+ * This entry point allocates nothing: it takes the configuration directly
+ * (no gm_ctx) and only device pointers (inputs [P][4][nl], outputs as in
+ * gm_invert; fitted, chi2, iters, status may be NULL).  Its scratch -- the
+ * work-stealing counters and the global stray-light profile -- lives in one
+ * file-scope device array of GM_NOALLOC_SCRATCH_BYTES that every GPU loading
+ * the library keeps until the process exits; requests needing more are
+ * rejected with GM_ERR_INVALID.  The first call on a device looks up that
+ * array's address and loads the kernel; make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race, so serialise
+ * them (one stream, or events).  Errors are reported by status only:
+ * GM_ERR_INVALID (bad configuration, host pointer, or scratch over the
+ * maximum), GM_ERR_UNSUPPORTED, GM_ERR_CUDA. */
+#define GM_NOALLOC_SCRATCH_BYTES 4096
+gm_status gm_invert_noalloc(const gm_config *cfg, const float *iquv, int64_t npix, int nl,
+                            float *model, float *chi2, int *iters, float *fitted,
+                            uint32_t *status, void *stream);
+
 /* One Levenberg-Marquardt iteration from explicit per-pixel states
  * (models [P][11], damping flambda): the step delta [P][10] from the damped
  * normal equations, the trial model [P][11] after step limits and range
