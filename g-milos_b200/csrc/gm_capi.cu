@@ -376,15 +376,15 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   if (e != cudaSuccess) return cuda_fail(ctx, e, "work counter reset");
   const int per_sm = std::max(1, gm::invert_blocks_per_sm(nl));
   int64_t grid = (int64_t)per_sm * ctx->sms;
-  const int64_t needed = (npix + gm::kWarpsPerBlock - 1) / gm::kWarpsPerBlock;
+  const int64_t needed = (npix + gm::warps_for_nl(nl) - 1) / gm::warps_for_nl(nl);
   if (grid > needed) grid = needed;
   cudaEventRecord(ctx->ev0, s);
   e = gm::launch_invert(d, ia, (int)grid, s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "inversion kernel launch");
   cudaEventRecord(ctx->ev1, s);
   ctx->stats.grid_blocks = (int)grid;
-  ctx->stats.block_threads = gm::kWarpsPerBlock * 32;
-  ctx->stats.warps_per_block = gm::kWarpsPerBlock;
+  ctx->stats.block_threads = gm::warps_for_nl(nl) * 32;
+  ctx->stats.warps_per_block = gm::warps_for_nl(nl);
   ctx->stats.kernel_launches = 1;
   ctx->stats.pixels = npix;
   const Arg* outs[] = {&a_model, &a_m64, &a_chi, &a_it, &a_acc, &a_fit, &a_st,
@@ -729,7 +729,7 @@ extern "C" gm_status gm_invert_noalloc(const gm_config* cfg, const float* iquv, 
   ia.work = (gm::WorkCounters*)scratch;
   const int per_sm = std::max(1, gm::invert_blocks_per_sm(nl));
   int64_t grid = (int64_t)per_sm * sms;
-  const int64_t needed = (npix + gm::kWarpsPerBlock - 1) / gm::kWarpsPerBlock;
+  const int64_t needed = (npix + gm::warps_for_nl(nl) - 1) / gm::warps_for_nl(nl);
   if (grid > needed) grid = needed;
   e = gm::launch_invert(d, ia, (int)grid, s);
   return e == cudaSuccess ? GM_OK : GM_ERR_CUDA;

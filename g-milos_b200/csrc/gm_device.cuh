@@ -135,6 +135,13 @@ struct Lane {
   float lh[LPL][3], lf[LPL][3], lu[LPL][3];
 };
 
+// Rows staged for the PSF: Stokes s x RF slot {eta0, B, vlos, dopp, damping,
+// gamma, azimuth, S1} (S0's RF is constant, alpha's is never convolved).
+constexpr int kRows = 32;
+__host__ __device__ constexpr int rf_row(int s, int t) { return s * 8 + (t == 8 ? 7 : t); }
+template <int LPL>
+__host__ __device__ constexpr int row_off() { return 16 * LPL; }   // samples at [16 LPL, 48 LPL)
+
 // Warp-private shared memory.
 template <int LPL>
 struct WarpSmem {
@@ -146,8 +153,12 @@ struct WarpSmem {
   float vec[12];
   float cs[18][5], sn[18][5];
   float red[96];
-  float stg[96 * LPL];   // zero-padded PSF staging row
+  float ic[kRows];       // continuum about which each staged I row is reflected
+  float rows[kRows][64 * LPL];   // zero-padded rows for the PSF
 };
+
+template <int LPL>
+__host__ __device__ constexpr int warps_per_block() { return LPL == 1 ? 4 : 2; }
 
 // Rotation pairs of the parallel Jacobi: lane b < 5 owns diagonal block
 // (b, b); lanes 5..14 own the off-diagonal blocks (p, q), p < q.
@@ -163,17 +174,14 @@ __device__ __forceinline__ int rr_perm(int i) {
 }
 
 // --------------------------------------------------------------- PSF
-// Same-size correlation of one row (LPL samples per lane) with the nl-tap
-// PSF centred at nl/2, zero padded; with use_ic the row is reflected about
-// max(first, last) before and after (direct_convolution{,_ic},
-// convolution.cu:153-241).  stg is this warp's staging row: samples live at
-// [32*LPL, 64*LPL), the rest stays zero.
+// Stage one row (LPL samples per lane) in shared memory; I rows are
+// reflected about their continuum max(first, last) (direct_convolution_ic,
+// convolution.cu:200-241).
 template <int LPL>
-__device__ __forceinline__ void psf_row(float (&x)[LPL], float* stg, const DevCfg& c,
-                                        int lane, bool use_ic) {
-  const int nl = c.nl;
+__device__ __forceinline__ void put_row(WarpSmem<LPL>& sm, int r, const float (&x)[LPL], int nl,
+                                        int lane, bool reflect) {
   float ic = 0.f;
-  if (use_ic) {
+  if (reflect) {
     const float first = __shfl_sync(kFull, x[0], 0);
     const int kl = (nl - 1) >> 5, ll = (nl - 1) & 31;
     float lastv = x[0];
@@ -182,28 +190,50 @@ __device__ __forceinline__ void psf_row(float (&x)[LPL], float* stg, const DevCf
       if (k == kl) lastv = x[k];
     const float last = __shfl_sync(kFull, lastv, ll);
     ic = first > last ? first : last;
+    if (lane == 0) sm.ic[r] = ic;
   }
-  __syncwarp();
 #pragma unroll
   for (int k = 0; k < LPL; ++k) {
     const int l = lane + 32 * k;
-    stg[32 * LPL + l] = (l < nl) ? (use_ic ? ic - x[k] : x[k]) : 0.f;
+    sm.rows[r][row_off<LPL>() + l] = (l < nl) ? (reflect ? ic - x[k] : x[k]) : 0.f;
+  }
+}
+
+// In-place same-size correlation of the staged rows in `mask` with the
+// nl-tap PSF centred at nl/2, zero padded, two partial sums over even and
+// odd taps (direct_convolution{,_ic}, convolution.cu:153-241); rows in
+// `reflect` are reflected back about sm.ic.  The caller syncs the warp after
+// staging.  One loop over rows keeps the code small whatever the row count.
+template <int LPL>
+__device__ __forceinline__ void psf_rows(WarpSmem<LPL>& sm, const DevCfg& c, uint32_t mask,
+                                         uint32_t reflect, int lane) {
+  const int nl = c.nl, half = nl >> 1;
+  while (mask) {
+    const int r = __ffs(mask) - 1;
+    mask &= mask - 1;
+    float out[LPL];
+#pragma unroll
+    for (int k = 0; k < LPL; ++k) {
+      const float* base = sm.rows[r] + row_off<LPL>() + lane + 32 * k - half;
+      float a0 = 0.f, a1 = 0.f;
+      int j = 0;
+      for (; j + 1 < nl; j += 2) {
+        a0 = fmaf(c.psf[j], base[j], a0);
+        a1 = fmaf(c.psf[j + 1], base[j + 1], a1);
+      }
+      if (j < nl) a0 = fmaf(c.psf[j], base[j], a0);
+      out[k] = a0 + a1;
+    }
+    __syncwarp();
+    const bool refl = (reflect >> r) & 1u;
+    const float ic = refl ? sm.ic[r] : 0.f;
+#pragma unroll
+    for (int k = 0; k < LPL; ++k) {
+      const int l = lane + 32 * k;
+      sm.rows[r][row_off<LPL>() + l] = (l < nl) ? (refl ? ic - out[k] : out[k]) : 0.f;
+    }
   }
   __syncwarp();
-  const int half = nl >> 1;
-#pragma unroll
-  for (int k = 0; k < LPL; ++k) {
-    const float* base = stg + 32 * LPL + lane + 32 * k - half;
-    float a0 = 0.f, a1 = 0.f;
-    int j = 0;
-    for (; j + 1 < nl; j += 2) {
-      a0 = fmaf(c.psf[j], base[j], a0);
-      a1 = fmaf(c.psf[j + 1], base[j + 1], a1);
-    }
-    if (j < nl) a0 = fmaf(c.psf[j], base[j], a0);
-    const float r = a0 + a1;
-    x[k] = use_ic ? ic - r : r;
-  }
 }
 
 // --------------------------------------------------------------- synthesis
@@ -214,7 +244,7 @@ template <int LPL>
 __device__ __forceinline__ void synth_lane(const DevCfg& c, const double* m, const float (&dlv)[LPL],
                                            int lane, Lane<LPL>& st, Angles& an,
                                            float (&spec)[LPL][4], float (&pure)[LPL][4],
-                                           const float (&sl)[LPL][4], float* stg) {
+                                           const float (&sl)[LPL][4], WarpSmem<LPL>& sm) {
   const float CC = (float)(kPi / 180.0), CC2 = (float)((kPi / 180.0) * 2);
   const double azi = m[AZ] * (double)CC, gmr = m[GM] * (double)CC;
   float sgm, cgm;
@@ -297,15 +327,21 @@ __device__ __forceinline__ void synth_lane(const DevCfg& c, const double* m, con
   }
 
   if (c.use_psf) {
+    __syncwarp();
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
       float row[LPL];
 #pragma unroll
       for (int k = 0; k < LPL; ++k) row[k] = spec[k][s];
-      psf_row<LPL>(row, stg, c, lane, s == 0);
-#pragma unroll
-      for (int k = 0; k < LPL; ++k) spec[k][s] = row[k];
+      put_row<LPL>(sm, s, row, c.nl, lane, s == 0);
     }
+    __syncwarp();
+    psf_rows<LPL>(sm, c, 0xfu, 0x1u, lane);
+#pragma unroll
+    for (int k = 0; k < LPL; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) spec[k][s] = sm.rows[s][row_off<LPL>() + lane + 32 * k];
+    __syncwarp();
   }
 #pragma unroll
   for (int k = 0; k < LPL; ++k)
@@ -322,18 +358,31 @@ __device__ __forceinline__ void synth_lane(const DevCfg& c, const double* m, con
 }
 
 // --------------------------------------------------------------- response functions
+// Staged rows of the free response functions that go through the PSF: every
+// free parameter but S0 (the azimuth RF of I and V is identically zero).
+__device__ __forceinline__ uint32_t rf_row_mask(const DevCfg& c) {
+  uint32_t mk = 0;
+#pragma unroll
+  for (int t = 0; t < 9; ++t) {
+    if (t == 7 || !c.fix[t]) continue;
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+      if (!(t == 6 && (s == 0 || s == 3))) mk |= 1u << rf_row(s, t);
+  }
+  return mk;
+}
+
 // Analytic derivatives of the last synthesis (me_der.cu:81-376): profile
 // derivatives of each group's last component (d_funcionComponentFor
 // :53-77), their Zeeman combination and the RTE derivative (me_der_kernel
-// :218-376), PSF of every free RF except S0's, stray-light scaling
-// (:191-211).  Rows of fixed parameters are left zero
-// (FijaACeroDerivadasNoNecesarias, milosUtils.cu:243-271).  J[k][s][t]:
-// sample k, Stokes s, parameter slot t (10-term layout: slot 9 = alpha).
+// :218-376), then the PSF of every free RF except S0's (:162-189), I rows
+// reflected about max(first, last).  The results stay in the staged rows
+// of sm (rf_row); gather_rf adds S0, alpha, the stray-light scaling
+// (:191-211) and the zeros of fixed parameters
+// (FijaACeroDerivadasNoNecesarias, milosUtils.cu:243-271).
 template <int LPL>
-__device__ __forceinline__ void rf_lane(const DevCfg& c, const double* m, const Lane<LPL>& st,
-                                        const Angles& an, const float (&asrc)[LPL][4],
-                                        const float (&sl)[LPL][4], int lane, float* stg,
-                                        float (&J)[LPL][4][10]) {
+__device__ __forceinline__ void rf_rows(const DevCfg& c, const double* m, const Lane<LPL>& st,
+                                        const Angles& an, int lane, WarpSmem<LPL>& sm) {
   const float auxCte = __fdividef((float)(-c.lambda0), (float)(kVlight * m[DOPP]));
   const double aa = m[AA], dopp = m[DOPP];
   // last component of each group: its scaled splitting and strength
@@ -347,7 +396,6 @@ __device__ __forceinline__ void rf_lane(const DevCfg& c, const double* m, const 
   wel[2] = c.wer[c.n_sig - 1];
 
   const float E0f = (float)(m[ETA0] * (double)c.fo);
-  const float E0d = (float)(m[ETA0] * (double)c.fo);
   const double E0dd = m[ETA0] * (double)c.fo;
   const float sc = __fdividef(E0f * (an.sinis * an.cosa), 2.f);
   const float ss = __fdividef(E0f * (an.sinis * an.sina), 2.f);
@@ -360,12 +408,14 @@ __device__ __forceinline__ void rf_lane(const DevCfg& c, const double* m, const 
   const float cosi_cosdi = an.cosi * an.cosdi * E0_2, sindi_E0_2 = an.sindi * E0_2;
   const float sinis_cosda = an.sinis * an.cosda, sinis_sinda = an.sinis * an.sinda;
   const float sinis_cosa = an.sinis * an.cosa, sinis_sina = an.sinis * an.sina;
-  const float E0s_2 = __fdividef((float)(m[ETA0] * (double)c.fo), 2.f);
   const float s1mu_f = (float)(-(m[S1] * (double)c.mu));
   const float muf = c.mu;
+  const uint32_t mask = rf_row_mask(c);
+  const int nl = c.nl;
 
 #pragma unroll
   for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
     float dfi[3][4], dshi[3][4];
 #pragma unroll
     for (int g = 0; g < 3; ++g) {
@@ -387,11 +437,11 @@ __device__ __forceinline__ void rf_lane(const DevCfg& c, const double* m, const 
     const float fp = st.fi[k][0], fb = st.fi[k][1], fr = st.fi[k][2];
     const float sp = st.shi[k][0], sb = st.shi[k][1], sr = st.shi[k][2];
     const float p1 = fb + fr;
-    const float p2 = E0s_2 * (fp - __fdividef(p1, 2.f));
-    const float p3 = E0s_2 * (sp - __fdividef(sb + sr, 2.f));
-    const float ein = E0s_2 * (fp * an.sinis + p1 * an.cosis_2);
-    const float eq = p2 * sinis_cosa, eu = p2 * sinis_sina, ev = (fr - fb) * (E0s_2 * an.cosi);
-    const float rq = p3 * sinis_cosa, ru = p3 * sinis_sina, rv = (sr - sb) * (E0s_2 * an.cosi);
+    const float p2 = E0_2 * (fp - __fdividef(p1, 2.f));
+    const float p3 = E0_2 * (sp - __fdividef(sb + sr, 2.f));
+    const float ein = E0_2 * (fp * an.sinis + p1 * an.cosis_2);
+    const float eq = p2 * sinis_cosa, eu = p2 * sinis_sina, ev = (fr - fb) * (E0_2 * an.cosi);
+    const float rq = p3 * sinis_cosa, ru = p3 * sinis_sina, rv = (sr - sb) * (E0_2 * an.cosi);
     const float ei = 1.f + ein;
     const float ei2 = ei * ei;
     const float gp1 = ei2 - eq * eq - eu * eu - ev * ev + rq * rq + ru * ru + rv * rv;
@@ -401,40 +451,6 @@ __device__ __forceinline__ void rf_lane(const DevCfg& c, const double* m, const 
     const float g4 = (ei2 * eq + ei * (ev * ru - eu * rv)) + rq * gp2;
     const float g5 = (ei2 * eu + ei * (eq * rv - ev * rq)) + ru * gp2;
     const float g6 = (ei2 * ev + ei * (eu * rq - eq * ru)) + rv * gp2;
-
-    float de[7], dq[7], du[7], dv[7], drq[7], dru[7], drv[7];
-    de[0] = (float)((double)ein / E0dd);
-    dq[0] = __fdividef(eq, E0d); du[0] = __fdividef(eu, E0d); dv[0] = __fdividef(ev, E0d);
-    drq[0] = __fdividef(rq, E0d); dru[0] = __fdividef(ru, E0d); drv[0] = __fdividef(rv, E0d);
-#pragma unroll
-    for (int j = 1; j < 5; ++j) {
-      const float dsum = dfi[1][j - 1] + dfi[2][j - 1];
-      de[j] = dfi[0][j - 1] * sinis_E0_2 + dsum * cosis_2_E0_2;
-      const float aux = dfi[0][j - 1] - __fdividef(dsum, 2.f);
-      dq[j] = aux * sc;
-      du[j] = aux * ss;
-      dv[j] = (dfi[2][j - 1] - dfi[1][j - 1]) * cosi_2_E0;
-      const float s1 = dshi[1][j - 1], s2 = dshi[2][j - 1];
-      const float aux2 = dshi[0][j - 1] - __fdividef(s1 + s2, 2.f);
-      drq[j] = aux2 * sc;
-      dru[j] = aux2 * ss;
-      drv[j] = (s2 - s1) * cosi_2_E0;
-    }
-    de[5] = fp * sindi_E0_2 + p1 * cosi_cosdi;
-    dq[5] = p2 * sindi_cosa;
-    du[5] = p2 * sindi_sina;
-    dv[5] = (fr - fb) * cosdi_E0_2;
-    drq[5] = p3 * sindi_cosa;
-    dru[5] = p3 * sindi_sina;
-    drv[5] = (sr - sb) * cosdi_E0_2;
-    de[6] = 0.f;
-    dv[6] = 0.f;
-    drv[6] = 0.f;
-    dq[6] = p2 * sinis_cosda;
-    du[6] = p2 * sinis_sinda;
-    drq[6] = p3 * sinis_cosda;
-    dru[6] = p3 * sinis_sinda;
-
     const float dtaux = __fdividef(s1mu_f, dt * dt);
     const float eigp3 = ei * gp3;
     const float a2 = 2.f * ei;
@@ -442,103 +458,155 @@ __device__ __forceinline__ void rf_lane(const DevCfg& c, const double* m, const 
     const float ext2 = a2 * eu + eq * rv - ev * rq;
     const float ext3 = a2 * ev + eu * rq - eq * ru;
     const float ext4 = a2 * gp1;
+
 #pragma unroll
-    for (int il = 0; il < 7; ++il) {
-      const float dgp1 = 2.f * (ei * de[il] - eq * dq[il] - eu * du[il] - ev * dv[il] +
-                               rq * drq[il] + ru * dru[il] + rv * drv[il]);
-      const float dgp2 = rq * dq[il] + eq * drq[il] + ru * du[il] + eu * dru[il] +
-                         rv * dv[il] + ev * drv[il];
-      const float ddt = ext4 * de[il] + ei2 * dgp1 - 2.f * gp2 * dgp2;
-      const float dgp3 = 2.f * (ei * de[il] + rq * drq[il] + ru * dru[il] + rv * drv[il]);
-      const float dgp4 = de[il] * ext1 + ei2 * dq[il] +
-                         ei * (ru * dv[il] + ev * dru[il] - rv * du[il] - eu * drv[il]);
-      const float dgp5 = de[il] * ext2 + ei2 * du[il] +
-                         ei * (rv * dq[il] + eq * drv[il] - rq * dv[il] - ev * drq[il]);
-      const float dgp6 = de[il] * ext3 + ei2 * dv[il] +
-                         ei * (rq * du[il] + eu * drq[il] - ru * dq[il] - eq * dru[il]);
-      J[k][0][il] = -(((de[il] * gp3 + ei * dgp3) * dt - ddt * eigp3) * dtaux);
-      J[k][1][il] = ((dgp4 + drq[il] * gp2 + rq * dgp2) * dt - ddt * g4) * dtaux;
-      J[k][2][il] = ((dgp5 + dru[il] * gp2 + ru * dgp2) * dt - ddt * g5) * dtaux;
-      J[k][3][il] = ((dgp6 + drv[il] * gp2 + rv * dgp2) * dt - ddt * g6) * dtaux;
+    for (int il = 0; il < 9; ++il) {
+      if (il == 7) continue;
+      float de = 0.f, dq = 0.f, du = 0.f, dv = 0.f, drq = 0.f, dru = 0.f, drv = 0.f;
+      if (il == 0) {
+        de = (float)((double)ein / E0dd);
+        dq = __fdividef(eq, (float)E0dd);
+        du = __fdividef(eu, (float)E0dd);
+        dv = __fdividef(ev, (float)E0dd);
+        drq = __fdividef(rq, (float)E0dd);
+        dru = __fdividef(ru, (float)E0dd);
+        drv = __fdividef(rv, (float)E0dd);
+      } else if (il < 5) {
+        const int j = il - 1;
+        const float dsum = dfi[1][j] + dfi[2][j];
+        de = dfi[0][j] * sinis_E0_2 + dsum * cosis_2_E0_2;
+        const float aux = dfi[0][j] - __fdividef(dsum, 2.f);
+        dq = aux * sc;
+        du = aux * ss;
+        dv = (dfi[2][j] - dfi[1][j]) * cosi_2_E0;
+        const float s1 = dshi[1][j], s2 = dshi[2][j];
+        const float aux2 = dshi[0][j] - __fdividef(s1 + s2, 2.f);
+        drq = aux2 * sc;
+        dru = aux2 * ss;
+        drv = (s2 - s1) * cosi_2_E0;
+      } else if (il == 5) {
+        de = fp * sindi_E0_2 + p1 * cosi_cosdi;
+        dq = p2 * sindi_cosa;
+        du = p2 * sindi_sina;
+        dv = (fr - fb) * cosdi_E0_2;
+        drq = p3 * sindi_cosa;
+        dru = p3 * sindi_sina;
+        drv = (sr - sb) * cosdi_E0_2;
+      } else if (il == 6) {
+        dq = p2 * sinis_cosda;
+        du = p2 * sinis_sinda;
+        drq = p3 * sinis_cosda;
+        dru = p3 * sinis_sinda;
+      }
+      float o[4];
+      if (il == 8) {   // source-function gradient
+        const float dti = -(__fdividef(1.f, dt) * muf);
+        o[0] = -dti * eigp3;
+        o[1] = dti * g4;
+        o[2] = dti * g5;
+        o[3] = dti * g6;
+      } else {
+        const float dgp1 = 2.f * (ei * de - eq * dq - eu * du - ev * dv + rq * drq + ru * dru + rv * drv);
+        const float dgp2 = rq * dq + eq * drq + ru * du + eu * dru + rv * dv + ev * drv;
+        const float ddt = ext4 * de + ei2 * dgp1 - 2.f * gp2 * dgp2;
+        const float dgp3 = 2.f * (ei * de + rq * drq + ru * dru + rv * drv);
+        const float dgp4 = de * ext1 + ei2 * dq + ei * (ru * dv + ev * dru - rv * du - eu * drv);
+        const float dgp5 = de * ext2 + ei2 * du + ei * (rv * dq + eq * drv - rq * dv - ev * drq);
+        const float dgp6 = de * ext3 + ei2 * dv + ei * (rq * du + eu * drq - ru * dq - eq * dru);
+        o[0] = -(((de * gp3 + ei * dgp3) * dt - ddt * eigp3) * dtaux);
+        o[1] = ((dgp4 + drq * gp2 + rq * dgp2) * dt - ddt * g4) * dtaux;
+        o[2] = ((dgp5 + dru * gp2 + ru * dgp2) * dt - ddt * g5) * dtaux;
+        o[3] = ((dgp6 + drv * gp2 + rv * dgp2) * dt - ddt * g6) * dtaux;
+      }
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const int r = rf_row(s, il);
+        if ((mask >> r) & 1u) sm.rows[r][row_off<LPL>() + l] = (l < nl) ? o[s] : 0.f;
+      }
     }
-    const float dti = -(__fdividef(1.f, dt) * muf);
-    J[k][0][8] = -dti * eigp3;
-    J[k][1][8] = dti * g4;
-    J[k][2][8] = dti * g5;
-    J[k][3][8] = dti * g6;
-    J[k][0][7] = 1.f;
-    J[k][1][7] = 0.f;
-    J[k][2][7] = 0.f;
-    J[k][3][7] = 0.f;
-    J[k][0][6] = 0.f;
-    J[k][3][6] = 0.f;
-#pragma unroll
-    for (int s = 0; s < 4; ++s) J[k][s][9] = 0.f;
   }
+  __syncwarp();
 
   if (c.use_psf) {
+    // reflect the I rows about max(first, last) (me_der.cu:167-176)
+    uint32_t refl = 0;
+    float icv[8];
 #pragma unroll
-    for (int t = 0; t < 9; ++t) {
-      if (t == 7 || !c.fix[t]) continue;
+    for (int tt = 0; tt < 8; ++tt) {
+      const int r = rf_row(0, tt == 7 ? 8 : tt);
+      icv[tt] = 0.f;
+      if (!((mask >> r) & 1u)) continue;
+      refl |= 1u << r;
+      const float f0 = sm.rows[r][row_off<LPL>()];
+      const float f1 = sm.rows[r][row_off<LPL>() + nl - 1];
+      icv[tt] = f0 > f1 ? f0 : f1;
+      if (lane == 0) sm.ic[r] = icv[tt];
+    }
+    __syncwarp();   // every lane has read the end samples before any is overwritten
 #pragma unroll
-      for (int s = 0; s < 4; ++s) {
-        float row[LPL];
+    for (int tt = 0; tt < 8; ++tt) {
+      const int r = rf_row(0, tt == 7 ? 8 : tt);
+      if (!((refl >> r) & 1u)) continue;
 #pragma unroll
-        for (int k = 0; k < LPL; ++k) row[k] = J[k][s][t];
-        psf_row<LPL>(row, stg, c, lane, s == 0);
-#pragma unroll
-        for (int k = 0; k < LPL; ++k) J[k][s][t] = row[k];
+      for (int k = 0; k < LPL; ++k) {
+        const int l = lane + 32 * k;
+        if (l < nl) sm.rows[r][row_off<LPL>() + l] = icv[tt] - sm.rows[r][row_off<LPL>() + l];
       }
     }
+    __syncwarp();
+    psf_rows<LPL>(sm, c, mask, refl, lane);
   }
-  if (c.use_slight) {
-    const double a = m[ALFA];
-#pragma unroll
-    for (int k = 0; k < LPL; ++k)
-#pragma unroll
-      for (int s = 0; s < 4; ++s) {
-#pragma unroll
-        for (int t = 0; t < 9; ++t) J[k][s][t] = (float)((double)J[k][s][t] * a);
-        J[k][s][9] = asrc[k][s] - sl[k][s];
-      }
-  }
-#pragma unroll
-  for (int t = 0; t < 10; ++t) {
-    const int key = (t == 9) ? 10 : t;
-    if (!c.fix[key]) {
-#pragma unroll
-      for (int k = 0; k < LPL; ++k)
-#pragma unroll
-        for (int s = 0; s < 4; ++s) J[k][s][t] = 0.f;
-    }
-  }
+}
+
+// Response function of sample l, Stokes s, slot t in the reference's
+// 10-term layout (slot 7 = S0, slot 9 = alpha) after the PSF: stray-light
+// scaling, alpha's RF from the unscaled profile, zero for fixed parameters.
+template <int LPL>
+__device__ __forceinline__ float gather_rf(const DevCfg& c, const WarpSmem<LPL>& sm, double alfa,
+                                           float asrc, float sl, int l, int s, int t) {
+  const int key = (t == 9) ? 10 : t;
+  if (!c.fix[key]) return 0.f;
+  if (t == 9) return c.use_slight ? asrc - sl : 0.f;
+  float v;
+  if (t == 7) v = (s == 0) ? 1.f : 0.f;
+  else if (t == 6 && (s == 0 || s == 3)) v = 0.f;
+  else v = sm.rows[rf_row(s, t)][row_off<LPL>() + l];
+  if (c.use_slight) v = (float)((double)v * alfa);
+  return v;
 }
 
 // packed index of (i <= h) in the upper triangle of a 10x10 matrix
 __host__ __device__ constexpr int upk(int i, int h) { return i * 10 - (i * (i - 1)) / 2 + (h - i); }
 
 // Normal equations alpha = sum_s w_s/sigma^2 J^T J and beta = sum_s w_s J^T
-// (syn - obs) / sigma^2 (covarmf, lib.cu:65-118) reduced across the warp;
-// results land in sm.alpha (packed) and sm.beta.
+// (syn - obs) / sigma^2 (covarmf, lib.cu:65-118) from the staged response
+// functions, reduced across the warp; results land in sm.alpha (packed) and
+// sm.beta.
 template <int LPL>
-__device__ __forceinline__ void normal_eq(const DevCfg& c, const float (&J)[LPL][4][10],
+__device__ __forceinline__ void normal_eq(const DevCfg& c, const double* m,
+                                          const float (&asrc)[LPL][4], const float (&sl)[LPL][4],
                                           const float (&syn)[LPL][4], const float (&ob)[LPL][4],
                                           const bool (&valid)[LPL], int lane, WarpSmem<LPL>& sm) {
   float v[96];
 #pragma unroll
   for (int i = 0; i < 96; ++i) v[i] = 0.f;
+  const double alfa = m[ALFA];
 #pragma unroll
   for (int k = 0; k < LPL; ++k) {
     if (!valid[k]) continue;
+    const int l = lane + 32 * k;
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
+      float J[10];
+#pragma unroll
+      for (int t = 0; t < 10; ++t) J[t] = gather_rf<LPL>(c, sm, alfa, asrc[k][s], sl[k][s], l, s, t);
       const float wd = c.wsig[s];
       const float r = c.weight[s] * (syn[k][s] - ob[k][s]);
 #pragma unroll
       for (int i = 0; i < 10; ++i) {
-        const float ji = J[k][s][i];
+        const float ji = J[i];
 #pragma unroll
-        for (int h = i; h < 10; ++h) v[upk(i, h)] = fmaf(wd * ji, J[k][s][h], v[upk(i, h)]);
+        for (int h = i; h < 10; ++h) v[upk(i, h)] = fmaf(wd * ji, J[h], v[upk(i, h)]);
         v[55 + i] = fmaf(r, ji, v[55 + i]);
       }
     }

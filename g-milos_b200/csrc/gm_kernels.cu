@@ -15,16 +15,25 @@ __device__ __forceinline__ void load_pixel(const float* __restrict__ p, int nl, 
   }
 }
 
+template <int LPL>
+__device__ __forceinline__ void zero_padding(WarpSmem<LPL>& sm, int lane) {
+  for (int i = lane; i < kRows * 64 * LPL; i += 32) (&sm.rows[0][0])[i] = 0.f;
+  __syncwarp();
+}
+
 // One warp per pixel, pixels taken from a global cursor until the cube is
 // done (lm_mils, milosUtils.cu:574-710, with its per-thread contiguous pixel
-// slice replaced by work stealing).
+// slice replaced by work stealing).  The initial point is handled as an
+// accepted step of the same loop, so the synthesis and the response
+// functions each appear once in the code.
 template <int LPL>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+__global__ void __launch_bounds__(warps_per_block<LPL>() * 32)
 invert_kernel(const DevCfg c, const InvertArgs a) {
-  __shared__ WarpSmem<LPL> smem[kWarpsPerBlock];
+  constexpr int WPB = warps_per_block<LPL>();
+  __shared__ WarpSmem<LPL> smem[WPB];
   const int lane = threadIdx.x & 31;
   WarpSmem<LPL>& sm = smem[threadIdx.x >> 5];
-  for (int i = lane; i < 96 * LPL; i += 32) sm.stg[i] = 0.f;
+  zero_padding<LPL>(sm, lane);
 
   const int nl = c.nl;
   float dlv[LPL];
@@ -45,7 +54,6 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
 #pragma unroll
       for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
   }
-  __syncwarp();
 
   unsigned long long my_iter = 0, my_acc = 0;
   while (true) {
@@ -60,10 +68,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
     if (c.use_slight && c.slight_per_pixel) load_pixel<LPL>(c.slight + off, nl, lane, slg);
 
     // initial model
-    if (lane < 11) {
-      const double v = a.init_models ? a.init_models[pix * 11 + lane] : c.init[lane];
-      sm.m[lane] = v;
-    }
+    if (lane < 11) sm.m[lane] = a.init_models ? a.init_models[pix * 11 + lane] : c.init[lane];
     __syncwarp();
     uint32_t st = 0;
     if (c.init_mode == 0) st |= classical_warp<LPL>(c, ob, dld, valid, lane, sm.m);
@@ -72,54 +77,64 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
     Lane<LPL> ln;
     Angles an;
     float syn[LPL][4], pure[LPL][4];
-    float J[LPL][4][10];
-    synth_lane<LPL>(c, sm.m, dlv, lane, ln, an, syn, pure, slg, sm.stg);
-    rf_lane<LPL>(c, sm.m, ln, an, pure, slg, lane, sm.stg, J);
-    normal_eq<LPL>(c, J, syn, ob, valid, lane, sm);
-    float ochisqr = chisq<LPL>(c, syn, ob, valid);
-    const float chisqr0 = ochisqr;
-    if (lane < 11) sm.t[lane] = sm.m[lane];
-    __syncwarp();
-
-    float flambda = c.ilambda, pbf = 1.f;
+    float flambda = c.ilambda, pbf = 1.f, ochisqr = 0.f, chisqr0 = 0.f;
     int iter = 0, acc = 0;
-    bool stop = false;
-    do {
-      solve10<LPL>(sm, flambda, lane, c.numerics != 0);
-      if (lane == 0) apply_delta_check(c, sm.m, sm.vec, sm.t);
-      __syncwarp();
-      synth_lane<LPL>(c, sm.t, dlv, lane, ln, an, syn, pure, slg, sm.stg);
-      const float chisqr = chisq<LPL>(c, syn, ob, valid);
-      if (iter == 0) {
-        if (a.step_delta && lane < 10) a.step_delta[pix * 10 + lane] = sm.vec[lane];
-        if (a.step_trial && lane < 11) a.step_trial[pix * 11 + lane] = sm.t[lane];
-        if (lane == 0 && a.step_chi2_start) a.step_chi2_start[pix] = chisqr0;
-        if (lane == 0 && a.step_chi2_trial) a.step_chi2_trial[pix] = chisqr;
-      }
-      if ((double)fabsf(((ochisqr) - (chisqr)) * 100 / (chisqr)) < c.toplim || (chisqr) < 0.0001f) {
-        stop = true;
-        st |= GM_PIX_CHI2_EXIT;
-      }
-      if ((chisqr) - (ochisqr) < 0.f) {
-        flambda = flambda / (5.f * pbf);
-        if (lane < 11) sm.m[lane] = sm.t[lane];
+    bool stop = false, first = true;
+    while (true) {
+      if (!first) {
+        solve10<LPL>(sm, flambda, lane, c.numerics != 0);
+        if (lane == 0) apply_delta_check(c, sm.m, sm.vec, sm.t);
         __syncwarp();
-        if (c.quirks) rf_lane<LPL>(c, sm.m, ln, an, syn, slg, lane, sm.stg, J);
-        else rf_lane<LPL>(c, sm.m, ln, an, pure, slg, lane, sm.stg, J);
-        normal_eq<LPL>(c, J, syn, ob, valid, lane, sm);
-        if (c.stop_dchi2 > 0.0 && (double)(ochisqr - chisqr) < c.stop_dchi2) stop = true;
+      }
+      synth_lane<LPL>(c, first ? sm.m : sm.t, dlv, lane, ln, an, syn, pure, slg, sm);
+      const float chisqr = chisq<LPL>(c, syn, ob, valid);
+      bool accept = first;
+      if (!first) {
+        if (iter == 0) {
+          if (a.step_delta && lane < 10) a.step_delta[pix * 10 + lane] = sm.vec[lane];
+          if (a.step_trial && lane < 11) a.step_trial[pix * 11 + lane] = sm.t[lane];
+          if (lane == 0 && a.step_chi2_start) a.step_chi2_start[pix] = chisqr0;
+          if (lane == 0 && a.step_chi2_trial) a.step_chi2_trial[pix] = chisqr;
+        }
+        // stop rules and damping schedule (milosUtils.cu:667-696)
+        if ((double)fabsf(((ochisqr) - (chisqr)) * 100 / (chisqr)) < c.toplim || (chisqr) < 0.0001f) {
+          stop = true;
+          st |= GM_PIX_CHI2_EXIT;
+        }
+        accept = (chisqr) - (ochisqr) < 0.f;
+        if (accept) {
+          flambda = flambda / (5.f * pbf);
+          if (c.stop_dchi2 > 0.0 && (double)(ochisqr - chisqr) < c.stop_dchi2) stop = true;
+          if (lane < 11) sm.m[lane] = sm.t[lane];
+          __syncwarp();
+          ++acc;
+        } else {
+          flambda = flambda * 10.f * pbf;
+        }
+        if (flambda > 1e+7f || flambda < 1e-25f) {
+          stop = true;
+          st |= GM_PIX_LAMBDA_EXIT;
+        }
+        ++iter;
+        if (c.logclambda) pbf = log10f(chisqr) / log10f(chisqr0);
+      }
+      if (accept) {
+        // response functions and normal equations at the accepted model; the
+        // alpha RF uses the mixed profile after the first step (milosUtils.cu:675)
+        rf_rows<LPL>(c, sm.m, ln, an, lane, sm);
+        if (first || !c.quirks) normal_eq<LPL>(c, sm.m, pure, slg, syn, ob, valid, lane, sm);
+        else normal_eq<LPL>(c, sm.m, syn, slg, syn, ob, valid, lane, sm);
         ochisqr = chisqr;
-        ++acc;
-      } else {
-        flambda = flambda * 10.f * pbf;
       }
-      if (flambda > 1e+7f || flambda < 1e-25f) {
-        stop = true;
-        st |= GM_PIX_LAMBDA_EXIT;
+      if (first) {
+        chisqr0 = ochisqr;
+        if (lane < 11) sm.t[lane] = sm.m[lane];
+        __syncwarp();
+        first = false;
+        continue;
       }
-      ++iter;
-      if (c.logclambda) pbf = log10f(chisqr) / log10f(chisqr0);
-    } while (iter < c.miter && !stop);
+      if (iter >= c.miter || stop) break;
+    }
     if (!stop) st |= GM_PIX_MAXITER;
     if (!isfinite(ochisqr)) st |= GM_PIX_NONFINITE;
 
@@ -156,12 +171,13 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
 // Synthesis (+ response functions) of one model per warp
 // (kernel_synthesis, gmilos.cu:71-84, batched).
 template <int LPL>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+__global__ void __launch_bounds__(warps_per_block<LPL>() * 32)
 synth_kernel(const DevCfg c, const SynthArgs a) {
-  __shared__ WarpSmem<LPL> smem[kWarpsPerBlock];
+  constexpr int WPB = warps_per_block<LPL>();
+  __shared__ WarpSmem<LPL> smem[WPB];
   const int lane = threadIdx.x & 31;
   WarpSmem<LPL>& sm = smem[threadIdx.x >> 5];
-  for (int i = lane; i < 96 * LPL; i += 32) sm.stg[i] = 0.f;
+  zero_padding<LPL>(sm, lane);
   const int nl = c.nl, nt = c.nterms;
   float dlv[LPL];
 #pragma unroll
@@ -177,9 +193,8 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
 #pragma unroll
       for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
   }
-  __syncwarp();
-  const int64_t wid = (int64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
-  const int64_t nw = (int64_t)gridDim.x * kWarpsPerBlock;
+  const int64_t wid = (int64_t)blockIdx.x * WPB + (threadIdx.x >> 5);
+  const int64_t nw = (int64_t)gridDim.x * WPB;
   for (int64_t pix = wid; pix < a.npix; pix += nw) {
     const size_t off = (size_t)pix * 4 * nl;
     if (c.use_slight && c.slight_per_pixel) load_pixel<LPL>(c.slight + off, nl, lane, slg);
@@ -188,7 +203,7 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
     Lane<LPL> ln;
     Angles an;
     float syn[LPL][4], pure[LPL][4];
-    synth_lane<LPL>(c, sm.m, dlv, lane, ln, an, syn, pure, slg, sm.stg);
+    synth_lane<LPL>(c, sm.m, dlv, lane, ln, an, syn, pure, slg, sm);
 #pragma unroll
     for (int k = 0; k < LPL; ++k) {
       const int l = lane + 32 * k;
@@ -197,8 +212,7 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
         for (int s = 0; s < 4; ++s) a.iquv[off + s * nl + l] = syn[k][s];
     }
     if (a.rf) {
-      float J[LPL][4][10];
-      rf_lane<LPL>(c, sm.m, ln, an, pure, slg, lane, sm.stg, J);
+      rf_rows<LPL>(c, sm.m, ln, an, lane, sm);
       const size_t roff = (size_t)pix * 4 * nt * nl;
 #pragma unroll
       for (int k = 0; k < LPL; ++k) {
@@ -207,7 +221,9 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
 #pragma unroll
           for (int s = 0; s < 4; ++s)
 #pragma unroll
-            for (int t = 0; t < 10; ++t) a.rf[roff + ((size_t)s * nt + t) * nl + l] = J[k][s][t];
+            for (int t = 0; t < 10; ++t)
+              a.rf[roff + ((size_t)s * nt + t) * nl + l] =
+                  gather_rf<LPL>(c, sm, sm.m[ALFA], pure[k][s], slg[k][s], l, s, t);
       }
     }
     __syncwarp();
@@ -291,14 +307,14 @@ cudaError_t launch_peak(int kind, int blocks, int threads, int iters, void* sink
 
 int invert_blocks_per_sm(int nl) {
   int n = 0;
-  if (nl <= 32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, invert_kernel<1>, kWarpsPerBlock * 32, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, invert_kernel<2>, kWarpsPerBlock * 32, 0);
+  if (nl <= 32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, invert_kernel<1>, warps_per_block<1>() * 32, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, invert_kernel<2>, warps_per_block<2>() * 32, 0);
   return n;
 }
 
 cudaError_t launch_invert(const DevCfg& cfg, const InvertArgs& a, int grid, cudaStream_t s) {
-  if (cfg.nl <= 32) invert_kernel<1><<<grid, kWarpsPerBlock * 32, 0, s>>>(cfg, a);
-  else invert_kernel<2><<<grid, kWarpsPerBlock * 32, 0, s>>>(cfg, a);
+  if (cfg.nl <= 32) invert_kernel<1><<<grid, warps_per_block<1>() * 32, 0, s>>>(cfg, a);
+  else invert_kernel<2><<<grid, warps_per_block<2>() * 32, 0, s>>>(cfg, a);
   return cudaGetLastError();
 }
 
@@ -306,11 +322,11 @@ cudaError_t launch_synth(const DevCfg& cfg, const SynthArgs& a, cudaStream_t s) 
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int64_t need = (a.npix + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  int64_t need = (a.npix + warps_for_nl(cfg.nl) - 1) / warps_for_nl(cfg.nl);
   int grid = (int)(need < (int64_t)sms * 16 ? need : (int64_t)sms * 16);
   if (grid < 1) grid = 1;
-  if (cfg.nl <= 32) synth_kernel<1><<<grid, kWarpsPerBlock * 32, 0, s>>>(cfg, a);
-  else synth_kernel<2><<<grid, kWarpsPerBlock * 32, 0, s>>>(cfg, a);
+  if (cfg.nl <= 32) synth_kernel<1><<<grid, warps_per_block<1>() * 32, 0, s>>>(cfg, a);
+  else synth_kernel<2><<<grid, warps_per_block<2>() * 32, 0, s>>>(cfg, a);
   return cudaGetLastError();
 }
 

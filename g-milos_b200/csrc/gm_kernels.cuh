@@ -8,7 +8,8 @@
 
 namespace gm {
 
-constexpr int kWarpsPerBlock = 4;
+// warps per block of the inversion and synthesis kernels for a grid of nl samples
+inline int warps_for_nl(int nl) { return nl <= 32 ? warps_per_block<1>() : warps_per_block<2>(); }
 
 // Work counters shared by the warps of one persistent launch.
 struct WorkCounters {
