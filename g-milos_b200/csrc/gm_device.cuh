@@ -33,6 +33,7 @@ struct DevCfg {
   int use_psf, use_slight, slight_per_pixel;
   int init_mode, miter, logclambda, quirks;
   int numerics;          // 0: reference intrinsics, 1: accurate trigonometry
+  int tap_lo, tap_hi;    // PSF taps outside [tap_lo, tap_hi] are below float resolution
   int n_pi, n_sig;
   int fix[11];
   float dl[kMaxNl];      // (float)(lambda - lambda0), the reference's sub_aux
@@ -147,10 +148,10 @@ template <int LPL>
 struct WarpSmem {
   double m[11];          // current (last accepted) model: the reference's initModel
   double t[11];          // trial model, persistent like the reference's `model`
-  float A[10][11];       // Jacobi working matrix (upper triangle)
+  float A[2][10][11];    // Jacobi working matrix (upper triangle), double-buffered
   float alpha[56];       // undamped normal matrix, packed upper triangle
   float beta[12];
-  float vec[12];
+  float vec[2][12];      // rotated beta, double-buffered; the step lands in vec[0]
   float cs[18][5], sn[18][5];
   float red[96];
   float ic[kRows];       // continuum about which each staged I row is reflected
@@ -159,19 +160,6 @@ struct WarpSmem {
 
 template <int LPL>
 __host__ __device__ constexpr int warps_per_block() { return LPL == 1 ? 4 : 2; }
-
-// Rotation pairs of the parallel Jacobi: lane b < 5 owns diagonal block
-// (b, b); lanes 5..14 own the off-diagonal blocks (p, q), p < q.
-__device__ __forceinline__ void block_of_lane(int lane, int& p, int& q) {
-  const int bp[15] = {0, 1, 2, 3, 4, 0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
-  const int bq[15] = {0, 1, 2, 3, 4, 1, 2, 3, 4, 2, 3, 4, 3, 4, 4};
-  if (lane < 15) { p = bp[lane]; q = bq[lane]; } else { p = 0; q = 0; }
-}
-// index i moves to rr_perm(i) after every step (gmilos.cu:108-128)
-__device__ __forceinline__ int rr_perm(int i) {
-  const int t[10] = {0, 2, 4, 1, 6, 3, 8, 5, 9, 7};
-  return t[i];
-}
 
 // --------------------------------------------------------------- PSF
 // Stage one row (LPL samples per lane) in shared memory; I rows are
@@ -208,6 +196,7 @@ template <int LPL>
 __device__ __forceinline__ void psf_rows(WarpSmem<LPL>& sm, const DevCfg& c, uint32_t mask,
                                          uint32_t reflect, int lane) {
   const int nl = c.nl, half = nl >> 1;
+  (void)nl;
   while (mask) {
     const int r = __ffs(mask) - 1;
     mask &= mask - 1;
@@ -216,12 +205,12 @@ __device__ __forceinline__ void psf_rows(WarpSmem<LPL>& sm, const DevCfg& c, uin
     for (int k = 0; k < LPL; ++k) {
       const float* base = sm.rows[r] + row_off<LPL>() + lane + 32 * k - half;
       float a0 = 0.f, a1 = 0.f;
-      int j = 0;
-      for (; j + 1 < nl; j += 2) {
+      int j = c.tap_lo;
+      for (; j < c.tap_hi; j += 2) {
         a0 = fmaf(c.psf[j], base[j], a0);
         a1 = fmaf(c.psf[j + 1], base[j + 1], a1);
       }
-      if (j < nl) a0 = fmaf(c.psf[j], base[j], a0);
+      if (j == c.tap_hi) a0 = fmaf(c.psf[j], base[j], a0);
       out[k] = a0 + a1;
     }
     __syncwarp();
@@ -644,103 +633,134 @@ __device__ __forceinline__ float chisq(const DevCfg& c, const float (&syn)[LPL][
 // triangle; after every step the rotated blocks are written to the
 // round-robin relabelled positions.  V is never formed: the step rotations
 // are applied to beta on the way in and replayed transposed, in reverse, on
-// the way out.  Input: sm.alpha (packed), damping flambda; output sm.vec.
+// the way out.  The matrix and the vector are double-buffered so a step
+// needs one warp barrier, and every lane runs the same instruction stream
+// (lanes past 14 shadow block (0, 0) and store nothing).
+struct SolvePlan {
+  int src;                      // offset of this lane's block in the working matrix
+  int d00, d01, d10, d11;       // offsets its four entries move to
+  int p, q;                     // block row / column (rotation pair)
+  int vin, vout0, vout1;        // beta pair read / relabelled write positions
+  int init0, init1;             // packed-triangle entries this lane copies in (-1: none)
+  int ioff0, ioff1;             // and where they go
+};
+
+__device__ __forceinline__ SolvePlan make_solve_plan(int lane) {
+  SolvePlan s;
+  const int bp[15] = {0, 1, 2, 3, 4, 0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
+  const int bq[15] = {0, 1, 2, 3, 4, 1, 2, 3, 4, 2, 3, 4, 3, 4, 4};
+  const int pr[10] = {0, 2, 4, 1, 6, 3, 8, 5, 9, 7};
+  s.p = lane < 15 ? bp[lane] : 0;
+  s.q = lane < 15 ? bq[lane] : 0;
+  const int r0 = 2 * s.p, c0 = 2 * s.q;
+  s.src = r0 * 11 + c0;
+  auto dst = [&](int r, int c) {
+    const int a = pr[r], b = pr[c];
+    return (a < b ? a : b) * 11 + (a < b ? b : a);
+  };
+  s.d00 = dst(r0, c0);
+  s.d01 = dst(r0, c0 + 1);
+  s.d10 = dst(r0 + 1, c0);
+  s.d11 = dst(r0 + 1, c0 + 1);
+  s.vin = r0;
+  s.vout0 = pr[r0];
+  s.vout1 = pr[r0 + 1];
+  // packed upper-triangle index i -> (row, col)
+  s.init0 = -1;
+  s.init1 = -1;
+  s.ioff0 = 0;
+  s.ioff1 = 0;
+  int i = 0;
+  for (int r = 0; r < 10; ++r)
+    for (int c = r; c < 10; ++c, ++i) {
+      if (i == lane) { s.init0 = i; s.ioff0 = r * 11 + c + (r == c ? 1000 : 0); }
+      if (i == lane + 32) { s.init1 = i; s.ioff1 = r * 11 + c + (r == c ? 1000 : 0); }
+    }
+  return s;
+}
+
 template <int LPL>
-__device__ __forceinline__ void solve10(WarpSmem<LPL>& sm, float flambda, int lane, bool accurate) {
-  // damped matrix into the working array (milosUtils.cu:648-652)
-  for (int i = lane; i < 55; i += 32) {
-    int r = 0, cc = i;
-    while (cc >= 10 - r) { cc -= 10 - r; ++r; }
-    const int col = r + cc;
-    float a = sm.alpha[i];
-    if (col == r) a = (float)((double)a * (1.0 + (double)flambda));
-    sm.A[r][col] = a;
+__device__ __forceinline__ void solve10(WarpSmem<LPL>& sm, const SolvePlan& pl, float flambda,
+                                        int lane, bool accurate) {
+  // damped matrix (diagonal x (1 + lambda), milosUtils.cu:648-652)
+  const double damp = 1.0 + (double)flambda;
+  float* A = &sm.A[0][0][0];
+  float* B = &sm.A[1][0][0];
+  if (pl.init0 >= 0) {
+    const float a = sm.alpha[pl.init0];
+    A[pl.ioff0 % 1000] = (pl.ioff0 >= 1000) ? (float)((double)a * damp) : a;
   }
-  if (lane < 10) sm.vec[lane] = sm.beta[lane];
+  if (pl.init1 >= 0) {
+    const float a = sm.alpha[pl.init1];
+    A[pl.ioff1 % 1000] = (pl.ioff1 >= 1000) ? (float)((double)a * damp) : a;
+  }
+  float* va = &sm.vec[0][0];
+  float* vb = &sm.vec[1][0];
+  if (lane < 10) va[lane] = sm.beta[lane];
   __syncwarp();
 
-  int p, q;
-  block_of_lane(lane, p, q);
-  const int r0 = 2 * p, c0 = 2 * q;
   const float quarter = (float)(kPi / 4);
   const float qclamp = __fdividef((float)kPi, 4.f);
-  // destinations of this lane's four entries (fixed for every step)
-  const int d00r = min(rr_perm(r0), rr_perm(c0)), d00c = max(rr_perm(r0), rr_perm(c0));
-  const int d01r = min(rr_perm(r0), rr_perm(c0 + 1)), d01c = max(rr_perm(r0), rr_perm(c0 + 1));
-  const int d10r = min(rr_perm(r0 + 1), rr_perm(c0)), d10c = max(rr_perm(r0 + 1), rr_perm(c0));
-  const int d11r = min(rr_perm(r0 + 1), rr_perm(c0 + 1)), d11c = max(rr_perm(r0 + 1), rr_perm(c0 + 1));
-  const bool active = lane < 15, diag = lane < 5;
-
+  const bool diag = lane < 5, active = lane < 15;
   for (int step = 0; step < 18; ++step) {
-    float m00 = 0.f, m01 = 0.f, m10 = 0.f, m11 = 0.f, b0 = 0.f, b1 = 0.f;
-    if (active) {
-      m00 = sm.A[r0][c0];
-      m01 = sm.A[r0][c0 + 1];
-      m10 = diag ? m01 : sm.A[r0 + 1][c0];
-      m11 = sm.A[r0 + 1][c0 + 1];
+    const float m00 = A[pl.src], m01 = A[pl.src + 1], m11 = A[pl.src + 12];
+    const float m10 = diag ? m01 : A[pl.src + 11];
+    const float b0 = va[pl.vin], b1 = va[pl.vin + 1];
+    float th;
+    if (m00 == m11) {
+      th = quarter;
+    } else {
+      const float arc = accurate ? (2.f * m01) / (m11 - m00) : __fdividef(2.f * m01, m11 - m00);
+      th = accurate ? atanf(arc) / 2.f : __fdividef(atanf(arc), 2.f);
+      th = fminf(fmaxf(th, -qclamp), qclamp);
     }
-    float cs = 1.f, sn = 0.f;
+    float sn, cs;
+    sincos_mode(th, &sn, &cs, accurate);
     if (diag) {
-      b0 = sm.vec[r0];
-      b1 = sm.vec[r0 + 1];
-      float th;
-      if (m00 == m11) {
-        th = quarter;
-      } else {
-        const float arc = accurate ? (2.f * m01) / (m11 - m00) : __fdividef(2.f * m01, m11 - m00);
-        th = accurate ? atanf(arc) / 2.f : __fdividef(atanf(arc), 2.f);
-        if (th > qclamp) th = qclamp;
-        if (th < -qclamp) th = -qclamp;
-      }
-      sincos_mode(th, &sn, &cs, accurate);
       sm.cs[step][lane] = cs;
       sm.sn[step][lane] = sn;
     }
-    const float cr = __shfl_sync(kFull, cs, p), sr = __shfl_sync(kFull, sn, p);
-    const float cc = __shfl_sync(kFull, cs, q), sc = __shfl_sync(kFull, sn, q);
-    __syncwarp();
+    const float cr = __shfl_sync(kFull, cs, pl.p), sr = __shfl_sync(kFull, sn, pl.p);
+    const float cc = __shfl_sync(kFull, cs, pl.q), sc = __shfl_sync(kFull, sn, pl.q);
+    const float t0 = m00 * cr - m10 * sr, t1 = m00 * sr + m10 * cr;
+    const float u0 = m01 * cr - m11 * sr, u1 = m01 * sr + m11 * cr;
+    const float n00 = t0 * cc - u0 * sc, n11 = t1 * sc + u1 * cc;
+    const float n01 = diag ? 0.f : t0 * sc + u0 * cc;
+    const float n10 = diag ? 0.f : t1 * cc - u1 * sc;
     if (active) {
-      const float t0 = m00 * cr - m10 * sr, t1 = m00 * sr + m10 * cr;
-      const float u0 = m01 * cr - m11 * sr, u1 = m01 * sr + m11 * cr;
-      const float n00 = t0 * cc - u0 * sc, n11 = t1 * sc + u1 * cc;
-      if (diag) {
-        sm.A[d00r][d00c] = n00;
-        sm.A[d01r][d01c] = 0.f;
-        sm.A[d11r][d11c] = n11;
-        sm.vec[rr_perm(r0)] = cs * b0 - sn * b1;
-        sm.vec[rr_perm(r0 + 1)] = sn * b0 + cs * b1;
-      } else {
-        sm.A[d00r][d00c] = n00;
-        sm.A[d01r][d01c] = t0 * sc + u0 * cc;
-        sm.A[d10r][d10c] = t1 * cc - u1 * sc;
-        sm.A[d11r][d11c] = n11;
-      }
+      B[pl.d00] = n00;
+      B[pl.d01] = n01;
+      B[pl.d10] = n10;
+      B[pl.d11] = n11;
+    }
+    if (diag) {
+      vb[pl.vout0] = cs * b0 - sn * b1;
+      vb[pl.vout1] = sn * b0 + cs * b1;
     }
     __syncwarp();
+    float* tA = A; A = B; B = tA;
+    float* tv = va; va = vb; vb = tv;
   }
-  // z = (V^T beta) / w with the |w| <= 1e-12 cut
+  // 18 steps: the final matrix and vector are back in the first buffers, in
+  // the original index order.  z = (V^T beta) / w with the |w| <= 1e-12 cut.
   if (lane < 10) {
-    const float w = sm.A[lane][lane];
+    const float w = A[lane * 12];
     const float inv = ((double)fabsf(w) > 1e-12) ? (1.f / w) : 0.f;
-    sm.vec[lane] = sm.vec[lane] * inv;
+    va[lane] = va[lane] * inv;
   }
   __syncwarp();
   // delta = V z: undo the steps in reverse order
   for (int step = 17; step >= 0; --step) {
-    float y0 = 0.f, y1 = 0.f, cs = 0.f, sn = 0.f;
+    const float y0 = va[pl.vout0], y1 = va[pl.vout1];
+    const float cs = sm.cs[step][pl.p], sn = sm.sn[step][pl.p];
     if (diag) {
-      y0 = sm.vec[rr_perm(r0)];
-      y1 = sm.vec[rr_perm(r0 + 1)];
-      cs = sm.cs[step][lane];
-      sn = sm.sn[step][lane];
+      vb[pl.vin] = cs * y0 + sn * y1;
+      vb[pl.vin + 1] = -sn * y0 + cs * y1;
     }
     __syncwarp();
-    if (diag) {
-      sm.vec[r0] = cs * y0 + sn * y1;
-      sm.vec[r0 + 1] = -sn * y0 + cs * y1;
-    }
-    __syncwarp();
+    float* tv = va; va = vb; vb = tv;
   }
+  // 18 swaps: the result is in sm.vec[0]
 }
 
 // --------------------------------------------------------------- model updates

@@ -27,7 +27,7 @@ __device__ __forceinline__ void zero_padding(WarpSmem<LPL>& sm, int lane) {
 // accepted step of the same loop, so the synthesis and the response
 // functions each appear once in the code.
 template <int LPL>
-__global__ void __launch_bounds__(warps_per_block<LPL>() * 32)
+__global__ void __launch_bounds__(warps_per_block<LPL>() * 32, LPL == 1 ? 4 : 2)
 invert_kernel(const DevCfg c, const InvertArgs a) {
   constexpr int WPB = warps_per_block<LPL>();
   __shared__ WarpSmem<LPL> smem[WPB];
@@ -55,6 +55,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
       for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
   }
 
+  const SolvePlan plan = make_solve_plan(lane);
   unsigned long long my_iter = 0, my_acc = 0;
   while (true) {
     unsigned long long pix = 0;
@@ -82,8 +83,8 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
     bool stop = false, first = true;
     while (true) {
       if (!first) {
-        solve10<LPL>(sm, flambda, lane, c.numerics != 0);
-        if (lane == 0) apply_delta_check(c, sm.m, sm.vec, sm.t);
+        solve10<LPL>(sm, plan, flambda, lane, c.numerics != 0);
+        if (lane == 0) apply_delta_check(c, sm.m, sm.vec[0], sm.t);
         __syncwarp();
       }
       synth_lane<LPL>(c, first ? sm.m : sm.t, dlv, lane, ln, an, syn, pure, slg, sm);
@@ -91,7 +92,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
       bool accept = first;
       if (!first) {
         if (iter == 0) {
-          if (a.step_delta && lane < 10) a.step_delta[pix * 10 + lane] = sm.vec[lane];
+          if (a.step_delta && lane < 10) a.step_delta[pix * 10 + lane] = sm.vec[0][lane];
           if (a.step_trial && lane < 11) a.step_trial[pix * 11 + lane] = sm.t[lane];
           if (lane == 0 && a.step_chi2_start) a.step_chi2_start[pix] = chisqr0;
           if (lane == 0 && a.step_chi2_trial) a.step_chi2_trial[pix] = chisqr;
