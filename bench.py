@@ -46,7 +46,9 @@ C_VOIGT, C_RTE, C_DVOIGT, C_DRTE = 100, 85, 23, 870
 
 
 def flops_model(nl, ntaps, n_free, s0_free, psf, stray, ncomp=3):
-    """F_trial, F_acc, F_init of one pixel."""
+    """Algorithmic FLOPs of one pixel: F_trial (one synthesis + chi2 + solve),
+    F_acc (response functions + normal equations at an accepted model) and
+    F_init (classical estimates + the initial synthesis and RF)."""
     n = n_free
     n_conv = n - (1 if s0_free else 0)
     f_trial = nl * (ncomp * C_VOIGT + C_RTE) + (8 * nl * ntaps if psf else 0) + (12 * nl if stray else 0) \
@@ -308,7 +310,7 @@ def run_engine(args):
     clocks = summarize_clocks(clk)
 
     result = {
-        "metric": "converged pixels/s (1024^2 x 4 x 30 lambda, PSF, stray light, 9 ME + alpha free, <=50 LM iterations)",
+        "metric": METRIC,
         "value": value, "unit": "pixels/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 (f64 Voigt polynomials and model parameters)", "data": "synthetic",
@@ -329,6 +331,29 @@ def run_engine(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(obs[: min(P, 200000)].cpu().numpy(), slight, psf, lam, seconds=args.cpu_seconds)
+    if rank == 0 and world == 1 and args.ref_gpu_pixels > 0:
+        import ref
+        n = min(P, args.ref_gpu_pixels)
+        if ref.available(gpu=True):
+            try:
+                rg = reference_gpu(obs[:n].cpu().numpy(), slight, psf, lam, nstreams=args.ref_gpu_streams)
+                rep = rg["report"]
+                cmp_ = _fit_comparison(outs["model"][:n].double().cpu().numpy(), outs["chi2"][:n].cpu().numpy(),
+                                       outs["iters"][:n].cpu().numpy(), rg["model"], rg["chi2"], rg["iters"])
+                result["reference_gpu"] = {
+                    "what": "the reference's own lm_mils built for sm_100a (child launches run in-thread), "
+                            "its launch geometry, streams and device heap, same cube",
+                    "value": rg["value"], "e2e": rg["e2e"], "unit": "pixels/s",
+                    "sample": "first %d pixels of the same cube" % n,
+                    "geometry": {"blocks_per_stream": rep["num_blocks"], "threads_per_block": rep["threads_per_block"],
+                                 "streams": rep["nstreams"], "registers": rep["regs"],
+                                 "stack_bytes": rep["local_bytes"]},
+                    "speedup_value": value / rg["value"], "speedup_e2e": e2e_value / rg["e2e"],
+                    "fit_vs_engine": cmp_}
+            except Exception as exc:  # the comparison must not take the bench line down
+                result["reference_gpu"] = {"unavailable": str(exc)[:200]}
+        else:
+            result["reference_gpu"] = {"unavailable": "oracle/_ref/libgmref_gpu.so not built"}
     if rank == 0:
         print(json.dumps(result), flush=True)
     eng.close()
@@ -336,27 +361,29 @@ def run_engine(args):
         dist.destroy_process_group()
 
 
-# ----------------------------------------------------------------- CPU arms
-def _ref_lib():
-    path = os.path.join(ROOT, "oracle", "_ref", "libgmref.so")
-    return path if os.path.exists(path) else None
+# ----------------------------------------------------------------- reference arms
+def _ref_setup(lam, psf):
+    """The reference's configuration for this workload (oracle/ref.py)."""
+    import oracle as O
+    import ref
+    l0, z = O.fe6173()
+    cfg = O.make_cfg(lam, l0, z, psf=psf, fix=FIX, init=GUESS, miter=MAXITER)
+    return ref.setup_from_cfg(cfg), cfg
 
 
 def cpu_baseline(obs, slight, psf, lam, seconds=15.0, nthreads=0):
     """Time the CPU implementation of the path on a bounded sample of the
-    workload: the reference's routines compiled host-side (oracle/_ref) when
-    built, else the oracle's restatement."""
+    workload: the reference's own routines compiled host-side
+    (oracle/_ref/libgmref_cpu.so, kind "reference") when built, else the
+    oracle's restatement (kind "port")."""
     import oracle as O
-    l0, z = O.fe6173()
+    import ref
     nthreads = nthreads or os.cpu_count()
-    ref = _ref_lib()
-    if ref:
-        import ref_runner
-        runner = ref_runner.RefRunner(ref, lam, l0, psf, slight, FIX, GUESS, MAXITER)
-        run = lambda o: runner.invert(o, nthreads)
+    s, cfg = _ref_setup(lam, psf)
+    if ref.available():
+        run = lambda o: ref.invert_cpu(s, o, slight=slight, nthreads=nthreads)
         kind = "reference"
     else:
-        cfg = O.make_cfg(lam, l0, z, psf=psf, fix=FIX, init=GUESS, miter=MAXITER)
         run = lambda o: O.lm_batch_f(cfg, o, slight=slight, nthreads=nthreads)
         kind = "port"
     probe = min(len(obs), max(256, 16 * nthreads))
@@ -371,26 +398,60 @@ def cpu_baseline(obs, slight, psf, lam, seconds=15.0, nthreads=0):
             "sample": "%d pixels of the same cube (first %d), %.1f s" % (n, n, dt)}
 
 
-def run_reference(args):
-    rank = int(os.environ.get("RANK", 0))
-    if rank != 0:
-        return
+def reference_gpu(obs, slight, psf, lam, nstreams=16):
+    """The reference's own lm_mils built for sm_100a (oracle/_ref/
+    libgmref_gpu.so) on host buffers, with its launch geometry: blocks per
+    stream = occupancy per SM, 32 threads per block, `nstreams` streams.
+    Returns pixels / event-timed kernel time (gmilos.cu:1196-1220), the same
+    with H2D/D2H included, and the fit results for the equal-chi2 check."""
+    import ref
+    s, _ = _ref_setup(lam, psf)
+    m, chi, it, _, rep = ref.invert_gpu(s, np.ascontiguousarray(obs), slight=slight, nstreams=nstreams)
+    P = len(obs)
+    return {"value": P / (rep["kernel_ms"] / 1e3), "e2e": P / (rep["e2e_ms"] / 1e3), "report": rep,
+            "model": m, "chi2": chi, "iters": it}
+
+
+def _fit_comparison(mg, cg, ig, mr, cr, ir):
+    agree = ((np.abs(mg[:, 1] - mr[:, 1]) < 1.0)
+             & (np.minimum(np.abs(mg[:, 5] - mr[:, 5]) % 360, 360 - np.abs(mg[:, 5] - mr[:, 5]) % 360) < 0.1)
+             & (np.minimum(np.abs(mg[:, 6] - mr[:, 6]) % 180, 180 - np.abs(mg[:, 6] - mr[:, 6]) % 180) < 0.1)
+             & (np.abs(mg[:, 2] - mr[:, 2]) < 0.005))
+    return {"median_chi2": [float(np.median(cg)), float(np.median(cr))],
+            "mean_iterations": [float(np.mean(ig)), float(np.mean(ir))],
+            "agree": float(agree.mean()),
+            "engine_chi2_worse": float((~agree & (cg > cr * (1 + 1e-3) + 1e-6)).mean()),
+            "reference_chi2_worse": float((~agree & (cr > cg * (1 + 1e-3) + 1e-6)).mean())}
+
+
+def _reference_sample(args):
+    """A bounded sample of the workload synthesised on the CPU (oracle), so
+    that no engine code runs in the reference arms."""
     import oracle as O
     lam, off = grid()
     x, y = psf_table()
-    l0, z = O.fe6173()
     psf = O.psf_from_table(x, y, off, GRID[1])
     slight = stray_profile_cpu(off)
     rng = np.random.default_rng(args.seed)
-    nthreads = os.cpu_count()
-    # observations of a bounded sample, synthesised on the CPU
-    sample = args.ref_pixels
-    truth = truth_models(sample, rng)
+    truth = truth_models(args.ref_pixels, rng)
     obs = _fine_synth_cpu(O, truth, off)
     a = truth[:, 10][:, None, None].astype(np.float32)
     obs = a * obs + (1 - a) * slight[None]
     obs += (NOISE * np.random.default_rng(args.seed + 1000).standard_normal(obs.shape)).astype(np.float32)
-    obs = np.ascontiguousarray(obs, dtype=np.float32)
+    return np.ascontiguousarray(obs, dtype=np.float32), slight, psf, lam
+
+
+METRIC = "converged pixels/s (1024^2 x 4 x 30 lambda, PSF, stray light, 9 ME + alpha free, <=50 LM iterations)"
+
+
+def run_reference(args):
+    """--impl reference: the reference's own per-pixel routines compiled
+    host-side, on every host thread, on a bounded sample per step."""
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    obs, slight, psf, lam = _reference_sample(args)
+    nthreads = os.cpu_count()
     times = []
     base = None
     for k in range(args.warmup + args.steps):
@@ -400,7 +461,7 @@ def run_reference(args):
             base = b
     value = float(np.mean(times))
     result = {
-        "metric": "converged pixels/s (1024^2 x 4 x 30 lambda, PSF, stray light, 9 ME + alpha free, <=50 LM iterations)",
+        "metric": METRIC,
         "value": value, "unit": "pixels/s", "n_gpus": int(os.environ.get("WORLD_SIZE", 1)), "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic", "impl": "reference",
@@ -413,23 +474,61 @@ def run_reference(args):
     print(json.dumps(result), flush=True)
 
 
+def run_reference_gpu(args):
+    """--impl reference_gpu: the reference's own lm_mils built for sm_100a,
+    one inversion of a bounded sample per step (pixels / event-timed kernel
+    time, as the reference reports it; e2e adds its H2D and D2H copies)."""
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return
+    import ref
+    if not ref.available(gpu=True):
+        print(json.dumps({"impl": "reference_gpu", "unavailable": "oracle/_ref/libgmref_gpu.so not built"}))
+        return
+    obs, slight, psf, lam = _reference_sample(args)
+    vals, e2es, rep = [], [], None
+    for k in range(args.warmup + args.steps):
+        rg = reference_gpu(obs, slight, psf, lam, nstreams=args.ref_gpu_streams)
+        if k >= args.warmup:
+            vals.append(rg["value"])
+            e2es.append(rg["e2e"])
+            rep = rg["report"]
+    P = len(obs)
+    result = {
+        "metric": METRIC, "value": float(np.mean(vals)), "unit": "pixels/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": P / float(np.mean(vals)) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "impl": "reference_gpu",
+        "config": {"workload": "%d px of the full-cube workload x 4 Stokes x 30 lambda" % P,
+                   "blocks_per_stream": rep["num_blocks"], "threads_per_block": rep["threads_per_block"],
+                   "streams": rep["nstreams"], "registers": rep["regs"], "stack_bytes": rep["local_bytes"],
+                   "heap_bytes": rep["heap_bytes"]},
+        "e2e": {"value": float(np.mean(e2es)), "unit": "pixels/s", "h2d_bytes_per_step": obs.nbytes,
+                "d2h_bytes_per_step": P * (11 * 8 + 4 + 4) + obs.nbytes},
+    }
+    print(json.dumps(result), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference", "reference_gpu"])
     ap.add_argument("--pixels", type=int, default=1024 * 1024)
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-pixels", type=int, default=65536)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-gpu-pixels", type=int, default=65536,
+                    help="pixels of the cube run through the reference's sm_100a build (0: skip)")
+    ap.add_argument("--ref-gpu-streams", type=int, default=16)
     args = ap.parse_args()
-    if args.warmup < 3 and args.impl == "engine" and "--allow-short" not in sys.argv:
-        pass
     if args.impl == "reference":
         run_reference(args)
+    elif args.impl == "reference_gpu":
+        run_reference_gpu(args)
     else:
         run_engine(args)
 

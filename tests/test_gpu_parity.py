@@ -122,7 +122,7 @@ def test_float32_and_float64_models_agree(engine):
 def test_one_lm_step_matches_reference(engine, psf, flambda):
     """One iteration from an identical state: the damped normal equations, the
     18-step parallel-Jacobi solve and the step limits against the faithful
-    oracle (north_star: within 1e-4), with accurate trigonometry."""
+    oracle (required: within 1e-4), with accurate trigonometry."""
     rng = np.random.default_rng(300)
     ocfg, gcfg, _ = configs(psf=psf, numerics=1)
     t = H.truth_models(256, rng)
@@ -156,7 +156,7 @@ def test_inversion_matches_reference(engine, psf, stray):
     algorithm in FP32; pixels agree unless rounding flips an accept/reject
     decision, after which both trajectories are still valid fits.  Pixels
     where parameters differ must then have a chi2 no worse than the oracle's
-    (within 1e-3) on >= 99 %, and >= 95 % must agree to the north_star
+    (within 1e-3) on >= 99 %, and >= 95 % must agree to the stated
     tolerances outright."""
     rng = np.random.default_rng(400 + psf)
     fix = H.FREE9[:10] + (1 if stray else 0,)
