@@ -41,6 +41,11 @@ FIX = (1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 1)          # 9 ME parameters + alpha
 STRAY_MODEL = (10.0, 0.0, 0.0, 0.03, 0.1, 0.0, 0.0, 0.3, 0.7, 0.0, 1.0)
 MAXITER = 50
 
+# DRAM bytes (read + write) per pixel of the inversion kernel, measured with
+# ncu (dram__bytes_read.sum + dram__bytes_write.sum) on one 65 536-pixel
+# launch of this workload; traffic grows with the pixel count.
+DRAM_BYTES_PER_PIXEL = 487.0
+
 # Algorithmic FLOPs per pixel (per-wavelength costs counted from the formulas)
 C_VOIGT, C_RTE, C_DVOIGT, C_DRTE = 100, 85, 23, 870
 
@@ -323,7 +328,9 @@ def run_engine(args):
         "e2e": {"value": e2e_value, "unit": "pixels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": 2 * args.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                     "frac": achieved / fp32_peak if fp32_peak else None, "traffic": None,
+                     "frac": achieved / fp32_peak if fp32_peak else None,
+                     "traffic": DRAM_BYTES_PER_PIXEL * P,
+                     "traffic_note": "bytes per launch, scaled from an ncu capture of a 65536-pixel launch",
                      "peak_source": "measured FFMA microbenchmark (gm_measure_peaks), burst",
                      "fp64_peak": fp64_peak,
                      "flops_per_launch": flops_launch, "launch_ms": launch_avg},
