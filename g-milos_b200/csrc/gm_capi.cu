@@ -145,14 +145,12 @@ gm_status build_devcfg(gm_ctx* ctx, const gm_config& c, gm::DevCfg* d) {
   const gm_zeeman& z = c.zeeman;
   if (z.n_pi < 1 || z.n_pi > 10 || z.n_sig < 1 || z.n_sig > 10)
     return fail(ctx, GM_ERR_INVALID, "Zeeman pattern needs 1..10 pi and sigma components");
-  if (c.fix[GM_NPAR - 2] && c.fix[GM_NPAR - 1])
-    return fail(ctx, GM_ERR_UNSUPPORTED, "free macroturbulence together with free alpha (11-term FP64 path) is not available yet");
-  if (c.init_model[9] > 0.0001)
-    return fail(ctx, GM_ERR_UNSUPPORTED, "macroturbulence convolution (v_mac > 1e-4) is not available yet");
   if (c.noise <= 0.f) return fail(ctx, GM_ERR_INVALID, "noise must be > 0");
   std::memset(d, 0, sizeof(*d));
   d->nl = c.nl;
-  d->nterms = 10;
+  // the reference switches to its 11-term kernel when v_mac and alpha are
+  // both free (gmilos.cu:1016-1021)
+  d->nterms = (c.fix[9] && c.fix[10]) ? 11 : 10;
   d->use_psf = c.use_psf ? 1 : 0;
   d->use_slight = c.use_slight ? 1 : 0;
   d->slight_per_pixel = c.slight_per_pixel ? 1 : 0;
@@ -171,6 +169,8 @@ gm_status build_devcfg(gm_ctx* ctx, const gm_config& c, gm::DevCfg* d) {
     d->dl[l] = (float)off;
     d->dld[l] = off;
     d->psf[l] = (float)c.psf[l];
+    d->psfd[l] = c.psf[l];
+    d->lam[l] = c.lambda[l];
   }
   // Taps whose weight is below 1e-10 of the largest contribute less than
   // float resolution to any sample (their total is < 1e-8 of the sum): the
@@ -361,7 +361,7 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   if ((st = stage_out(ctx, "status", status, sizeof(uint32_t) * npix, &a_st)) != GM_OK) return st;
   Arg a_sd, a_strial, a_sc0, a_sc1;
   if (so) {
-    if ((st = stage_out(ctx, "sdelta", so->delta, sizeof(float) * 10 * npix, &a_sd)) != GM_OK) return st;
+    if ((st = stage_out(ctx, "sdelta", so->delta, sizeof(float) * d.nterms * npix, &a_sd)) != GM_OK) return st;
     if ((st = stage_out(ctx, "strial", so->trial, sizeof(double) * 11 * npix, &a_strial)) != GM_OK) return st;
     if ((st = stage_out(ctx, "sc0", so->chi2_start, sizeof(float) * npix, &a_sc0)) != GM_OK) return st;
     if ((st = stage_out(ctx, "sc1", so->chi2_trial, sizeof(float) * npix, &a_sc1)) != GM_OK) return st;
@@ -385,7 +385,7 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   ia.work = ctx->work;
   cudaError_t e = cudaMemsetAsync(ctx->work, 0, sizeof(gm::WorkCounters), s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "work counter reset");
-  const int per_sm = std::max(1, gm::invert_blocks_per_sm(nl));
+  const int per_sm = std::max(1, gm::invert_blocks_per_sm(d, ia.init_models != nullptr));
   int64_t grid = (int64_t)per_sm * ctx->sms;
   const int64_t needed = (npix + gm::warps_for_nl(nl) - 1) / gm::warps_for_nl(nl);
   if (grid > needed) grid = needed;
@@ -683,7 +683,12 @@ gm_status noalloc_scratch(int dev, void** out) {
       cudaGetLastError();
       return GM_ERR_CUDA;
     }
-    if (gm::invert_blocks_per_sm(32) < 1 || gm::invert_blocks_per_sm(64) < 1) {
+    gm::DevCfg probe{};
+    probe.nl = 32;
+    probe.nterms = 10;
+    const int b32 = gm::invert_blocks_per_sm(probe, false);
+    probe.nl = 64;
+    if (b32 < 1 || gm::invert_blocks_per_sm(probe, false) < 1) {
       cudaGetLastError();
       return GM_ERR_CUDA;
     }
@@ -738,7 +743,7 @@ extern "C" gm_status gm_invert_noalloc(const gm_config* cfg, const float* iquv, 
   ia.fitted = fitted;
   ia.status = status;
   ia.work = (gm::WorkCounters*)scratch;
-  const int per_sm = std::max(1, gm::invert_blocks_per_sm(nl));
+  const int per_sm = std::max(1, gm::invert_blocks_per_sm(d, false));
   int64_t grid = (int64_t)per_sm * sms;
   const int64_t needed = (npix + gm::warps_for_nl(nl) - 1) / gm::warps_for_nl(nl);
   if (grid > needed) grid = needed;

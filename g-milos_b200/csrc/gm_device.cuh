@@ -39,6 +39,8 @@ struct DevCfg {
   float dl[kMaxNl];      // (float)(lambda - lambda0), the reference's sub_aux
   double dld[kMaxNl];    // lambda - lambda0 in double (classical estimates)
   float psf[kMaxNl];     // PSF taps
+  double psfd[kMaxNl];   // the same taps in double (folded into the macroturbulence kernel)
+  double lam[kMaxNl];    // absolute wavelengths (macroturbulence kernel)
   float nup[10], nub[10], wep[10], web[10], wer[10];
   float geff, fo, mu, ilambda, noise;
   float weight[4];
@@ -126,36 +128,62 @@ struct Angles {
   float cosi, sinis, sina, cosa, sinda, cosda, sindi, cosdi, cosis_2;
 };
 
+// Kernel variants.  V = 0: the reference's 10-term path without
+// macroturbulence; V = 1: 10 terms with the macroturbulence convolution
+// (a fixed v_mac > 0, or per-pixel start models); V = 2: the 11-term path
+// (v_mac and alpha both free: lm_mils_11, milosUtils.cu:713-850) with its
+// FP64 solve.
+template <int V>
+struct Variant {
+  static constexpr int NT = (V == 2) ? 11 : 10;         // terms of the normal equations
+  static constexpr bool MAC = V != 0;                    // macroturbulence-capable
+  static constexpr int ROWS = MAC ? 36 : 32;             // staged rows (+4 for the v_mac RF)
+};
+
 // Per-lane results of a synthesis that the response functions reuse:
 // absorption / dispersion profiles of the pi, blue and red groups and the
 // last component's H, F, v of each group (the reference's profile
-// derivatives keep only the last component of a group, me_der.cu:66-74).
-template <int LPL>
+// derivatives keep only the last component of a group, me_der.cu:66-74);
+// with macroturbulence also the profile before any convolution (the
+// reference's spectra_mc, mil_sinrf.cu:425-430).
+template <int LPL, int V>
 struct Lane {
   float fi[LPL][3], shi[LPL][3];
   float lh[LPL][3], lf[LPL][3], lu[LPL][3];
+  float mc[Variant<V>::MAC ? LPL : 1][4];
 };
 
 // Rows staged for the PSF: Stokes s x RF slot {eta0, B, vlos, dopp, damping,
-// gamma, azimuth, S1} (S0's RF is constant, alpha's is never convolved).
+// gamma, azimuth, S1} (S0's RF is constant, alpha's is never convolved);
+// macroturbulence variants add the v_mac RF of Stokes s at row 32 + s.
 constexpr int kRows = 32;
 __host__ __device__ constexpr int rf_row(int s, int t) { return s * 8 + (t == 8 ? 7 : t); }
+__host__ __device__ constexpr int mac_row(int s) { return kRows + s; }
 template <int LPL>
 __host__ __device__ constexpr int row_off() { return 16 * LPL; }   // samples at [16 LPL, 48 LPL)
 
 // Warp-private shared memory.
-template <int LPL>
+template <int LPL, int V>
 struct WarpSmem {
+  static constexpr int NR = Variant<V>::ROWS;
+  static constexpr bool S11 = V == 2;
   double m[11];          // current (last accepted) model: the reference's initModel
   double t[11];          // trial model, persistent like the reference's `model`
   float A[2][10][11];    // Jacobi working matrix (upper triangle), double-buffered
-  float alpha[56];       // undamped normal matrix, packed upper triangle
+  float alpha[68];       // undamped normal matrix, packed upper triangle (55 or 66)
   float beta[12];
   float vec[2][12];      // rotated beta, double-buffered; the step lands in vec[0]
   float cs[18][5], sn[18][5];
   float red[96];
-  float ic[kRows];       // continuum about which each staged I row is reflected
-  float rows[kRows][64 * LPL];   // zero-padded rows for the PSF
+  float ic[NR];          // continuum about which each staged I row is reflected
+  double gk[Variant<V>::MAC ? kMaxNl : 1];   // macroturbulence kernel (PSF folded in)
+  double gd[Variant<V>::MAC ? kMaxNl : 1];   // its derivative with respect to v_mac
+  double dd[12];         // FP64 step of the 11-term solve
+  double A11[S11 ? 2 : 1][S11 ? 144 : 1];    // 11-term Jacobi matrix (12x12), double-buffered
+  double V11[S11 ? 2 : 1][S11 ? 144 : 1];    // its accumulated rotations
+  double b11[S11 ? 12 : 1], z11[S11 ? 12 : 1];
+  double c11[S11 ? 6 : 1], s11[S11 ? 6 : 1]; // the step's rotations
+  float rows[NR][64 * LPL];   // zero-padded rows for the PSF
 };
 
 template <int LPL>
@@ -165,8 +193,8 @@ __host__ __device__ constexpr int warps_per_block() { return LPL == 1 ? 4 : 2; }
 // Stage one row (LPL samples per lane) in shared memory; I rows are
 // reflected about their continuum max(first, last) (direct_convolution_ic,
 // convolution.cu:200-241).
-template <int LPL>
-__device__ __forceinline__ void put_row(WarpSmem<LPL>& sm, int r, const float (&x)[LPL], int nl,
+template <int LPL, int V>
+__device__ __forceinline__ void put_row(WarpSmem<LPL, V>& sm, int r, const float (&x)[LPL], int nl,
                                         int lane, bool reflect) {
   float ic = 0.f;
   if (reflect) {
@@ -192,8 +220,8 @@ __device__ __forceinline__ void put_row(WarpSmem<LPL>& sm, int r, const float (&
 // odd taps (direct_convolution{,_ic}, convolution.cu:153-241); rows in
 // `reflect` are reflected back about sm.ic.  The caller syncs the warp after
 // staging.  One loop over rows keeps the code small whatever the row count.
-template <int LPL>
-__device__ __forceinline__ void psf_rows(WarpSmem<LPL>& sm, const DevCfg& c, uint32_t mask,
+template <int LPL, int V>
+__device__ __forceinline__ void psf_rows(WarpSmem<LPL, V>& sm, const DevCfg& c, uint32_t mask,
                                          uint32_t reflect, int lane) {
   const int nl = c.nl, half = nl >> 1;
   (void)nl;
@@ -225,15 +253,121 @@ __device__ __forceinline__ void psf_rows(WarpSmem<LPL>& sm, const DevCfg& c, uin
   __syncwarp();
 }
 
+// --------------------------------------------------------------- macroturbulence
+// The macroturbulence kernel: a Gaussian in wavelength of width
+// lambda0 * v_mac / c sampled on the grid about sample nl/2 and normalised to
+// unit sum (fgauss, fgauss.cu:16-63), in sm.gk; with `deriv` also its
+// derivative with respect to v_mac, g / v_mac * (x^2 - 1) (me_der.cu:122-129),
+// in sm.gd.  With a PSF both are then correlated with it in double, zero
+// padded about nl/2 (direct_convolution_double, convolution.cu:120-151;
+// mil_sinrf.cu:105-107, me_der.cu:131-136).
+template <int LPL, int V>
+__device__ __forceinline__ void mac_kernels(const DevCfg& c, WarpSmem<LPL, V>& sm, double mac,
+                                            int lane, bool deriv) {
+  const int nl = c.nl, half = nl >> 1;
+  const double ild = (c.lambda0 * mac) / kVlight;
+  const double lc = c.lam[half];
+  double g[LPL], x2[LPL], part = 0.0;
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+    g[k] = 0.0;
+    x2[k] = 0.0;
+    if (l < nl) {
+      const double x = (c.lam[l] - lc) / ild;
+      const double term = (x * x) / 2;
+      g[k] = term < 1e30 ? exp(-term) : 0.0;
+      x2[k] = x * x;
+      part += g[k];
+    }
+  }
+  const double sum = warp_sum_d(part);
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+    if (l < nl) {
+      const double gn = g[k] / sum;
+      sm.gk[l] = gn;
+      if (deriv) sm.gd[l] = gn / mac * (x2[k] - 1.0);
+    }
+  }
+  __syncwarp();
+  if (!c.use_psf) return;
+  double og[LPL], od[LPL];
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+    double a = 0.0, b = 0.0;
+    if (l < nl) {
+      for (int j = 0; j < nl; ++j) {
+        const int idx = l + j - half;
+        if (idx < 0 || idx >= nl) continue;
+        a += c.psfd[j] * sm.gk[idx];
+        if (deriv) b += c.psfd[j] * sm.gd[idx];
+      }
+    }
+    og[k] = a;
+    od[k] = b;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+    if (l < nl) {
+      sm.gk[l] = og[k];
+      if (deriv) sm.gd[l] = od[k];
+    }
+  }
+  __syncwarp();
+}
+
+// In-place circular convolution of the staged rows in `mask` with the nl-tap
+// kernel h, accumulated in double with kernel sample j at lag j, the result
+// rotated so that sample nl/2 is the zero lag (convCircular,
+// convolution.cu:251-279): output m takes the circular sum at index
+// (m + nl/2) mod nl.  The caller syncs the warp after staging.
+template <int LPL, int V>
+__device__ __forceinline__ void circ_rows(WarpSmem<LPL, V>& sm, const DevCfg& c, uint64_t mask,
+                                          const double* h, int lane) {
+  const int nl = c.nl, half = nl >> 1;
+  while (mask) {
+    const int r = __ffsll((long long)mask) - 1;
+    mask &= mask - 1;
+    const float* x = sm.rows[r] + row_off<LPL>();
+    float out[LPL];
+#pragma unroll
+    for (int k = 0; k < LPL; ++k) {
+      const int mo = lane + 32 * k;
+      double a = 0.0;
+      if (mo < nl) {
+        int idx = mo + half;
+        if (idx >= nl) idx -= nl;
+        for (int j = 0; j < nl; ++j) {
+          a += h[j] * (double)x[idx];
+          idx = (idx == 0) ? nl - 1 : idx - 1;
+        }
+      }
+      out[k] = (float)a;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < LPL; ++k) {
+      const int mo = lane + 32 * k;
+      if (mo < nl) sm.rows[r][row_off<LPL>() + mo] = out[k];
+    }
+  }
+  __syncwarp();
+}
+
 // --------------------------------------------------------------- synthesis
 // ME synthesis of this lane's samples (mil_sinrf.cu:27-142 with
 // mil_sinrf_kernel :334-433): Zeeman components through the Voigt
 // profiles, Unno-Rachkovsky solution, PSF, stray-light mix.
-template <int LPL>
+template <int LPL, int V>
 __device__ __forceinline__ void synth_lane(const DevCfg& c, const double* m, const float (&dlv)[LPL],
-                                           int lane, Lane<LPL>& st, Angles& an,
+                                           int lane, Lane<LPL, V>& st, Angles& an,
                                            float (&spec)[LPL][4], float (&pure)[LPL][4],
-                                           const float (&sl)[LPL][4], WarpSmem<LPL>& sm) {
+                                           const float (&sl)[LPL][4], WarpSmem<LPL, V>& sm) {
   const float CC = (float)(kPi / 180.0), CC2 = (float)((kPi / 180.0) * 2);
   const double azi = m[AZ] * (double)CC, gmr = m[GM] * (double)CC;
   float sgm, cgm;
@@ -315,17 +449,43 @@ __device__ __forceinline__ void synth_lane(const DevCfg& c, const double* m, con
     spec[k][3] = dtiaux * (gp6 + rv * gp2);
   }
 
-  if (c.use_psf) {
+  bool mac_on = false;
+  if constexpr (Variant<V>::MAC) {
+#pragma unroll
+    for (int k = 0; k < LPL; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) st.mc[k][s] = spec[k][s];
+    mac_on = m[MAC] > 0.0001;
+  }
+  if (mac_on) {
+    // macroturbulence with the PSF folded into its kernel; the PSF is not
+    // applied again (mil_sinrf.cu:101-130)
+    mac_kernels<LPL, V>(c, sm, m[MAC], lane, false);
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      float row[LPL];
+#pragma unroll
+      for (int k = 0; k < LPL; ++k) row[k] = spec[k][s];
+      put_row<LPL, V>(sm, s, row, c.nl, lane, false);
+    }
+    __syncwarp();
+    circ_rows<LPL, V>(sm, c, 0xfull, sm.gk, lane);
+#pragma unroll
+    for (int k = 0; k < LPL; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) spec[k][s] = sm.rows[s][row_off<LPL>() + lane + 32 * k];
+    __syncwarp();
+  } else if (c.use_psf) {
     __syncwarp();
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
       float row[LPL];
 #pragma unroll
       for (int k = 0; k < LPL; ++k) row[k] = spec[k][s];
-      put_row<LPL>(sm, s, row, c.nl, lane, s == 0);
+      put_row<LPL, V>(sm, s, row, c.nl, lane, s == 0);
     }
     __syncwarp();
-    psf_rows<LPL>(sm, c, 0xfu, 0x1u, lane);
+    psf_rows<LPL, V>(sm, c, 0xfu, 0x1u, lane);
 #pragma unroll
     for (int k = 0; k < LPL; ++k)
 #pragma unroll
@@ -369,9 +529,9 @@ __device__ __forceinline__ uint32_t rf_row_mask(const DevCfg& c) {
 // of sm (rf_row); gather_rf adds S0, alpha, the stray-light scaling
 // (:191-211) and the zeros of fixed parameters
 // (FijaACeroDerivadasNoNecesarias, milosUtils.cu:243-271).
-template <int LPL>
-__device__ __forceinline__ void rf_rows(const DevCfg& c, const double* m, const Lane<LPL>& st,
-                                        const Angles& an, int lane, WarpSmem<LPL>& sm) {
+template <int LPL, int V>
+__device__ __forceinline__ void rf_rows(const DevCfg& c, const double* m, const Lane<LPL, V>& st,
+                                        const Angles& an, int lane, WarpSmem<LPL, V>& sm) {
   const float auxCte = __fdividef((float)(-c.lambda0), (float)(kVlight * m[DOPP]));
   const double aa = m[AA], dopp = m[DOPP];
   // last component of each group: its scaled splitting and strength
@@ -516,7 +676,26 @@ __device__ __forceinline__ void rf_rows(const DevCfg& c, const double* m, const 
   }
   __syncwarp();
 
-  if (c.use_psf) {
+  bool mac_on = false;
+  if constexpr (Variant<V>::MAC) mac_on = m[MAC] > 0.0001;
+  if (mac_on) {
+    if constexpr (Variant<V>::MAC) {
+      // macroturbulence (me_der.cu:117-156): the v_mac RF is the profile
+      // before convolution through the kernel's derivative; every other
+      // staged RF goes through the kernel (PSF folded into both)
+      mac_kernels<LPL, V>(c, sm, m[MAC], lane, true);
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        float row[LPL];
+#pragma unroll
+        for (int k = 0; k < LPL; ++k) row[k] = st.mc[k][s];
+        put_row<LPL, V>(sm, mac_row(s), row, nl, lane, false);
+      }
+      __syncwarp();
+      circ_rows<LPL, V>(sm, c, 0xfull << kRows, sm.gd, lane);
+      circ_rows<LPL, V>(sm, c, (uint64_t)mask, sm.gk, lane);
+    }
+  } else if (c.use_psf) {
     // reflect the I rows about max(first, last) (me_der.cu:167-176)
     uint32_t refl = 0;
     float icv[8];
@@ -543,60 +722,90 @@ __device__ __forceinline__ void rf_rows(const DevCfg& c, const double* m, const 
       }
     }
     __syncwarp();
-    psf_rows<LPL>(sm, c, mask, refl, lane);
+    psf_rows<LPL, V>(sm, c, mask, refl, lane);
   }
 }
 
-// Response function of sample l, Stokes s, slot t in the reference's
-// 10-term layout (slot 7 = S0, slot 9 = alpha) after the PSF: stray-light
-// scaling, alpha's RF from the unscaled profile, zero for fixed parameters.
-template <int LPL>
-__device__ __forceinline__ float gather_rf(const DevCfg& c, const WarpSmem<LPL>& sm, double alfa,
-                                           float asrc, float sl, int l, int s, int t) {
-  const int key = (t == 9) ? 10 : t;
+// Response function of sample l, Stokes s, slot t in the reference's layout
+// after the PSF: 10 terms (slot 7 = S0, slot 9 = alpha) or 11 terms (slot 9
+// = v_mac, slot 10 = alpha).  Stray-light scaling, alpha's RF from the
+// unscaled profile (me_der.cu:191-211), zero for fixed parameters
+// (FijaACeroDerivadasNoNecesarias, milosUtils.cu:243-271; in the 10-term
+// layout slot 9 follows alpha's flag).  mac_on: the v_mac RF rows hold the
+// derivative of the macroturbulence convolution.
+template <int LPL, int V>
+__device__ __forceinline__ float gather_rf(const DevCfg& c, const WarpSmem<LPL, V>& sm, double alfa,
+                                           float asrc, float sl, int l, int s, int t, bool mac_on) {
+  constexpr int NT = Variant<V>::NT;
+  const int key = (NT == 10 && t == 9) ? 10 : t;
   if (!c.fix[key]) return 0.f;
-  if (t == 9) return c.use_slight ? asrc - sl : 0.f;
-  float v;
-  if (t == 7) v = (s == 0) ? 1.f : 0.f;
-  else if (t == 6 && (s == 0 || s == 3)) v = 0.f;
-  else v = sm.rows[rf_row(s, t)][row_off<LPL>() + l];
+  float v = 0.f;
+  if (t == NT - 1) {
+    // alpha's slot; without stray light the 10-term slot keeps the v_mac RF
+    // me_der wrote there (me_der.cu:140-143)
+    if (c.use_slight) return asrc - sl;
+    if constexpr (Variant<V>::MAC && NT == 10) {
+      if (mac_on) return sm.rows[mac_row(s)][row_off<LPL>() + l];
+    }
+    return 0.f;
+  }
+  if (t == 9) {
+    if constexpr (Variant<V>::MAC) {
+      if (mac_on) v = sm.rows[mac_row(s)][row_off<LPL>() + l];
+    }
+  } else if (t == 7) {
+    v = (s == 0) ? 1.f : 0.f;
+  } else if (t == 6 && (s == 0 || s == 3)) {
+    v = 0.f;
+  } else {
+    v = sm.rows[rf_row(s, t)][row_off<LPL>() + l];
+  }
   if (c.use_slight) v = (float)((double)v * alfa);
   return v;
 }
 
-// packed index of (i <= h) in the upper triangle of a 10x10 matrix
-__host__ __device__ constexpr int upk(int i, int h) { return i * 10 - (i * (i - 1)) / 2 + (h - i); }
+// packed index of (i <= h) in the upper triangle of an n x n matrix
+template <int NT>
+__host__ __device__ constexpr int upk(int i, int h) { return i * NT - (i * (i - 1)) / 2 + (h - i); }
 
 // Normal equations alpha = sum_s w_s/sigma^2 J^T J and beta = sum_s w_s J^T
-// (syn - obs) / sigma^2 (covarmf, lib.cu:65-118) from the staged response
-// functions, reduced across the warp; results land in sm.alpha (packed) and
-// sm.beta.
-template <int LPL>
-__device__ __forceinline__ void normal_eq(const DevCfg& c, const double* m,
-                                          const float (&asrc)[LPL][4], const float (&sl)[LPL][4],
+// (syn - obs) / sigma^2 (covarmf, lib.cu:65-118; covarm, lib.cu:12-63 for
+// 11 terms) from the staged response functions, reduced across the warp;
+// results land in sm.alpha (packed) and sm.beta.  alpha's RF is taken from
+// the mixed profile `syn` when alpha_mixed (milosUtils.cu:675), else from the
+// unmixed `pure`.
+template <int LPL, int V>
+__device__ __forceinline__ void normal_eq(const DevCfg& c, const double* m, bool alpha_mixed,
+                                          const float (&pure)[LPL][4], const float (&sl)[LPL][4],
                                           const float (&syn)[LPL][4], const float (&ob)[LPL][4],
-                                          const bool (&valid)[LPL], int lane, WarpSmem<LPL>& sm) {
+                                          const bool (&valid)[LPL], int lane, WarpSmem<LPL, V>& sm) {
+  constexpr int NT = Variant<V>::NT;
+  constexpr int NP = NT * (NT + 1) / 2;
+  static_assert(NP + NT <= 96, "normal equations exceed the reduction width");
   float v[96];
 #pragma unroll
   for (int i = 0; i < 96; ++i) v[i] = 0.f;
   const double alfa = m[ALFA];
+  bool mac_on = false;
+  if constexpr (Variant<V>::MAC) mac_on = m[MAC] > 0.0001;
 #pragma unroll
   for (int k = 0; k < LPL; ++k) {
     if (!valid[k]) continue;
     const int l = lane + 32 * k;
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
-      float J[10];
+      float J[NT];
+      const float asrc = alpha_mixed ? syn[k][s] : pure[k][s];
 #pragma unroll
-      for (int t = 0; t < 10; ++t) J[t] = gather_rf<LPL>(c, sm, alfa, asrc[k][s], sl[k][s], l, s, t);
+      for (int t = 0; t < NT; ++t) J[t] = gather_rf<LPL, V>(c, sm, alfa, asrc, sl[k][s], l, s, t, mac_on);
       const float wd = c.wsig[s];
       const float r = c.weight[s] * (syn[k][s] - ob[k][s]);
 #pragma unroll
-      for (int i = 0; i < 10; ++i) {
+      for (int i = 0; i < NT; ++i) {
         const float ji = J[i];
 #pragma unroll
-        for (int h = i; h < 10; ++h) v[upk(i, h)] = fmaf(wd * ji, J[h], v[upk(i, h)]);
-        v[55 + i] = fmaf(r, ji, v[55 + i]);
+        for (int h = i; h < NT; ++h) v[upk<NT>(i, h)] = fmaf(wd * ji, J[h], v[upk<NT>(i, h)]);
+        v[NP + i] = fmaf(r, ji, v[NP + i]);
       }
     }
   }
@@ -604,8 +813,8 @@ __device__ __forceinline__ void normal_eq(const DevCfg& c, const double* m,
 #pragma unroll
   for (int i = 0; i < 3; ++i) sm.red[3 * lane + i] = v[i];
   __syncwarp();
-  for (int i = lane; i < 55; i += 32) sm.alpha[i] = sm.red[i];
-  if (lane < 10) sm.beta[lane] = __fdividef(sm.red[55 + lane], c.noise);
+  for (int i = lane; i < NP; i += 32) sm.alpha[i] = sm.red[i];
+  if (lane < NT) sm.beta[lane] = __fdividef(sm.red[NP + lane], c.noise);
   __syncwarp();
 }
 
@@ -679,8 +888,8 @@ __device__ __forceinline__ SolvePlan make_solve_plan(int lane) {
   return s;
 }
 
-template <int LPL>
-__device__ __forceinline__ void solve10(WarpSmem<LPL>& sm, const SolvePlan& pl, float flambda,
+template <int LPL, int V>
+__device__ __forceinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, float flambda,
                                         int lane, bool accurate) {
   // damped matrix (diagonal x (1 + lambda), milosUtils.cu:648-652)
   const double damp = 1.0 + (double)flambda;
@@ -763,12 +972,159 @@ __device__ __forceinline__ void solve10(WarpSmem<LPL>& sm, const SolvePlan& pl, 
   // 18 swaps: the result is in sm.vec[0]
 }
 
+// --------------------------------------------------------------- 11x11 solve (FP64)
+// delta = V diag(1/w) V^T beta for the damped 11x11 normal matrix in double
+// with the |w| <= 1e-12 cut (mil_svd, milosUtils.cu:280-325).  The reference
+// takes (w, V) from a converged Golub-Reinsch SVD (svdcmp, svdcmp.cu:37-234);
+// for this symmetric positive semi-definite matrix the same decomposition is
+// reached by cyclic two-sided Jacobi rotations run to convergence.  The
+// matrix is padded to 12x12 with a zero row and column (eigenvalue 0, cut).
+// Lanes 0..20 own the 21 2x2 blocks of the upper triangle and write each
+// rotated block to its round-robin relabelled position (a 12-index
+// tournament: every index pair meets once in 11 steps); V's columns follow
+// the same relabelling while its rows stay in parameter order.  Sweeps
+// repeat until one leaves every off-diagonal entry at or below 1e-15 of the
+// geometric mean of its diagonal pair, at most 16.
+struct Solve11Plan {
+  int src;                 // this lane's block (row-major 12x12 offset)
+  int d00, d01, d10, d11;  // where its entries move
+  int p, q;                // block row / column (rotation pair)
+  int vrow, vpair;         // V update: row and first of three pairs (lanes < 24)
+};
+
+__device__ __forceinline__ int perm12(int i) {
+  const int pr[12] = {0, 2, 4, 1, 6, 3, 8, 5, 10, 7, 11, 9};
+  return pr[i];
+}
+
+__device__ __forceinline__ Solve11Plan make_solve11_plan(int lane) {
+  Solve11Plan s;
+  int p = 0, q = 0;
+  if (lane < 6) {
+    p = q = lane;
+  } else if (lane < 21) {
+    int k = 6;
+    for (int a = 0; a < 6; ++a)
+      for (int b = a + 1; b < 6; ++b, ++k)
+        if (k == lane) { p = a; q = b; }
+  }
+  s.p = p;
+  s.q = q;
+  const int r0 = 2 * p, c0 = 2 * q;
+  s.src = r0 * 12 + c0;
+  auto dst = [](int r, int c) {
+    const int a = perm12(r), b = perm12(c);
+    return (a < b ? a : b) * 12 + (a < b ? b : a);
+  };
+  s.d00 = dst(r0, c0);
+  s.d01 = dst(r0, c0 + 1);
+  s.d10 = dst(r0 + 1, c0);
+  s.d11 = dst(r0 + 1, c0 + 1);
+  s.vrow = lane % 12;
+  s.vpair = (lane / 12) * 3;
+  return s;
+}
+
+template <int LPL, int V>
+__device__ __forceinline__ void solve11(WarpSmem<LPL, V>& sm, const Solve11Plan& pl, float flambda,
+                                        int lane) {
+  static_assert(V == 2, "the FP64 solve belongs to the 11-term variant");
+  // damped matrix in double (milosUtils.cu:787-791), padded to 12x12
+  const double damp = 1.0 + (double)flambda;
+  double* A = sm.A11[0];
+  double* B = sm.A11[1];
+  double* Va = sm.V11[0];
+  double* Vb = sm.V11[1];
+  for (int i = lane; i < 144; i += 32) {
+    const int r = i / 12, c = i - 12 * (i / 12);
+    double v = 0.0;
+    if (r < 11 && c < 11) {
+      const int a = r < c ? r : c, b = r < c ? c : r;
+      v = (double)sm.alpha[upk<11>(a, b)];
+      if (r == c) v = v * damp;
+    }
+    A[i] = v;
+    Va[i] = (r == c) ? 1.0 : 0.0;
+  }
+  if (lane < 12) sm.b11[lane] = lane < 11 ? (double)sm.beta[lane] : 0.0;
+  __syncwarp();
+
+  const bool diag = lane < 6, active = lane < 21, vlane = lane < 24;
+  bool sweep_moved = false;
+  for (int step = 0; step < 16 * 11; ++step) {
+    const double m00 = A[pl.src], m01 = A[pl.src + 1], m11 = A[pl.src + 13];
+    const double m10 = diag ? m01 : A[pl.src + 12];
+    bool moved = false;
+    if (diag) {
+      double cs = 1.0, sn = 0.0;
+      if (m01 != 0.0) {
+        moved = fabs(m01) > 1e-15 * sqrt(fabs(m00)) * sqrt(fabs(m11));
+        const double tau = (m11 - m00) / (2.0 * m01);
+        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+        cs = 1.0 / sqrt(1.0 + t * t);
+        sn = t * cs;
+      }
+      sm.c11[lane] = cs;
+      sm.s11[lane] = sn;
+    }
+    sweep_moved |= __any_sync(kFull, moved);
+    __syncwarp();
+    const double cr = sm.c11[pl.p], sr = sm.s11[pl.p];
+    const double cc = sm.c11[pl.q], sc = sm.s11[pl.q];
+    const double t0 = m00 * cr - m10 * sr, t1 = m00 * sr + m10 * cr;
+    const double u0 = m01 * cr - m11 * sr, u1 = m01 * sr + m11 * cr;
+    const double n00 = t0 * cc - u0 * sc, n11 = t1 * sc + u1 * cc;
+    const double n01 = diag ? 0.0 : t0 * sc + u0 * cc;
+    const double n10 = diag ? 0.0 : t1 * cc - u1 * sc;
+    if (active) {
+      B[pl.d00] = n00;
+      B[pl.d01] = n01;
+      B[pl.d10] = n10;
+      B[pl.d11] = n11;
+    }
+    if (vlane) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int pp = pl.vpair + k;
+        const double c2 = sm.c11[pp], s2 = sm.s11[pp];
+        const double v0 = Va[pl.vrow * 12 + 2 * pp], v1 = Va[pl.vrow * 12 + 2 * pp + 1];
+        Vb[pl.vrow * 12 + perm12(2 * pp)] = v0 * c2 - v1 * s2;
+        Vb[pl.vrow * 12 + perm12(2 * pp + 1)] = v0 * s2 + v1 * c2;
+      }
+    }
+    __syncwarp();
+    double* tA = A; A = B; B = tA;
+    double* tV = Va; Va = Vb; Vb = tV;
+    if (step % 11 == 10) {
+      if (!sweep_moved) break;
+      sweep_moved = false;
+    }
+  }
+  // z = V^T beta / w with the cut, then delta = V z
+  if (lane < 12) {
+    double z = 0.0;
+    for (int r = 0; r < 11; ++r) z += sm.b11[r] * Va[r * 12 + lane];
+    const double w = A[lane * 13];
+    sm.z11[lane] = z * ((fabs(w) > 1e-12) ? (1 / w) : 0.0);
+  }
+  __syncwarp();
+  if (lane < 11) {
+    double d = 0.0;
+    for (int k = 0; k < 12; ++k) d += Va[lane * 12 + k] * sm.z11[k];
+    sm.dd[lane] = d;
+  }
+  __syncwarp();
+}
+
 // --------------------------------------------------------------- model updates
 // model -= delta on free parameters with the reference's step limits
-// (AplicaDeltaf, milosUtils.cu:93-159), then range checks (check, :160-238).
-__device__ __forceinline__ void apply_delta_check(const DevCfg& c, const double* m, const float* d,
+// (AplicaDeltaf, milosUtils.cu:93-159, float delta; AplicaDelta, :30-91,
+// double delta for 11 terms), then range checks (check, :160-238).  The
+// filling factor's step is slot 9 of 10 or slot 10 of 11.
+template <int NT, typename T>
+__device__ __forceinline__ void apply_delta_check(const DevCfg& c, const double* m, const T* d,
                                                   double* t) {
-  float aux;
+  T aux;
   if (c.fix[ETA0]) t[ETA0] = m[ETA0] - d[0];
   if (c.fix[BFLD]) {
     aux = d[1];
@@ -791,7 +1147,7 @@ __device__ __forceinline__ void apply_delta_check(const DevCfg& c, const double*
   if (c.fix[S0]) t[S0] = m[S0] - d[7];
   if (c.fix[S1]) t[S1] = m[S1] - d[8];
   if (c.fix[MAC]) t[MAC] = m[MAC] - d[9];
-  if (c.fix[ALFA]) t[ALFA] = m[ALFA] - d[9];
+  if (c.fix[ALFA]) t[ALFA] = m[ALFA] - d[NT == 11 ? 10 : 9];
   if (t[BFLD] < 0) { t[BFLD] = -t[BFLD]; t[GM] = 180.0 - t[GM]; }
   if (t[BFLD] > 5000) t[BFLD] = 5000;
   if (t[GM] < 0) t[GM] = -t[GM];

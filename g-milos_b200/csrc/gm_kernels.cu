@@ -15,25 +15,36 @@ __device__ __forceinline__ void load_pixel(const float* __restrict__ p, int nl, 
   }
 }
 
-template <int LPL>
-__device__ __forceinline__ void zero_padding(WarpSmem<LPL>& sm, int lane) {
-  for (int i = lane; i < kRows * 64 * LPL; i += 32) (&sm.rows[0][0])[i] = 0.f;
+template <int LPL, int V>
+__device__ __forceinline__ void zero_padding(WarpSmem<LPL, V>& sm, int lane) {
+  for (int i = lane; i < WarpSmem<LPL, V>::NR * 64 * LPL; i += 32) (&sm.rows[0][0])[i] = 0.f;
   __syncwarp();
 }
 
+// Warp-private shared memory lives in the dynamic allocation (the larger
+// variants exceed the 48 KB static limit).
+extern __shared__ __align__(16) unsigned char gm_dyn_smem[];
+
+template <int LPL, int V>
+__device__ __forceinline__ WarpSmem<LPL, V>& warp_smem() {
+  return reinterpret_cast<WarpSmem<LPL, V>*>(gm_dyn_smem)[threadIdx.x >> 5];
+}
+
+template <int LPL, int V>
+constexpr int min_blocks() { return LPL == 1 ? (V == 2 ? 3 : 4) : 2; }
+
 // One warp per pixel, pixels taken from a global cursor until the cube is
-// done (lm_mils, milosUtils.cu:574-710, with its per-thread contiguous pixel
-// slice replaced by work stealing).  The initial point is handled as an
-// accepted step of the same loop, so the synthesis and the response
-// functions each appear once in the code.
-template <int LPL>
-__global__ void __launch_bounds__(warps_per_block<LPL>() * 32, LPL == 1 ? 4 : 2)
+// done (lm_mils, milosUtils.cu:574-710, and lm_mils_11, :713-850, with their
+// per-thread contiguous pixel slices replaced by work stealing).  The
+// initial point is handled as an accepted step of the same loop, so the
+// synthesis and the response functions each appear once in the code.
+template <int LPL, int V>
+__global__ void __launch_bounds__(warps_per_block<LPL>() * 32, min_blocks<LPL, V>())
 invert_kernel(const DevCfg c, const InvertArgs a) {
-  constexpr int WPB = warps_per_block<LPL>();
-  __shared__ WarpSmem<LPL> smem[WPB];
+  constexpr int NT = Variant<V>::NT;
   const int lane = threadIdx.x & 31;
-  WarpSmem<LPL>& sm = smem[threadIdx.x >> 5];
-  zero_padding<LPL>(sm, lane);
+  WarpSmem<LPL, V>& sm = warp_smem<LPL, V>();
+  zero_padding<LPL, V>(sm, lane);
 
   const int nl = c.nl;
   float dlv[LPL];
@@ -56,6 +67,8 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
   }
 
   const SolvePlan plan = make_solve_plan(lane);
+  Solve11Plan plan11;
+  if constexpr (NT == 11) plan11 = make_solve11_plan(lane);
   unsigned long long my_iter = 0, my_acc = 0;
   while (true) {
     unsigned long long pix = 0;
@@ -75,7 +88,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
     if (c.init_mode == 0) st |= classical_warp<LPL>(c, ob, dld, valid, lane, sm.m);
     __syncwarp();
 
-    Lane<LPL> ln;
+    Lane<LPL, V> ln;
     Angles an;
     float syn[LPL][4], pure[LPL][4];
     float flambda = c.ilambda, pbf = 1.f, ochisqr = 0.f, chisqr0 = 0.f;
@@ -83,16 +96,22 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
     bool stop = false, first = true;
     while (true) {
       if (!first) {
-        solve10<LPL>(sm, plan, flambda, lane, c.numerics != 0);
-        if (lane == 0) apply_delta_check(c, sm.m, sm.vec[0], sm.t);
+        if constexpr (NT == 10) {
+          solve10<LPL, V>(sm, plan, flambda, lane, c.numerics != 0);
+          if (lane == 0) apply_delta_check<10>(c, sm.m, sm.vec[0], sm.t);
+        } else {
+          solve11<LPL, V>(sm, plan11, flambda, lane);
+          if (lane == 0) apply_delta_check<11>(c, sm.m, sm.dd, sm.t);
+        }
         __syncwarp();
       }
-      synth_lane<LPL>(c, first ? sm.m : sm.t, dlv, lane, ln, an, syn, pure, slg, sm);
+      synth_lane<LPL, V>(c, first ? sm.m : sm.t, dlv, lane, ln, an, syn, pure, slg, sm);
       const float chisqr = chisq<LPL>(c, syn, ob, valid);
       bool accept = first;
       if (!first) {
         if (iter == 0) {
-          if (a.step_delta && lane < 10) a.step_delta[pix * 10 + lane] = sm.vec[0][lane];
+          if (a.step_delta && lane < NT)
+            a.step_delta[pix * NT + lane] = (NT == 10) ? sm.vec[0][lane] : (float)sm.dd[lane];
           if (a.step_trial && lane < 11) a.step_trial[pix * 11 + lane] = sm.t[lane];
           if (lane == 0 && a.step_chi2_start) a.step_chi2_start[pix] = chisqr0;
           if (lane == 0 && a.step_chi2_trial) a.step_chi2_trial[pix] = chisqr;
@@ -122,9 +141,8 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
       if (accept) {
         // response functions and normal equations at the accepted model; the
         // alpha RF uses the mixed profile after the first step (milosUtils.cu:675)
-        rf_rows<LPL>(c, sm.m, ln, an, lane, sm);
-        if (first || !c.quirks) normal_eq<LPL>(c, sm.m, pure, slg, syn, ob, valid, lane, sm);
-        else normal_eq<LPL>(c, sm.m, syn, slg, syn, ob, valid, lane, sm);
+        rf_rows<LPL, V>(c, sm.m, ln, an, lane, sm);
+        normal_eq<LPL, V>(c, sm.m, !first && c.quirks, pure, slg, syn, ob, valid, lane, sm);
         ochisqr = chisqr;
       }
       if (first) {
@@ -171,15 +189,15 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
 
 // Synthesis (+ response functions) of one model per warp
 // (kernel_synthesis, gmilos.cu:71-84, batched).
-template <int LPL>
+template <int LPL, int V>
 __global__ void __launch_bounds__(warps_per_block<LPL>() * 32)
 synth_kernel(const DevCfg c, const SynthArgs a) {
-  constexpr int WPB = warps_per_block<LPL>();
-  __shared__ WarpSmem<LPL> smem[WPB];
+  constexpr int NT = Variant<V>::NT;
+  const int WPB = warps_per_block<LPL>();
   const int lane = threadIdx.x & 31;
-  WarpSmem<LPL>& sm = smem[threadIdx.x >> 5];
-  zero_padding<LPL>(sm, lane);
-  const int nl = c.nl, nt = c.nterms;
+  WarpSmem<LPL, V>& sm = warp_smem<LPL, V>();
+  zero_padding<LPL, V>(sm, lane);
+  const int nl = c.nl;
   float dlv[LPL];
 #pragma unroll
   for (int k = 0; k < LPL; ++k) {
@@ -201,10 +219,10 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
     if (c.use_slight && c.slight_per_pixel) load_pixel<LPL>(c.slight + off, nl, lane, slg);
     if (lane < 11) sm.m[lane] = a.models_f64 ? a.models_f64[pix * 11 + lane] : (double)a.models_f32[pix * 11 + lane];
     __syncwarp();
-    Lane<LPL> ln;
+    Lane<LPL, V> ln;
     Angles an;
     float syn[LPL][4], pure[LPL][4];
-    synth_lane<LPL>(c, sm.m, dlv, lane, ln, an, syn, pure, slg, sm);
+    synth_lane<LPL, V>(c, sm.m, dlv, lane, ln, an, syn, pure, slg, sm);
 #pragma unroll
     for (int k = 0; k < LPL; ++k) {
       const int l = lane + 32 * k;
@@ -213,8 +231,10 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
         for (int s = 0; s < 4; ++s) a.iquv[off + s * nl + l] = syn[k][s];
     }
     if (a.rf) {
-      rf_rows<LPL>(c, sm.m, ln, an, lane, sm);
-      const size_t roff = (size_t)pix * 4 * nt * nl;
+      rf_rows<LPL, V>(c, sm.m, ln, an, lane, sm);
+      bool mac_on = false;
+      if constexpr (Variant<V>::MAC) mac_on = sm.m[MAC] > 0.0001;
+      const size_t roff = (size_t)pix * 4 * NT * nl;
 #pragma unroll
       for (int k = 0; k < LPL; ++k) {
         const int l = lane + 32 * k;
@@ -222,9 +242,9 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
 #pragma unroll
           for (int s = 0; s < 4; ++s)
 #pragma unroll
-            for (int t = 0; t < 10; ++t)
-              a.rf[roff + ((size_t)s * nt + t) * nl + l] =
-                  gather_rf<LPL>(c, sm, sm.m[ALFA], pure[k][s], slg[k][s], l, s, t);
+            for (int t = 0; t < NT; ++t)
+              a.rf[roff + ((size_t)s * NT + t) * nl + l] =
+                  gather_rf<LPL, V>(c, sm, sm.m[ALFA], pure[k][s], slg[k][s], l, s, t, mac_on);
       }
     }
     __syncwarp();
@@ -306,16 +326,69 @@ cudaError_t launch_peak(int kind, int blocks, int threads, int iters, void* sink
   return cudaGetLastError();
 }
 
-int invert_blocks_per_sm(int nl) {
+// ---------------------------------------------------------------- launchers
+template <int LPL, int V>
+size_t smem_bytes() { return sizeof(WarpSmem<LPL, V>) * warps_per_block<LPL>(); }
+
+template <int LPL, int V>
+cudaError_t prepare_invert() {
+  return cudaFuncSetAttribute(invert_kernel<LPL, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem_bytes<LPL, V>());
+}
+
+template <int LPL, int V>
+int blocks_per_sm_t() {
   int n = 0;
-  if (nl <= 32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, invert_kernel<1>, warps_per_block<1>() * 32, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, invert_kernel<2>, warps_per_block<2>() * 32, 0);
+  if (prepare_invert<LPL, V>() != cudaSuccess) return 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, invert_kernel<LPL, V>, warps_per_block<LPL>() * 32,
+                                                smem_bytes<LPL, V>());
   return n;
 }
 
+int kernel_variant(const DevCfg& cfg, bool per_pixel_init) {
+  if (cfg.nterms == 11) return 2;
+  return (cfg.init[MAC] > 0.0001 || per_pixel_init) ? 1 : 0;
+}
+
+int invert_blocks_per_sm(const DevCfg& cfg, bool per_pixel_init) {
+  const int v = kernel_variant(cfg, per_pixel_init);
+  if (cfg.nl <= 32) {
+    if (v == 0) return blocks_per_sm_t<1, 0>();
+    if (v == 1) return blocks_per_sm_t<1, 1>();
+    return blocks_per_sm_t<1, 2>();
+  }
+  if (v == 0) return blocks_per_sm_t<2, 0>();
+  if (v == 1) return blocks_per_sm_t<2, 1>();
+  return blocks_per_sm_t<2, 2>();
+}
+
+template <int LPL, int V>
+cudaError_t launch_invert_t(const DevCfg& cfg, const InvertArgs& a, int grid, cudaStream_t s) {
+  cudaError_t e = prepare_invert<LPL, V>();
+  if (e != cudaSuccess) return e;
+  invert_kernel<LPL, V><<<grid, warps_per_block<LPL>() * 32, smem_bytes<LPL, V>(), s>>>(cfg, a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_invert(const DevCfg& cfg, const InvertArgs& a, int grid, cudaStream_t s) {
-  if (cfg.nl <= 32) invert_kernel<1><<<grid, warps_per_block<1>() * 32, 0, s>>>(cfg, a);
-  else invert_kernel<2><<<grid, warps_per_block<2>() * 32, 0, s>>>(cfg, a);
+  const int v = kernel_variant(cfg, a.init_models != nullptr);
+  if (cfg.nl <= 32) {
+    if (v == 0) return launch_invert_t<1, 0>(cfg, a, grid, s);
+    if (v == 1) return launch_invert_t<1, 1>(cfg, a, grid, s);
+    return launch_invert_t<1, 2>(cfg, a, grid, s);
+  }
+  if (v == 0) return launch_invert_t<2, 0>(cfg, a, grid, s);
+  if (v == 1) return launch_invert_t<2, 1>(cfg, a, grid, s);
+  return launch_invert_t<2, 2>(cfg, a, grid, s);
+}
+
+template <int LPL, int V>
+cudaError_t launch_synth_t(const DevCfg& cfg, const SynthArgs& a, int grid, cudaStream_t s) {
+  const size_t bytes = sizeof(WarpSmem<LPL, V>) * warps_per_block<LPL>();
+  cudaError_t e = cudaFuncSetAttribute(synth_kernel<LPL, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)bytes);
+  if (e != cudaSuccess) return e;
+  synth_kernel<LPL, V><<<grid, warps_per_block<LPL>() * 32, bytes, s>>>(cfg, a);
   return cudaGetLastError();
 }
 
@@ -326,9 +399,10 @@ cudaError_t launch_synth(const DevCfg& cfg, const SynthArgs& a, cudaStream_t s) 
   int64_t need = (a.npix + warps_for_nl(cfg.nl) - 1) / warps_for_nl(cfg.nl);
   int grid = (int)(need < (int64_t)sms * 16 ? need : (int64_t)sms * 16);
   if (grid < 1) grid = 1;
-  if (cfg.nl <= 32) synth_kernel<1><<<grid, warps_per_block<1>() * 32, 0, s>>>(cfg, a);
-  else synth_kernel<2><<<grid, warps_per_block<2>() * 32, 0, s>>>(cfg, a);
-  return cudaGetLastError();
+  // the synthesis of arbitrary models always takes the macroturbulence-capable code
+  const bool v2 = cfg.nterms == 11;
+  if (cfg.nl <= 32) return v2 ? launch_synth_t<1, 2>(cfg, a, grid, s) : launch_synth_t<1, 1>(cfg, a, grid, s);
+  return v2 ? launch_synth_t<2, 2>(cfg, a, grid, s) : launch_synth_t<2, 1>(cfg, a, grid, s);
 }
 
 cudaError_t launch_synth_grid(const DevCfg& cfg, const double* models, int64_t npix,

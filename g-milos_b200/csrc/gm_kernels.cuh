@@ -30,7 +30,7 @@ struct InvertArgs {
   int* accepted;              // [P] or null
   float* fitted;              // [P][4][nl] or null
   uint32_t* status;           // [P] or null
-  float* step_delta;          // [P][10] first-iteration step, or null
+  float* step_delta;          // [P][nterms] first-iteration step, or null
   double* step_trial;         // [P][11] first-iteration trial model, or null
   float* step_chi2_start;     // [P] chi2 of the starting model, or null
   float* step_chi2_trial;     // [P] chi2 of the first trial, or null
@@ -42,7 +42,7 @@ struct SynthArgs {
   const double* models_f64;
   int64_t npix;
   float* iquv;                // [P][4][nl]
-  float* rf;                  // [P][4][nterms][nl] or null
+  float* rf;                  // [P][4][nterms][nl] or null (nterms 10 or 11)
 };
 
 // launchers (gm_kernels.cu); return the CUDA error of the launch
@@ -50,8 +50,11 @@ cudaError_t launch_invert(const DevCfg& cfg, const InvertArgs& a, int grid, cuda
 cudaError_t launch_synth(const DevCfg& cfg, const SynthArgs& a, cudaStream_t s);
 cudaError_t launch_synth_grid(const DevCfg& cfg, const double* models, int64_t npix,
                               const double* offsets, int ngrid, float* out, cudaStream_t s);
-// resident blocks per SM of the inversion kernel for this nl
-int invert_blocks_per_sm(int nl);
+// kernel variant for a configuration (0: 10 terms, 1: 10 terms with
+// macroturbulence, 2: 11 terms); per_pixel_init: start models given per pixel
+int kernel_variant(const DevCfg& cfg, bool per_pixel_init);
+// resident blocks per SM of the inversion kernel for this configuration
+int invert_blocks_per_sm(const DevCfg& cfg, bool per_pixel_init);
 
 // FMA-issue-bound microbenchmark (kind 0: FP32, 1: FP64); each thread runs
 // kPeakChains independent FMA chains of `iters` steps.

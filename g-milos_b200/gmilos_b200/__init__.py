@@ -264,6 +264,11 @@ class Engine:
     def nl(self):
         return self.cfg.nl
 
+    @property
+    def nterms(self):
+        """Terms of the normal equations: 11 when v_mac and alpha are both free."""
+        return 11 if (self.cfg.fix[9] and self.cfg.fix[10]) else 10
+
     def invert(self, iquv, init_models=None, fitted=False, out=None, stream=None):
         """Invert a cube iquv [P][4][nl] (numpy: host; torch CUDA tensor: device).
 
@@ -305,11 +310,11 @@ class Engine:
         return o
 
     def lm_step(self, iquv, models, flambda):
-        """One LM iteration from explicit states: (delta [P][10], trial [P][11],
+        """One LM iteration from explicit states: (delta [P][nterms], trial [P][11],
         chi2_start [P], chi2_trial [P]) as host numpy arrays."""
         P = int(iquv.shape[0])
         models = np.ascontiguousarray(models, dtype=np.float64)
-        d = np.empty((P, 10), dtype=np.float32)
+        d = np.empty((P, self.nterms), dtype=np.float32)
         t = np.empty((P, NPAR), dtype=np.float64)
         c0 = np.empty(P, dtype=np.float32)
         c1 = np.empty(P, dtype=np.float32)
@@ -318,18 +323,18 @@ class Engine:
         return d, t, c0, c1
 
     def synthesize(self, models, rf=False, stream=None):
-        """Synthesis (+ response functions [P][4][10][nl]) of models [P][11] (float64 or float32)."""
+        """Synthesis (+ response functions [P][4][nterms][nl]) of models [P][11] (float64 or float32)."""
         P = int(models.shape[0])
-        nl = self.nl
+        nl, nt = self.nl, self.nterms
         is_t = hasattr(models, "data_ptr")
         if is_t:
             import torch
             spec = torch.empty((P, 4, nl), dtype=torch.float32, device=models.device)
-            r = torch.empty((P, 4, 10, nl), dtype=torch.float32, device=models.device) if rf else None
+            r = torch.empty((P, 4, nt, nl), dtype=torch.float32, device=models.device) if rf else None
             f64 = models.dtype == torch.float64
         else:
             spec = np.empty((P, 4, nl), dtype=np.float32)
-            r = np.empty((P, 4, 10, nl), dtype=np.float32) if rf else None
+            r = np.empty((P, 4, nt, nl), dtype=np.float32) if rf else None
             f64 = models.dtype == np.float64
         fn = lib().gm_synthesize_f64 if f64 else lib().gm_synthesize
         _check(fn(self._ctx, _ptr(models), P, _ptr(spec), _ptr(r), C.c_void_p(stream) if stream else None),

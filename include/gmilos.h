@@ -170,7 +170,8 @@ gm_status gm_invert_noalloc(const gm_config *cfg, const float *iquv, int64_t npi
                             uint32_t *status, void *stream);
 
 /* One Levenberg-Marquardt iteration from explicit per-pixel states
- * (models [P][11], damping flambda): the step delta [P][10] from the damped
+ * (models [P][11], damping flambda): the step delta [P][nterms] (10, or 11
+ * when v_mac and alpha are both free) from the damped
  * normal equations, the trial model [P][11] after step limits and range
  * checks, and chi2 of the start and trial models (milosUtils.cu:645-660).
  * Any output may be NULL. */

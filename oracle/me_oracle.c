@@ -70,6 +70,54 @@ static void orc_check(double *m)
     if (m[ORC_ALFA] > 1.0) m[ORC_ALFA] = 1.0;
 }
 
+/* Macroturbulence kernel: a Gaussian in wavelength of width
+ * sigma = lambda0 * mac / c, sampled on the grid about its central sample
+ * nl/2 and normalised to unit sum (fgauss, fgauss.cu:16-63). */
+static void orc_fgauss(const orc_cfg *c, double mac, double *g)
+{
+    const int nl = c->nl;
+    const double ild = (c->lambda0 * mac) / 2.99792458e5;
+    const double lc = c->lambda[nl / 2];
+    double sum = 0;
+    for (int i = 0; i < nl; i++) {
+        const double x = (c->lambda[i] - lc) / ild;
+        const double term = (x * x) / 2;
+        g[i] = term < 1e30 ? exp(-term) : 0;
+    }
+    for (int i = 0; i < nl; i++) sum += g[i];
+    for (int i = 0; i < nl; i++) g[i] /= sum;
+}
+
+/* Derivative of the macroturbulence kernel with respect to mac,
+ * g / mac * (x^2 - 1) (me_der.cu:122-129). */
+static void orc_fgauss_deriv(const orc_cfg *c, double mac, const double *g, double *gd)
+{
+    const int nl = c->nl;
+    const double ild = (c->lambda0 * mac) / 2.99792458e5;
+    const double lc = c->lambda[nl / 2];
+    for (int i = 0; i < nl; i++) {
+        const double x = (c->lambda[i] - lc) / ild;
+        gd[i] = g[i] / mac * ((x * x) - 1.0);
+    }
+}
+
+/* In-place same-size correlation of a double vector with the nl-tap PSF
+ * centred at nl/2, zero padded (direct_convolution_double,
+ * convolution.cu:120-151): used to fold the PSF into the macroturbulence
+ * kernels. */
+static void orc_conv_double(double *x, int nl, const double *h)
+{
+    double pad[3 * ORC_MAXNL];
+    const int c = nl / 2;
+    for (int k = 0; k < 2 * nl; k++) pad[k] = 0;
+    for (int k = 0; k < nl; k++) pad[k + c] = x[k];
+    for (int k = 0; k < nl; k++) {
+        double a = 0;
+        for (int j = 0; j < nl; j++) a += h[j] * pad[j + k];
+        x[k] = a;
+    }
+}
+
 /* ---------------- reference-faithful single precision ------------------ */
 #define R float
 #define SFX(n) n##_f
@@ -398,14 +446,24 @@ void orc_lm_step_f(const orc_cfg *c, const double *model, const float *obs,
     float alpha[121], beta[11], covar[121], d10[10];
     double dd[11];
     orc_normal_f(c, model, obs, slight, alpha, beta, chi2_model);
-    for (int i = 0; i < 100; i++) covar[i] = alpha[i];
-    for (int j = 0; j < 10; j++) covar[j * 11] = (float)((double)alpha[j * 11] * (1.0 + (double)flambda));
-    solve10_f(covar, beta, d10);
-    for (int j = 0; j < 10; j++) {
-        delta[j] = d10[j];
-        dd[j] = d10[j];
+    if (c->nterms == 11) {
+        /* the 11-term step in double (milosUtils.cu:787-792) */
+        double cv[121], b11[11];
+        for (int i = 0; i < 121; i++) cv[i] = (double)alpha[i];
+        for (int j = 0; j < 11; j++) cv[j * 12] = (double)alpha[j * 12] * (1.0 + (double)flambda);
+        for (int j = 0; j < 11; j++) b11[j] = (double)beta[j];
+        solve11_f(cv, b11, dd);
+        for (int j = 0; j < 11; j++) delta[j] = (float)dd[j];
+    } else {
+        for (int i = 0; i < 100; i++) covar[i] = alpha[i];
+        for (int j = 0; j < 10; j++) covar[j * 11] = (float)((double)alpha[j * 11] * (1.0 + (double)flambda));
+        solve10_f(covar, beta, d10);
+        for (int j = 0; j < 10; j++) {
+            delta[j] = d10[j];
+            dd[j] = d10[j];
+        }
+        dd[10] = 0;
     }
-    dd[10] = 0;
     for (int i = 0; i < ORC_NPAR; i++) model_trial[i] = model[i];
     apply_delta_f(c, model, dd, model_trial);
     orc_check(model_trial);

@@ -91,7 +91,8 @@ void orc_svdcmp(double *a, int m, int n, double *w, double *v);
 void orc_normal_f(const orc_cfg *c, const double *model, const float *obs,
                   const float *slight, float *alpha, float *beta, float *chi2);
 
-/* one LM iteration from an explicit state (model, lambda_LM) */
+/* one LM iteration from an explicit state (model, lambda_LM); delta holds
+ * nterms entries (10, or 11 for the FP64 11-term step) */
 void orc_lm_step_f(const orc_cfg *c, const double *model, const float *obs,
                    const float *slight, float flambda, float *delta,
                    double *model_trial, float *chi2_trial, float *chi2_model);

@@ -270,7 +270,7 @@ def lm_step_f(cfg, model, obs, flambda, slight=None):
     m = np.ascontiguousarray(model, dtype=np.float64)
     o = np.ascontiguousarray(obs, dtype=np.float32).reshape(-1)
     sl = None if slight is None else np.ascontiguousarray(slight, dtype=np.float32)
-    delta = np.zeros(10, dtype=np.float32)
+    delta = np.zeros(cfg.nterms, dtype=np.float32)
     trial = np.zeros(NPAR)
     c1 = np.zeros(1, dtype=np.float32)
     c0 = np.zeros(1, dtype=np.float32)

@@ -61,7 +61,7 @@ def cpu_lib():
         sp = C.POINTER(Setup)
         fp, dp, ip = C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int)
         L.gmref_cpu_invert.argtypes = [sp, fp, C.c_longlong, fp, C.c_int, dp, fp, ip, fp, C.c_int]
-        L.gmref_cpu_synth.argtypes = [sp, dp, fp, fp, fp]
+        L.gmref_cpu_synth.argtypes = [sp, dp, fp, fp, fp, C.c_int]
         L.gmref_cpu_cuantic.argtypes = [sp, fp]
         L.gmref_cpu_max_threads.restype = C.c_int
         _cpu = L
@@ -120,17 +120,17 @@ def cuantic(setup):
     return out
 
 
-def synth(setup, model, slight=None, rf=False):
+def synth(setup, model, slight=None, rf=False, nterms=10):
     nl = setup.nl
     m = np.ascontiguousarray(model, dtype=np.float64)
     sl = None if slight is None else np.ascontiguousarray(slight, dtype=np.float32)
     spec = np.zeros(4 * nl, dtype=np.float32)
-    r = np.zeros(4 * 10 * nl, dtype=np.float32) if rf else None
+    r = np.zeros(4 * nterms * nl, dtype=np.float32) if rf else None
     if cpu_lib().gmref_cpu_synth(C.byref(setup), _p(m, C.c_double), _p(sl, C.c_float),
-                                 _p(spec, C.c_float), _p(r, C.c_float)):
+                                 _p(spec, C.c_float), _p(r, C.c_float), int(nterms)):
         raise RuntimeError("gmref_cpu_synth failed")
     spec = spec.reshape(4, nl)
-    return (spec, r.reshape(4, 10, nl)) if rf else spec
+    return (spec, r.reshape(4, nterms, nl)) if rf else spec
 
 
 def invert_cpu(setup, obs, slight=None, slight_per_pixel=False, nthreads=0, fitted=False):

@@ -38,7 +38,8 @@ typedef struct gmref_setup {
 
 /* ---- host (OpenMP) build ---- */
 
-/* Invert npix pixels of iquv [P][4][nl].  slight: NULL, one profile [4][nl]
+/* Invert npix pixels of iquv [P][4][nl] with lm_mils, or lm_mils_11 when
+ * fix[9] and fix[10] are both set.  slight: NULL, one profile [4][nl]
  * or, with slight_per_pixel, a map [P][4][nl].  Outputs: model [P][11]
  * (Init_Model layout), chi2 [P], iters [P], fitted [P][4][nl] (may be NULL).
  * nthreads <= 0 uses every OpenMP thread.  Returns 0 on success. */
@@ -47,9 +48,10 @@ int gmref_cpu_invert(const gmref_setup* s, const float* iquv, long long npix,
                      float* chi2, int* iters, float* fitted, int nthreads);
 
 /* Synthesis of one model (kernel_synthesis, gmilos.cu:71-84): profiles
- * [4][nl] and, when rf != NULL, response functions [4][10][nl]. */
+ * [4][nl] and, when rf != NULL, response functions [4][nterms][nl]
+ * (nterms 10 or 11). */
 int gmref_cpu_synth(const gmref_setup* s, const double* model, const float* slight,
-                    float* iquv, float* rf);
+                    float* iquv, float* rf, int nterms);
 
 /* The Zeeman pattern create_cuantic builds for the setup's quantum numbers:
  * out[0..1] = N_PI, N_SIG; out[2..61] = NUB, NUP, NUR, WEB, WEP, WER (10

@@ -164,8 +164,14 @@ extern "C" int gmref_cpu_invert(const gmref_setup* s, const float* iquv, long lo
     const int displ_spectro = 0, count = 1, displ_pixel = 0;
     REAL* sl = nullptr;
     if (slight) sl = (REAL*)(slight_per_pixel ? slight + p * stride : slight);
-    lm_mils(iquv + p * stride, out + p, chi2 + p, sl, iters + p, fit + p * stride,
-            &displ_spectro, &count, &displ_pixel, 1, 0, slight_per_pixel ? 1 : 0);
+    // the reference's main picks the 11-term kernel when both macroturbulence
+    // and the filling factor are free (gmilos.cu:1016-1021, 1233-1240)
+    if (s->fix[9] && s->fix[10])
+      lm_mils_11(iquv + p * stride, out + p, chi2 + p, sl, iters + p, fit + p * stride,
+                 &displ_spectro, &count, &displ_pixel, 1, 0, slight_per_pixel ? 1 : 0);
+    else
+      lm_mils(iquv + p * stride, out + p, chi2 + p, sl, iters + p, fit + p * stride,
+              &displ_spectro, &count, &displ_pixel, 1, 0, slight_per_pixel ? 1 : 0);
   }
   for (long long p = 0; p < npix; ++p) from_model(out[p], model + p * 11);
   free(out);
@@ -174,13 +180,13 @@ extern "C" int gmref_cpu_invert(const gmref_setup* s, const float* iquv, long lo
 }
 
 extern "C" int gmref_cpu_synth(const gmref_setup* s, const double* model_in, const float* slight,
-                               float* iquv, float* rf) {
+                               float* iquv, float* rf, int nterms) {
   std::lock_guard<std::mutex> lock(g_mu);
-  if (upload(s) || !model_in || !iquv) return -1;
+  if (upload(s) || !model_in || !iquv || (nterms != NTERMS && nterms != NTERMS_11)) return -1;
   const int nl = s->nl;
   Init_Model m = to_model(model_in);
   ProfilesMemory* pM = (ProfilesMemory*)malloc(sizeof(ProfilesMemory));
-  InitProfilesMemoryFromDevice(nl, pM, d_cuantic_const, NTERMS);
+  InitProfilesMemoryFromDevice(nl, pM, d_cuantic_const, nterms);
   REAL cosi, sinis, sina, cosa, sinda, cosda, sindi, cosdi, cosis_2;
   int uuGlobal, FGlobal, HGlobal;
   REAL* spectra = (REAL*)calloc(4 * nl, sizeof(REAL));
@@ -193,8 +199,8 @@ extern "C" int gmref_cpu_synth(const gmref_setup* s, const double* model_in, con
     me_der(&d_cuantic_const, &m, d_wlines_const, nl, pM->d_spectra, pM->spectra_mac,
            pM->spectra_slight, d_ah_const, (const REAL*)slight, d_use_convolution_const, pM,
            d_fix_const, cosi, sinis, sina, cosa, sinda, cosda, sindi, cosdi, cosis_2, &uuGlobal,
-           &FGlobal, &HGlobal, NTERMS);
-    for (int i = 0; i < 4 * NTERMS * nl; ++i) rf[i] = pM->d_spectra[i];
+           &FGlobal, &HGlobal, nterms);
+    for (int i = 0; i < 4 * nterms * nl; ++i) rf[i] = pM->d_spectra[i];
   }
   free(spectra);
   FreeProfilesMemoryFromDevice(pM, d_cuantic_const);

@@ -182,6 +182,8 @@ extern "C" int gmref_gpu_invert(const gmref_setup* s, const float* iquv, long lo
   cudaEvent_t e0 = nullptr, e1 = nullptr, start = nullptr, stop = nullptr;
   std::vector<Init_Model> h_models;
   int num_blocks = 0, nrte = 0, map_slight = 0, rc = -1;
+  bool use11 = false;
+  const void* kern = nullptr;
   size_t heap_need = 0, heap_now = 0, stack_now = 0;
   unsigned zero = 0, failures = 0;
   cudaFuncAttributes attr;
@@ -189,9 +191,10 @@ extern "C" int gmref_gpu_invert(const gmref_setup* s, const float* iquv, long lo
   const size_t cube_bytes = sizeof(float) * (size_t)per_pix * P;
 
   GMREF_CHECK(upload(s));
-  GMREF_CHECK(cudaFuncGetAttributes(&attr, (const void*)lm_mils));
-  GMREF_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&num_blocks, (const void*)lm_mils,
-                                                            kThreadsPerBlock, 0));
+  use11 = s->fix[9] && s->fix[10];   // gmilos.cu:1016-1021
+  kern = use11 ? (const void*)lm_mils_11 : (const void*)lm_mils;
+  GMREF_CHECK(cudaFuncGetAttributes(&attr, kern));
+  GMREF_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&num_blocks, kern, kThreadsPerBlock, 0));
   nrte = num_blocks * kThreadsPerBlock;
   rep->num_blocks = num_blocks;
   rep->threads_per_block = kThreadsPerBlock;
@@ -276,10 +279,16 @@ extern "C" int gmref_gpu_invert(const gmref_setup* s, const float* iquv, long lo
   GMREF_CHECK(cudaMemcpy(d_displs_pix, displs_pix.data(), sizeof(int) * counts.size(),
                          cudaMemcpyHostToDevice));
   GMREF_CHECK(cudaEventRecord(start, 0));
-  for (int i = 0; i < nstreams; ++i)
-    lm_mils<<<num_blocks, kThreadsPerBlock, 0, streams[i]>>>(
-        d_spectro, d_models, d_chi2, d_slight, d_iter, d_fit, d_displs_spectro, d_counts,
-        d_displs_pix, nrte, i, map_slight);
+  for (int i = 0; i < nstreams; ++i) {
+    if (use11)
+      lm_mils_11<<<num_blocks, kThreadsPerBlock, 0, streams[i]>>>(
+          d_spectro, d_models, d_chi2, d_slight, d_iter, d_fit, d_displs_spectro, d_counts,
+          d_displs_pix, nrte, i, map_slight);
+    else
+      lm_mils<<<num_blocks, kThreadsPerBlock, 0, streams[i]>>>(
+          d_spectro, d_models, d_chi2, d_slight, d_iter, d_fit, d_displs_spectro, d_counts,
+          d_displs_pix, nrte, i, map_slight);
+  }
   GMREF_CHECK(cudaGetLastError());
   GMREF_CHECK(cudaEventRecord(stop, 0));
   GMREF_CHECK(cudaEventSynchronize(stop));

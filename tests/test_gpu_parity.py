@@ -310,11 +310,17 @@ def test_reference_numerics_fit_quality(engine, psf):
     assert abs(out["iters"].mean() - ir.mean()) < 2.0
 
 
-def test_unsupported_configurations_are_errors(engine):
-    _, gcfg, _ = configs(fix=(1,) * 11)
+def test_invalid_configurations_are_errors(engine):
+    _, gcfg, _ = configs()
+    gcfg.noise = 0.0
     with pytest.raises(G.GmError) as e:
         engine.configure(gcfg)
-    assert e.value.status == 5
+    assert e.value.status == 1
+    _, gcfg, _ = configs()
+    gcfg.numerics = 7
+    with pytest.raises(G.GmError) as e:
+        engine.configure(gcfg)
+    assert e.value.status == 1
 
 
 def test_grid_synthesis_matches_synthesis(engine):

@@ -99,3 +99,35 @@ def test_inversions_match_reference_gpu_build(engine):
     assert agree.mean() >= 0.75
     assert worse_g.mean() <= worse_r.mean() + 0.01
     assert rec_g >= rec_r - 0.01
+
+
+@pytest.mark.skipif(not ref.available(), reason="libgmref_cpu.so not built")
+@pytest.mark.parametrize("fix", [FIX, (1,) * 11])
+def test_macroturbulence_iteration_matches_reference_host_build(engine, fix):
+    """One iteration with macroturbulence: the fixed-v_mac 10-term path and
+    the 11-term path (lm_mils_11, FP64 step) against the reference's host
+    build, ACCURATE numerics."""
+    lam, _ = H.grid(30)
+    l0, zo = H.fe_line()
+    zg = G.zeeman_from_levels(2, 1, 1.0, 2, 2, 0.0, 1.0)
+    p = O.psf_gauss(100.0, lam)
+    init = list(H.GUESS)
+    init[9] = 0.5
+    ocfg = O.make_cfg(lam, l0, zo, psf=p, fix=fix, init=init, miter=1)
+    sl = H.stray_profile(ocfg)
+    gcfg = G.make_config(lam, l0, zg, psf=p, fix=fix, init=init, slight=sl, miter=1,
+                         numerics=G.NUMERICS_ACCURATE)
+    rng = np.random.default_rng(23 + sum(fix))
+    t = H.truth_models(1024, rng, alpha_range=(0.7, 1.0))
+    t[:, 9] = rng.uniform(0.3, 2.0, len(t))
+    obs = H.observations(ocfg, t, rng, slight=sl)
+    engine.configure(gcfg)
+    out = engine.invert(obs)
+    mr, cr, ir, _ = ref.invert_cpu(ref.setup_from_cfg(ocfg), obs, slight=sl)
+    rel = np.abs(out["model64"] - mr) / np.maximum(np.abs(mr), 1e-3)
+    crel = np.abs(out["chi2"] - cr) / cr
+    print("v_mac one iteration (%d terms): model rel p99 %.2e, chi2 rel p99 %.2e"
+          % (engine.nterms, np.percentile(rel, 99), np.percentile(crel, 99)))
+    assert (out["iters"] == ir).all()
+    assert np.percentile(rel, 99) < 1e-4
+    assert np.percentile(crel, 99) < 1e-4

@@ -132,3 +132,59 @@ def test_per_pixel_stray_map_matches_reference():
     close = np.abs(mr[:, 1] - mo[:, 1]) < 1.0
     assert close.mean() >= 0.95
     assert ((co <= cr * (1 + 1e-3)) | close).mean() >= 0.99
+
+
+# ---------------------------------------------------------------- macroturbulence
+def mac_cfg(psf, stray, nt, miter=50):
+    lam, _ = H.grid(30)
+    l0, z = H.fe_line()
+    p = O.psf_gauss(100.0, lam) if psf else None
+    fix = (1,) * 11 if nt == 11 else (1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 1 if stray else 0)
+    init = list(H.GUESS)
+    init[9] = 0.5
+    cfg = O.make_cfg(lam, l0, z, psf=p, fix=fix, init=init, miter=miter)
+    sl = H.stray_profile(cfg) if stray else None
+    return cfg, sl
+
+
+@pytest.mark.parametrize("psf,stray,nt", [(False, False, 10), (True, True, 10), (False, True, 11),
+                                          (True, True, 11)])
+def test_oracle_macroturbulence_matches_reference(psf, stray, nt):
+    """fgauss + convCircular (+ PSF folded into the kernel) and the v_mac RF."""
+    cfg, sl = mac_cfg(psf, stray, nt)
+    s = ref.setup_from_cfg(cfg)
+    rng = np.random.default_rng(31)
+    truth = H.truth_models(16, rng, alpha_range=(0.7, 1.0) if stray else None)
+    truth[:, 9] = rng.uniform(0.3, 3.0, 16)
+    cols = list(range(9)) + ([9] if (stray or nt == 11) else []) + ([10] if nt == 11 else [])
+    for m in truth:
+        sr, rr = ref.synth(s, m, slight=sl, rf=True, nterms=nt)
+        so, ro = O.synth_f(cfg, m, slight=sl, rf=True)
+        assert H.rel_to_I(so, sr).max() < 1e-6
+        assert H.rf_rel(ro[:, cols], rr[:, cols]).max() < 1e-5
+
+
+@pytest.mark.parametrize("psf,nt", [(False, 10), (True, 10), (False, 11), (True, 11)])
+def test_macroturbulence_inversions_match_reference(psf, nt):
+    """lm_mils with a fixed v_mac and lm_mils_11 (FP64 Golub-Reinsch step):
+    one iteration to 1e-4 (p99), full inversions agreeing on >= 97 %."""
+    rng = np.random.default_rng(41 + nt)
+    for miter in (1, 50):
+        cfg, sl = mac_cfg(psf, True, nt, miter=miter)
+        s = ref.setup_from_cfg(cfg)
+        truth = H.truth_models(256, rng, alpha_range=(0.7, 1.0))
+        truth[:, 9] = rng.uniform(0.3, 2.0, 256)
+        obs = H.observations(cfg, truth, rng, slight=sl)
+        mr, cr, ir, _ = ref.invert_cpu(s, obs, slight=sl)
+        mo, co, io, _, _ = O.lm_batch_f(cfg, obs, slight=sl)
+        if miter == 1:
+            assert (ir == io).all()
+            rel = np.abs(mr - mo) / np.maximum(np.abs(mo), 1e-3)
+            assert np.percentile(rel, 99) < 1e-4
+        else:
+            # where the FP32 trajectories part, neither side is systematically better
+            close = np.abs(mr[:, 1] - mo[:, 1]) < 1.0
+            assert close.mean() >= 0.97
+            worse_o = (~close & (co > cr * (1 + 1e-3))).mean()
+            worse_r = (~close & (cr > co * (1 + 1e-3))).mean()
+            assert worse_o <= worse_r + 0.01
