@@ -36,7 +36,7 @@ LAMBDA0 = 6173.3356
 GRID = (-350.0, 35.0, 665.0)
 FWHM_MA = 100.0
 NOISE = 1e-3
-GUESS = (1.0, 1000.0, 0.2, 0.03, 0.05, 150.0, 110.0, 0.35, 0.5, 0.0, 1.0)
+GUESS = (40.0, 1000.0, 0.2, 0.03, 0.05, 150.0, 110.0, 0.35, 0.5, 0.0, 1.0)   # run/guess.mod
 FIX = (1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 1)          # 9 ME parameters + alpha
 STRAY_MODEL = (10.0, 0.0, 0.0, 0.03, 0.1, 0.0, 0.0, 0.3, 0.7, 0.0, 1.0)
 MAXITER = 50

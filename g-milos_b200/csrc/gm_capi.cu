@@ -243,7 +243,8 @@ void gm_config_defaults(gm_config* c) {
   c->miter = 50;
   c->init_mode = GM_INIT_CLASSICAL;
   c->reference_quirks = 1;
-  const double guess[GM_NPAR] = {1.0, 1000.0, 0.2, 0.03, 0.05, 150.0, 110.0, 0.35, 0.5, 0.0, 1.0};
+  // the values of the reference's run/guess.mod (eta_0 40, B 1000 G, ...)
+  const double guess[GM_NPAR] = {40.0, 1000.0, 0.2, 0.03, 0.05, 150.0, 110.0, 0.35, 0.5, 0.0, 1.0};
   for (int i = 0; i < GM_NPAR; ++i) c->init_model[i] = guess[i];
 }
 
@@ -531,6 +532,30 @@ gm_status gm_synthesize_grid(gm_ctx* ctx, const double* models, int64_t npix, co
   if (a_out.host || a_m.dev != (const void*)models || !stream) {
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "grid synthesis");
+  }
+  return GM_OK;
+}
+
+gm_status gm_classical(gm_ctx* ctx, const float* iquv, int64_t npix, int nl, double* models,
+                       void* stream) {
+  if (!ctx) return GM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->call_mu);
+  if (!ctx->configured) return fail(ctx, GM_ERR_NOT_CONFIGURED, "gm_configure first");
+  if (!iquv || !models || npix < 0) return fail(ctx, GM_ERR_INVALID, "bad argument");
+  if (nl != ctx->dev.nl) return fail(ctx, GM_ERR_INVALID, "nl differs from the configured grid");
+  if (npix == 0) return GM_OK;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  Arg a_in, a_out;
+  gm_status st;
+  if ((st = stage_in(ctx, "iquv", iquv, sizeof(float) * 4 * (size_t)nl * npix, &a_in, s)) != GM_OK) return st;
+  if ((st = stage_out(ctx, "cmodels", models, sizeof(double) * 11 * npix, &a_out)) != GM_OK) return st;
+  cudaError_t e = gm::launch_classical(ctx->dev, (const float*)a_in.dev, npix, (double*)a_out.dev, s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "classical-estimates launch");
+  if ((st = copy_back(ctx, a_out, s)) != GM_OK) return st;
+  if (a_out.host || a_in.dev != (const void*)iquv || !stream) {
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "classical estimates");
   }
   return GM_OK;
 }

@@ -1173,12 +1173,15 @@ __device__ __forceinline__ void apply_delta_check(const DevCfg& c, const double*
 }
 
 // Weak-field and centre-of-gravity estimates of B, vlos, gamma, phi
-// (estimacionesClasicas, milosUtils.cu:386-563) with the NaN fallbacks of
-// lm_mils (:621-628).  Sums are warp reductions in double.  Lane 0 writes m.
+// (estimacionesClasicas, milosUtils.cu:386-563).  Sums are warp reductions in
+// double.  Lane 0 writes m.  for_init (the LM start): gamma in (85, 95]
+// degrees is moved off 90 before B is formed, and lm_mils' NaN fallbacks
+// follow (:621-628); otherwise (the classical-estimates mode,
+// gmilos.cu:383-404) S0 receives the longitudinal field.
 template <int LPL>
 __device__ __forceinline__ uint32_t classical_warp(const DevCfg& c, const float (&ob)[LPL][4],
                                                    const double (&dld)[LPL], const bool (&valid)[LPL],
-                                                   int lane, double* m) {
+                                                   int lane, double* m, bool for_init = true) {
   const int nl = c.nl;
   int bmin = nl, emax = 0;
 #pragma unroll
@@ -1248,8 +1251,10 @@ __device__ __forceinline__ uint32_t classical_warp(const DevCfg& c, const float 
   const double tg = fabs(sqrt(x3 / y3));
   double grad = atan(tg);
   double gamma = grad * (180 / kPi);
-  if (gamma >= 85 && gamma <= 90) grad = 85 * (kPi / 180);
-  if (gamma > 90 && gamma <= 95) grad = 95 * (kPi / 180);
+  if (for_init) {
+    if (gamma >= 85 && gamma <= 90) grad = 85 * (kPi / 180);
+    if (gamma > 90 && gamma <= 95) grad = 95 * (kPi / 180);
+  }
   if (Blos < 0) gamma = (180) - gamma;
   double phi = (atan(su / sq) * 180 / kPi) / 2;
   if (su > 0 && sq > 0) {
@@ -1264,15 +1269,18 @@ __device__ __forceinline__ uint32_t classical_warp(const DevCfg& c, const float 
   if (Vlos < -4) Vlos = -4;
   if (Vlos > 4) Vlos = 4;
   double B = (Baux > 4000 ? 4000 : Baux);
-  if (isnan(B)) { B = 1; st |= 0x01u; }
-  if (isnan(Vlos)) { Vlos = 1e-3; st |= 0x01u; }
-  if (isnan(gamma)) { gamma = 1; st |= 0x01u; }
-  if (isnan(phi)) { phi = 1; st |= 0x01u; }
+  if (for_init) {
+    if (isnan(B)) { B = 1; st |= 0x01u; }
+    if (isnan(Vlos)) { Vlos = 1e-3; st |= 0x01u; }
+    if (isnan(gamma)) { gamma = 1; st |= 0x01u; }
+    if (isnan(phi)) { phi = 1; st |= 0x01u; }
+  }
   if (lane == 0) {
     m[BFLD] = B;
     m[VLOS] = Vlos;
     m[GM] = gamma;
     m[AZ] = phi;
+    if (!for_init) m[S0] = Blos;
   }
   return st;
 }

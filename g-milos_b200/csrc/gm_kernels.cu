@@ -251,6 +251,47 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
   }
 }
 
+// Classical estimates only, one warp per pixel: the configured guess model
+// with B, vlos, gamma, phi from the weak-field / centre-of-gravity estimates
+// and S0 = B_los (the reference's classical-estimates mode,
+// gmilos.cu:383-404).
+template <int LPL>
+__global__ void __launch_bounds__(128) classical_kernel(const DevCfg c, const float* __restrict__ iquv,
+                                                        int64_t npix, double* __restrict__ models) {
+  __shared__ double ms[4][11];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nl = c.nl;
+  double dld[LPL];
+  bool valid[LPL];
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+    valid[k] = l < nl;
+    dld[k] = valid[k] ? c.dld[l] : 0.0;
+  }
+  const int64_t nw = (int64_t)gridDim.x * 4;
+  for (int64_t pix = (int64_t)blockIdx.x * 4 + w; pix < npix; pix += nw) {
+    float ob[LPL][4];
+    load_pixel<LPL>(iquv + (size_t)pix * 4 * nl, nl, lane, ob);
+    if (lane < 11) ms[w][lane] = c.init[lane];
+    __syncwarp();
+    classical_warp<LPL>(c, ob, dld, valid, lane, ms[w], false);
+    __syncwarp();
+    if (lane < 11) models[pix * 11 + lane] = ms[w][lane];
+    __syncwarp();
+  }
+}
+
+cudaError_t launch_classical(const DevCfg& cfg, const float* iquv, int64_t npix, double* models,
+                             cudaStream_t s) {
+  int64_t blocks = (npix + 3) / 4;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  if (cfg.nl <= 32) classical_kernel<1><<<(int)blocks, 128, 0, s>>>(cfg, iquv, npix, models);
+  else classical_kernel<2><<<(int)blocks, 128, 0, s>>>(cfg, iquv, npix, models);
+  return cudaGetLastError();
+}
+
 // Pure ME profiles (no PSF, no stray light) on an arbitrary offset grid, one
 // thread per (pixel, sample): used to synthesise observations on fine grids.
 __global__ void synth_grid_kernel(const DevCfg c, const double* __restrict__ models, int64_t npix,

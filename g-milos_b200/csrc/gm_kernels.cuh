@@ -48,6 +48,8 @@ struct SynthArgs {
 // launchers (gm_kernels.cu); return the CUDA error of the launch
 cudaError_t launch_invert(const DevCfg& cfg, const InvertArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_synth(const DevCfg& cfg, const SynthArgs& a, cudaStream_t s);
+cudaError_t launch_classical(const DevCfg& cfg, const float* iquv, int64_t npix, double* models,
+                             cudaStream_t s);
 cudaError_t launch_synth_grid(const DevCfg& cfg, const double* models, int64_t npix,
                               const double* offsets, int ngrid, float* out, cudaStream_t s);
 // kernel variant for a configuration (0: 10 terms, 1: 10 terms with

@@ -37,7 +37,7 @@ EXPORTS = ("gm_create", "gm_destroy", "gm_last_error", "gm_status_string", "gm_c
            "gm_configure", "gm_invert", "gm_invert_ex", "gm_synthesize", "gm_synthesize_f64",
            "gm_synthesize_grid", "gm_lm_step", "gm_submit", "gm_poll", "gm_cancel", "gm_zeeman_from_levels",
            "gm_psf_gaussian", "gm_psf_from_table", "gm_get_stats", "gm_measure_peaks",
-           "gm_invert_noalloc")
+           "gm_invert_noalloc", "gm_classical")
 
 
 class GmError(RuntimeError):
@@ -103,6 +103,7 @@ def lib():
         L.gm_synthesize.argtypes = [vp, vp, i64, vp, vp, vp]
         L.gm_synthesize_f64.argtypes = [vp, vp, i64, vp, vp, vp]
         L.gm_synthesize_grid.argtypes = [vp, vp, i64, vp, C.c_int, vp, vp]
+        L.gm_classical.argtypes = [vp, vp, i64, C.c_int, vp, vp]
         L.gm_submit.argtypes = [vp, C.POINTER(Request), C.POINTER(C.c_uint64)]
         L.gm_poll.argtypes = [vp, C.c_uint64, C.c_int]
         L.gm_cancel.argtypes = [vp, C.c_uint64]
@@ -352,6 +353,13 @@ class Engine:
             out = np.empty((P, 4, n), dtype=np.float32)
         _check(lib().gm_synthesize_grid(self._ctx, _ptr(models), P, _ptr(offsets_A), n, _ptr(out),
                                         C.c_void_p(stream) if stream else None), self._ctx)
+        return out
+
+    def classical(self, iquv):
+        """Classical estimates only (the NumberOfCycles < 0 mode): models [P][11] f64."""
+        P = int(iquv.shape[0])
+        out = np.empty((P, NPAR), dtype=np.float64)
+        _check(lib().gm_classical(self._ctx, _ptr(iquv), P, self.nl, _ptr(out), None), self._ctx)
         return out
 
     def submit(self, iquv, model, chi2=None, iters=None, status=None, fix=None):

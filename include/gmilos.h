@@ -184,6 +184,13 @@ gm_status gm_lm_step(gm_ctx *ctx, const float *iquv, int64_t npix, int nl,
  * with nterms = 10 (11 when both vmac and alpha are free). */
 gm_status gm_synthesize(gm_ctx *ctx, const float *models, int64_t npix, float *iquv,
                         float *rf, void *stream);
+/* Classical estimates only (the reference's NumberOfCycles < 0 mode,
+ * gmilos.cu:309-431): models [P][11] (Init_Model layout) = the configured
+ * guess model with B, vlos, gamma, phi from the weak-field and
+ * centre-of-gravity estimates (estimacionesClasicas, milosUtils.cu:386-563,
+ * non-initialisation use) and S0 = the longitudinal field. */
+gm_status gm_classical(gm_ctx *ctx, const float *iquv, int64_t npix, int nl, double *models,
+                       void *stream);
 gm_status gm_synthesize_f64(gm_ctx *ctx, const double *models, int64_t npix, float *iquv,
                             float *rf, void *stream);
 

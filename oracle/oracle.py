@@ -167,7 +167,7 @@ def make_cfg(lam, lambda0, zeeman, psf=None, mu=1.0, weight=(1, 1, 1, 1), noise=
     for i in range(NPAR):
         c.fix[i] = int(fix[i])
     if init is None:
-        init = (1.0, 1000.0, 0.2, 0.03, 0.05, 150.0, 110.0, 0.35, 0.5, 0.0, 1.0)
+        init = (40.0, 1000.0, 0.2, 0.03, 0.05, 150.0, 110.0, 0.35, 0.5, 0.0, 1.0)   # run/guess.mod
     for i in range(NPAR):
         c.init[i] = init[i]
     c.miter = miter

@@ -3,7 +3,7 @@ import numpy as np
 
 import oracle as O
 
-GUESS = (1.0, 1000.0, 0.2, 0.03, 0.05, 150.0, 110.0, 0.35, 0.5, 0.0, 1.0)   # run/guess.mod
+GUESS = (40.0, 1000.0, 0.2, 0.03, 0.05, 150.0, 110.0, 0.35, 0.5, 0.0, 1.0)   # run/guess.mod
 FREE9 = (1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0)
 
 

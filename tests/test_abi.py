@@ -33,6 +33,16 @@ def test_library_exports_every_declared_function():
         assert re.search(r"\bT %s\b" % n, out), n
 
 
+def test_library_exports_every_file_format_function():
+    txt = open(os.path.join(ROOT, "include", "gmilos_io.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    names = sorted(set(re.findall(r"\b(gm_(?:io|fits)_[a-z0-9_]+)\s*\(", txt)))
+    assert len(names) >= 20, names
+    out = subprocess.run(["nm", "-D", "--defined-only", G.LIB_PATH], capture_output=True, text=True).stdout
+    for n in names:
+        assert re.search(r"\bT %s\b" % n, out), n
+
+
 def test_status_strings():
     lib = G.lib()
     assert lib.gm_status_string(0) == b"ok"
