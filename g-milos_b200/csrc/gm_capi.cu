@@ -26,12 +26,39 @@ struct DevBuf {
   size_t bytes = 0;
 };
 
+using Clock = std::chrono::steady_clock;
+
+// One inversion request of the serving path: its configuration snapshot, its
+// device buffers (the caller's when it passed device memory), and how far its
+// chunks have been launched and completed.
 struct Request {
   gm_request req;
-  std::vector<int> fix;
+  gm::DevCfg dev{};
   gm_status result = GM_OK;
   bool done = false;
   bool cancelled = false;
+  bool admitted = false;
+  // device views: input cube and outputs (owned when the caller's are host memory)
+  float* d_in = nullptr;
+  float* d_model = nullptr;
+  float* d_chi2 = nullptr;
+  int* d_iters = nullptr;
+  uint32_t* d_status = nullptr;
+  std::vector<void*> owned;
+  size_t bytes = 0;          // device memory charged to the HBM budget
+  int64_t next = 0;          // first pixel not yet launched
+  int outstanding = 0;       // launched chunks not yet complete
+  Clock::time_point t_submit, t_start;
+  bool started = false;
+};
+
+// A serving lane: a stream with its own work counters and one chunk in flight.
+struct ServeLane {
+  cudaStream_t stream = nullptr;
+  gm::WorkCounters* work = nullptr;
+  cudaEvent_t done = nullptr;
+  std::shared_ptr<Request> req;
+  bool busy = false;
 };
 
 }  // namespace
@@ -50,15 +77,22 @@ struct gm_ctx {
   std::map<std::string, DevBuf> bufs; // staging buffers for host-memory calls
   std::string err;
   gm_stats stats{};
-  // serving
+  // serving: continuous batching over `serve_streams` lanes
   std::mutex mu;
   std::condition_variable cv, done_cv;
-  std::deque<gm_ticket> queue;
+  std::deque<gm_ticket> queue;        // submitted, not yet admitted
   std::map<gm_ticket, std::shared_ptr<Request>> reqs;
+  std::vector<std::shared_ptr<Request>> active;   // admitted, chunks pending or in flight
+  std::vector<ServeLane> lanes;
+  size_t serve_bytes = 0;             // device memory held by admitted requests
+  int serve_streams = 4;
+  int64_t serve_chunk = 65536;        // pixels per launch
+  int serve_max_active = 16;
+  size_t rr = 0;                      // round-robin cursor over active requests
   gm_ticket next_ticket = 1;
   std::thread worker;
   bool stopping = false;
-  std::mutex call_mu;                 // serialises engine calls of the worker and the caller
+  std::mutex call_mu;                 // serialises the synchronous entry points
 };
 
 namespace {
@@ -596,17 +630,89 @@ gm_status gm_measure_peaks(gm_ctx* ctx, double* fp32_tflops, double* fp64_tflops
   return GM_OK;
 }
 
+}  // extern "C"
+
 // ---------------------------------------------------------------- serving
-// Requests are queued and run by one worker thread in arrival order; each
-// runs as its own persistent launch on the context stream.
+// Continuous batching.  Submitted requests wait in a FIFO until they fit:
+// at most serve_max_active admitted at a time and their device memory
+// within the context's HBM budget.  Admitted requests are cut into chunks
+// of serve_chunk pixels; a dispatcher thread keeps each of serve_streams
+// lanes (a stream with its own work counters) busy with the next chunk of
+// the admitted requests in round-robin order, so chunks of different
+// requests overlap on the device and a newly admitted request starts within
+// one chunk time.  Pixels are independent, so every result is the same
+// whatever the mix it ran in.
+namespace {
+
+size_t request_bytes(const gm_request& q) {
+  const size_t P = (size_t)q.npix;
+  size_t b = 0;
+  if (!is_device_ptr(q.iquv)) b += sizeof(float) * 4 * (size_t)q.nl * P;
+  if (!is_device_ptr(q.model)) b += sizeof(float) * 11 * P;
+  if (q.chi2 && !is_device_ptr(q.chi2)) b += sizeof(float) * P;
+  if (q.iters && !is_device_ptr(q.iters)) b += sizeof(int) * P;
+  if (q.status && !is_device_ptr(q.status)) b += sizeof(uint32_t) * P;
+  return b;
+}
+
+template <typename T>
+bool device_view(Request& r, T* user, size_t bytes, T** out) {
+  if (!user) {
+    *out = nullptr;
+    return true;
+  }
+  if (is_device_ptr(user)) {
+    *out = user;
+    return true;
+  }
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  r.owned.push_back(p);
+  *out = (T*)p;
+  return true;
+}
+
+void release(Request& r) {
+  for (void* p : r.owned) cudaFree(p);
+  r.owned.clear();
+}
+
+void serve_loop(gm_ctx* ctx);
+
+}  // namespace
+
+extern "C" {
+
+gm_status gm_serving_options(gm_ctx* ctx, int streams, int64_t chunk_pixels, int max_active) {
+  if (!ctx || streams < 1 || streams > 32 || chunk_pixels < 1 || max_active < 1) return GM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!ctx->lanes.empty()) return fail(ctx, GM_ERR_INVALID, "serving already started");
+  ctx->serve_streams = streams;
+  ctx->serve_chunk = chunk_pixels;
+  ctx->serve_max_active = max_active;
+  return GM_OK;
+}
+
 gm_status gm_submit(gm_ctx* ctx, const gm_request* req, gm_ticket* ticket) {
   if (!ctx || !req || !ticket) return GM_ERR_INVALID;
   if (!ctx->configured) return fail(ctx, GM_ERR_NOT_CONFIGURED, "gm_configure first");
   if (!req->iquv || !req->model || req->npix < 0 || req->nl != ctx->dev.nl)
     return fail(ctx, GM_ERR_INVALID, "bad request");
+  if (ctx->dev.use_slight && ctx->dev.slight_per_pixel)
+    return fail(ctx, GM_ERR_UNSUPPORTED, "serving takes one stray-light profile, not a per-pixel map");
   auto r = std::make_shared<Request>();
   r->req = *req;
-  if (req->fix) r->fix.assign(req->fix, req->fix + GM_NPAR);
+  r->dev = ctx->dev;
+  if (req->fix) {
+    for (int i = 0; i < GM_NPAR; ++i) r->dev.fix[i] = req->fix[i] ? 1 : 0;
+    r->dev.nterms = (r->dev.fix[9] && r->dev.fix[10]) ? 11 : 10;
+  }
+  r->bytes = request_bytes(*req);
+  if (r->bytes > ctx->budget) return fail(ctx, GM_ERR_NOMEM, "request exceeds the context's HBM budget");
+  r->t_submit = Clock::now();
   std::lock_guard<std::mutex> lk(ctx->mu);
   if (!ctx->worker.joinable()) ctx->worker = std::thread(serve_loop, ctx);
   const gm_ticket t = ctx->next_ticket++;
@@ -636,7 +742,7 @@ gm_status gm_cancel(gm_ctx* ctx, gm_ticket ticket) {
   auto it = ctx->reqs.find(ticket);
   if (it == ctx->reqs.end()) return fail(ctx, GM_ERR_INVALID, "unknown ticket");
   auto q = std::find(ctx->queue.begin(), ctx->queue.end(), ticket);
-  if (q != ctx->queue.end()) {
+  if (q != ctx->queue.end()) {   // not admitted yet: nothing of it runs
     ctx->queue.erase(q);
     it->second->cancelled = true;
     it->second->done = true;
@@ -649,35 +755,167 @@ gm_status gm_cancel(gm_ctx* ctx, gm_ticket ticket) {
 
 namespace {
 
+// Launch the next chunk of r on lane L (dispatcher thread only).
+gm_status launch_chunk(gm_ctx* ctx, ServeLane& L, const std::shared_ptr<Request>& rp) {
+  Request& r = *rp;
+  const gm_request& q = r.req;
+  const int nl = q.nl;
+  const int64_t off = r.next;
+  const int64_t n = std::min<int64_t>(ctx->serve_chunk, q.npix - off);
+  const size_t row = 4 * (size_t)nl;
+  cudaStream_t s = L.stream;
+  cudaError_t e = cudaSuccess;
+  if ((const void*)r.d_in != (const void*)q.iquv)
+    e = cudaMemcpyAsync(r.d_in + off * row, q.iquv + off * row, sizeof(float) * row * n,
+                        cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(L.work, 0, sizeof(gm::WorkCounters), s);
+  if (e != cudaSuccess) return GM_ERR_CUDA;
+  gm::InvertArgs ia{};
+  ia.iquv = r.d_in + off * row;
+  ia.npix = n;
+  ia.model = r.d_model + off * 11;
+  ia.chi2 = r.d_chi2 ? r.d_chi2 + off : nullptr;
+  ia.iters = r.d_iters ? r.d_iters + off : nullptr;
+  ia.status = r.d_status ? r.d_status + off : nullptr;
+  ia.work = L.work;
+  const int per_sm = std::max(1, gm::invert_blocks_per_sm(r.dev, false));
+  int64_t grid = (int64_t)per_sm * ctx->sms;
+  const int64_t needed = (n + gm::warps_for_nl(nl) - 1) / gm::warps_for_nl(nl);
+  if (grid > needed) grid = needed;
+  e = gm::launch_invert(r.dev, ia, (int)grid, s);
+  if (e != cudaSuccess) return GM_ERR_CUDA;
+  auto back = [&](void* host, const void* dev, size_t bytes) {
+    if (e == cudaSuccess && host && host != dev) e = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, s);
+  };
+  back(q.model + off * 11, r.d_model + off * 11, sizeof(float) * 11 * n);
+  if (q.chi2) back(q.chi2 + off, r.d_chi2 + off, sizeof(float) * n);
+  if (q.iters) back(q.iters + off, r.d_iters + off, sizeof(int) * n);
+  if (q.status) back(q.status + off, r.d_status + off, sizeof(uint32_t) * n);
+  if (e == cudaSuccess) e = cudaEventRecord(L.done, s);
+  if (e != cudaSuccess) return GM_ERR_CUDA;
+  r.next = off + n;
+  ++r.outstanding;
+  if (!r.started) {
+    r.started = true;
+    r.t_start = Clock::now();
+  }
+  L.req = rp;
+  L.busy = true;
+  return GM_OK;
+}
+
+void finish(gm_ctx* ctx, const std::shared_ptr<Request>& r, gm_status st) {
+  const auto now = Clock::now();
+  if (r->req.latency_ms)
+    *r->req.latency_ms = std::chrono::duration<double, std::milli>(now - r->t_submit).count();
+  if (r->req.queue_ms)
+    *r->req.queue_ms = std::chrono::duration<double, std::milli>((r->started ? r->t_start : now) - r->t_submit).count();
+  release(*r);
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->serve_bytes -= r->bytes;
+  ctx->active.erase(std::remove(ctx->active.begin(), ctx->active.end(), r), ctx->active.end());
+  r->result = st;
+  r->done = true;
+  ctx->done_cv.notify_all();
+}
+
 void serve_loop(gm_ctx* ctx) {
   cudaSetDevice(ctx->device);
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->lanes.resize(ctx->serve_streams);
+    for (ServeLane& L : ctx->lanes) {
+      cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking);
+      cudaMalloc(&L.work, sizeof(gm::WorkCounters));
+      cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming);
+    }
+  }
   for (;;) {
-    std::shared_ptr<Request> r;
-    {
-      std::unique_lock<std::mutex> lk(ctx->mu);
-      ctx->cv.wait(lk, [&] { return ctx->stopping || !ctx->queue.empty(); });
-      if (ctx->stopping && ctx->queue.empty()) return;
-      const gm_ticket t = ctx->queue.front();
-      ctx->queue.pop_front();
-      r = ctx->reqs[t];
-    }
-    gm_status st;
-    {
-      std::lock_guard<std::mutex> lk(ctx->call_mu);
-      gm::DevCfg d = ctx->dev;
-      if (!r->fix.empty())
-        for (int i = 0; i < GM_NPAR; ++i) d.fix[i] = r->fix[i] ? 1 : 0;
-      const gm_request& q = r->req;
-      st = invert_impl(ctx, d, q.iquv, q.npix, q.nl, nullptr, nullptr, q.model, nullptr, q.chi2,
-                       q.iters, nullptr, nullptr, q.status, nullptr);
-    }
+    bool progress = false;
+    // admission in arrival order, within the request-count and memory limits
+    std::vector<std::shared_ptr<Request>> admit;
     {
       std::lock_guard<std::mutex> lk(ctx->mu);
-      r->result = st;
-      r->done = true;
+      while (!ctx->queue.empty() && (int)ctx->active.size() + (int)admit.size() < ctx->serve_max_active) {
+        auto r = ctx->reqs[ctx->queue.front()];
+        if (ctx->serve_bytes + r->bytes > ctx->budget && !(ctx->active.empty() && admit.empty())) break;
+        ctx->queue.pop_front();
+        ctx->serve_bytes += r->bytes;
+        admit.push_back(r);
+      }
     }
-    ctx->done_cv.notify_all();
+    for (auto& r : admit) {
+      const gm_request& q = r->req;
+      const size_t P = (size_t)q.npix;
+      bool ok = device_view(*r, const_cast<float*>(q.iquv), sizeof(float) * 4 * (size_t)q.nl * P, &r->d_in) &&
+                device_view(*r, q.model, sizeof(float) * 11 * P, &r->d_model) &&
+                device_view(*r, q.chi2, sizeof(float) * P, &r->d_chi2) &&
+                device_view(*r, q.iters, sizeof(int) * P, &r->d_iters) &&
+                device_view(*r, q.status, sizeof(uint32_t) * P, &r->d_status);
+      {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        ctx->active.push_back(r);
+      }
+      if (!ok) finish(ctx, r, GM_ERR_NOMEM);
+      else if (q.npix == 0) finish(ctx, r, GM_OK);
+      progress = true;
+    }
+    // completed chunks
+    for (ServeLane& L : ctx->lanes) {
+      if (!L.busy) continue;
+      const cudaError_t e = cudaEventQuery(L.done);
+      if (e == cudaErrorNotReady) continue;
+      auto r = L.req;
+      L.busy = false;
+      L.req.reset();
+      progress = true;
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        r->result = GM_ERR_CUDA;
+      }
+      if (--r->outstanding == 0 && (r->next >= r->req.npix || r->result != GM_OK))
+        finish(ctx, r, r->result);
+    }
+    // keep every lane busy with the next chunk, round robin over requests
+    for (ServeLane& L : ctx->lanes) {
+      if (L.busy) continue;
+      std::shared_ptr<Request> pick;
+      {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        const size_t n = ctx->active.size();
+        for (size_t k = 0; k < n && !pick; ++k) {
+          auto& c = ctx->active[(ctx->rr + k) % n];
+          if (c->result == GM_OK && c->next < c->req.npix && !c->done) {
+            pick = c;
+            ctx->rr = (ctx->rr + k + 1) % n;
+          }
+        }
+      }
+      if (!pick) break;
+      if (launch_chunk(ctx, L, pick) != GM_OK) {
+        cudaGetLastError();
+        pick->result = GM_ERR_CUDA;
+        pick->next = pick->req.npix;
+        if (pick->outstanding == 0) finish(ctx, pick, GM_ERR_CUDA);
+      }
+      progress = true;
+    }
+    std::unique_lock<std::mutex> lk(ctx->mu);
+    bool idle = ctx->active.empty();
+    for (const ServeLane& L : ctx->lanes) idle = idle && !L.busy;
+    if (ctx->stopping && ctx->queue.empty() && idle) break;
+    if (!progress) {
+      if (idle && ctx->queue.empty()) ctx->cv.wait(lk, [&] { return ctx->stopping || !ctx->queue.empty(); });
+      else ctx->cv.wait_for(lk, std::chrono::microseconds(50));
+    }
   }
+  for (ServeLane& L : ctx->lanes) {
+    cudaStreamSynchronize(L.stream);
+    cudaFree(L.work);
+    cudaEventDestroy(L.done);
+    cudaStreamDestroy(L.stream);
+  }
+  ctx->lanes.clear();
 }
 
 }  // namespace

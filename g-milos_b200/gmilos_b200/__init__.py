@@ -37,7 +37,7 @@ EXPORTS = ("gm_create", "gm_destroy", "gm_last_error", "gm_status_string", "gm_c
            "gm_configure", "gm_invert", "gm_invert_ex", "gm_synthesize", "gm_synthesize_f64",
            "gm_synthesize_grid", "gm_lm_step", "gm_submit", "gm_poll", "gm_cancel", "gm_zeeman_from_levels",
            "gm_psf_gaussian", "gm_psf_from_table", "gm_get_stats", "gm_measure_peaks",
-           "gm_invert_noalloc", "gm_classical")
+           "gm_invert_noalloc", "gm_classical", "gm_serving_options")
 
 
 class GmError(RuntimeError):
@@ -68,7 +68,8 @@ class Config(C.Structure):
 class Request(C.Structure):
     _fields_ = [("iquv", C.c_void_p), ("npix", C.c_int64), ("nl", C.c_int),
                 ("model", C.c_void_p), ("chi2", C.c_void_p), ("iters", C.c_void_p),
-                ("status", C.c_void_p), ("fix", C.POINTER(C.c_int))]
+                ("status", C.c_void_p), ("fix", C.POINTER(C.c_int)),
+                ("latency_ms", C.POINTER(C.c_double)), ("queue_ms", C.POINTER(C.c_double))]
 
 
 class Stats(C.Structure):
@@ -104,6 +105,7 @@ def lib():
         L.gm_synthesize_f64.argtypes = [vp, vp, i64, vp, vp, vp]
         L.gm_synthesize_grid.argtypes = [vp, vp, i64, vp, C.c_int, vp, vp]
         L.gm_classical.argtypes = [vp, vp, i64, C.c_int, vp, vp]
+        L.gm_serving_options.argtypes = [vp, C.c_int, i64, C.c_int]
         L.gm_submit.argtypes = [vp, C.POINTER(Request), C.POINTER(C.c_uint64)]
         L.gm_poll.argtypes = [vp, C.c_uint64, C.c_int]
         L.gm_cancel.argtypes = [vp, C.c_uint64]
@@ -362,7 +364,14 @@ class Engine:
         _check(lib().gm_classical(self._ctx, _ptr(iquv), P, self.nl, _ptr(out), None), self._ctx)
         return out
 
+    def serving_options(self, streams=4, chunk_pixels=65536, max_active=16):
+        _check(lib().gm_serving_options(self._ctx, int(streams), int(chunk_pixels), int(max_active)),
+               self._ctx)
+
     def submit(self, iquv, model, chi2=None, iters=None, status=None, fix=None):
+        """Queue an inversion (continuous batching).  The engine reads and
+        writes the arrays until poll() returns for the ticket; this object
+        keeps them alive until then."""
         r = Request()
         r.iquv = _ptr(iquv)
         r.npix = int(iquv.shape[0])
@@ -374,12 +383,26 @@ class Engine:
         if fix is not None:
             arr = (C.c_int * NPAR)(*[int(x) for x in fix])
             r.fix = C.cast(arr, C.POINTER(C.c_int))
+        times = (C.c_double * 2)(-1.0, -1.0)
+        r.latency_ms = C.cast(C.byref(times, 0), C.POINTER(C.c_double))
+        r.queue_ms = C.cast(C.byref(times, C.sizeof(C.c_double)), C.POINTER(C.c_double))
         t = C.c_uint64()
         _check(lib().gm_submit(self._ctx, C.byref(r), C.byref(t)), self._ctx)
+        if not hasattr(self, "_times"):
+            self._times = {}
+        self._times[t.value] = (times, (iquv, model, chi2, iters, status))
         return t.value
 
     def poll(self, ticket, timeout_us=-1):
-        return lib().gm_poll(self._ctx, ticket, timeout_us)
+        """Status of the request (0 when done); its latency and queueing time
+        [ms] are then in last_latency_ms / last_queue_ms."""
+        st = lib().gm_poll(self._ctx, ticket, timeout_us)
+        if st != 6:   # not a timeout: the ticket is consumed
+            entry = getattr(self, "_times", {}).pop(ticket, None)
+            if entry is not None:
+                times = entry[0]
+                self.last_latency_ms, self.last_queue_ms = times[0], times[1]
+        return st
 
     def cancel(self, ticket):
         _check(lib().gm_cancel(self._ctx, ticket), self._ctx)

@@ -200,6 +200,14 @@ gm_status gm_synthesize_grid(gm_ctx *ctx, const double *models, int64_t npix,
                              const double *offsets_A, int ngrid, float *iquv, void *stream);
 
 /* ---------------- serving (continuous batching) --------------------------- */
+/* Requests (frames or ROIs of any size) are admitted in arrival order as
+ * slots and device memory free up: at most max_active at a time, their
+ * staging within the context's HBM budget.  Admitted requests are cut into
+ * chunks of chunk_pixels; `streams` lanes each keep one chunk on the device,
+ * taken round robin from the admitted requests, so requests that arrive
+ * while others run start within one chunk time and their work overlaps on
+ * the device.  Per-pixel results do not depend on the mix.  No counterpart
+ * in the reference (its main inverts one cube per process run). */
 typedef uint64_t gm_ticket;
 typedef struct {
     const float *iquv;            /* [P][4][nl] host or device */
@@ -210,10 +218,17 @@ typedef struct {
     int *iters;                   /* [P] (optional) */
     uint32_t *status;             /* [P] (optional) */
     const int *fix;               /* optional per-request free mask [11] */
+    double *latency_ms;           /* optional out: submit -> results in place */
+    double *queue_ms;             /* optional out: submit -> first chunk launched */
 } gm_request;
 
+/* before the first gm_submit: lanes (1..32, default 4), pixels per chunk
+ * (default 65536), admitted requests at a time (default 16) */
+gm_status gm_serving_options(gm_ctx *ctx, int streams, int64_t chunk_pixels, int max_active);
 gm_status gm_submit(gm_ctx *ctx, const gm_request *req, gm_ticket *ticket);
+/* wait for a request (timeout_us < 0: no limit); consumes the ticket */
 gm_status gm_poll(gm_ctx *ctx, gm_ticket ticket, int timeout_us);
+/* cancel a request that has not been admitted yet */
 gm_status gm_cancel(gm_ctx *ctx, gm_ticket ticket);
 
 /* ---------------- host helpers mirroring the reference's set-up ---------- */
