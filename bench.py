@@ -338,6 +338,8 @@ def run_engine(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(obs[: min(P, 200000)].cpu().numpy(), slight, psf, lam, seconds=args.cpu_seconds)
+    if rank == 0 and world == 1 and args.serve_requests > 0:
+        result["latency"] = serving_latency(eng, obs_h, args)
     if rank == 0 and world == 1 and args.ref_gpu_pixels > 0:
         import ref
         n = min(P, args.ref_gpu_pixels)
@@ -366,6 +368,58 @@ def run_engine(args):
     eng.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def serving_latency(eng, obs_h, args):
+    """Serving under load: a Poisson stream of inversion requests, frames of
+    side uniform in [side_min, side_max] px x 4 x 30 lambda with PSF and
+    stray light, half of them with S0 and S1 fixed (7 ME + alpha free instead
+    of 9 + alpha), host buffers in and out (pinned), through the engine's
+    continuous-batching entry points (gm_submit / gm_poll).  Latency is
+    submit -> results in host memory, taken by the engine.  Frames are cut
+    from the bench cube, tiled when a frame is larger than the cube."""
+    import torch
+    rng = np.random.default_rng(args.seed + 77)
+    n = args.serve_requests
+    sides = rng.integers(args.serve_side_min, args.serve_side_max + 1, n)
+    npix = (sides.astype(np.int64) ** 2)
+    fix7 = (1, 1, 1, 1, 1, 1, 1, 0, 0, 0, 1)
+    mixes = [FIX if k % 2 == 0 else fix7 for k in range(n)]
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n))
+    P = obs_h.shape[0]
+    reps = int(np.ceil(npix.max() / P))
+    pool = obs_h if reps <= 1 else torch.cat([obs_h] * reps).pin_memory()
+    starts = rng.integers(0, max(1, pool.shape[0] - int(npix.max()) + 1), n)
+    outs = [(torch.empty((int(k), 11), dtype=torch.float32).pin_memory(),
+             torch.empty(int(k), dtype=torch.float32).pin_memory(),
+             torch.empty(int(k), dtype=torch.int32).pin_memory()) for k in npix]
+    tickets = [None] * n
+    t0 = time.perf_counter()
+    for k in range(n):
+        delay = t0 + arrivals[k] - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        frame = pool[int(starts[k]): int(starts[k]) + int(npix[k])]
+        tickets[k] = eng.submit(frame, outs[k][0], chi2=outs[k][1], iters=outs[k][2], fix=mixes[k])
+    lat, queue = [], []
+    for k in range(n):
+        st = eng.poll(tickets[k])
+        if st != 0:
+            raise RuntimeError("serving request %d failed with status %d" % (k, st))
+        lat.append(eng.last_latency_ms)
+        queue.append(eng.last_queue_ms)
+    t_end = t0 + max(arrivals[k] + lat[k] / 1e3 for k in range(n))
+    lat = np.array(lat)
+    span = t_end - t0
+    return {"what": "Poisson stream of %d requests at %.2f req/s, frames %d^2-%d^2 px x 4 x 30 lambda, "
+                    "PSF + stray light, half with S0/S1 fixed; host buffers; continuous batching "
+                    "(%d lanes, %d-pixel chunks)" % (n, args.serve_rate, args.serve_side_min,
+                                                     args.serve_side_max, 4, 65536),
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
+            "mean_queue_ms": float(np.mean(queue)),
+            "pixels_per_s": float(npix.sum() / span), "offered_pixels_per_s": float(npix.sum() / arrivals[-1]),
+            "requests": n, "pixels": int(npix.sum())}
 
 
 # ----------------------------------------------------------------- reference arms
@@ -531,6 +585,11 @@ def main():
     ap.add_argument("--ref-gpu-pixels", type=int, default=65536,
                     help="pixels of the cube run through the reference's sm_100a build (0: skip)")
     ap.add_argument("--ref-gpu-streams", type=int, default=16)
+    ap.add_argument("--serve-requests", type=int, default=20,
+                    help="requests of the serving-latency phase (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=1.0, help="mean arrivals per second")
+    ap.add_argument("--serve-side-min", type=int, default=256)
+    ap.add_argument("--serve-side-max", type=int, default=2048)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
