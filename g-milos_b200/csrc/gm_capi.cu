@@ -240,6 +240,18 @@ gm_status build_devcfg(gm_ctx* ctx, const gm_config& c, gm::DevCfg* d) {
   return GM_OK;
 }
 
+// Blocks of a persistent inversion launch: every resident slot of every SM,
+// but no more blocks than the pixels need.
+int64_t invert_grid(const gm::DevCfg& d, bool per_pixel_init, int sms, int64_t npix,
+                    gm::InvertGeometry* out) {
+  const gm::InvertGeometry g = gm::invert_geometry(d, per_pixel_init);
+  if (out) *out = g;
+  int64_t grid = (int64_t)std::max(1, g.blocks_per_sm) * sms;
+  const int64_t needed = (npix + g.pixels_per_block - 1) / g.pixels_per_block;
+  if (grid > needed) grid = needed;
+  return grid < 1 ? 1 : grid;
+}
+
 void serve_loop(gm_ctx* ctx);
 
 }  // namespace
@@ -420,17 +432,15 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   ia.work = ctx->work;
   cudaError_t e = cudaMemsetAsync(ctx->work, 0, sizeof(gm::WorkCounters), s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "work counter reset");
-  const int per_sm = std::max(1, gm::invert_blocks_per_sm(d, ia.init_models != nullptr));
-  int64_t grid = (int64_t)per_sm * ctx->sms;
-  const int64_t needed = (npix + gm::warps_for_nl(nl) - 1) / gm::warps_for_nl(nl);
-  if (grid > needed) grid = needed;
+  gm::InvertGeometry geo;
+  const int64_t grid = invert_grid(d, ia.init_models != nullptr, ctx->sms, npix, &geo);
   cudaEventRecord(ctx->ev0, s);
   e = gm::launch_invert(d, ia, (int)grid, s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "inversion kernel launch");
   cudaEventRecord(ctx->ev1, s);
   ctx->stats.grid_blocks = (int)grid;
-  ctx->stats.block_threads = gm::warps_for_nl(nl) * 32;
-  ctx->stats.warps_per_block = gm::warps_for_nl(nl);
+  ctx->stats.block_threads = geo.threads;
+  ctx->stats.warps_per_block = geo.threads / 32;
   ctx->stats.kernel_launches = 1;
   ctx->stats.pixels = npix;
   const Arg* outs[] = {&a_model, &a_m64, &a_chi, &a_it, &a_acc, &a_fit, &a_st,
@@ -778,10 +788,7 @@ gm_status launch_chunk(gm_ctx* ctx, ServeLane& L, const std::shared_ptr<Request>
   ia.iters = r.d_iters ? r.d_iters + off : nullptr;
   ia.status = r.d_status ? r.d_status + off : nullptr;
   ia.work = L.work;
-  const int per_sm = std::max(1, gm::invert_blocks_per_sm(r.dev, false));
-  int64_t grid = (int64_t)per_sm * ctx->sms;
-  const int64_t needed = (n + gm::warps_for_nl(nl) - 1) / gm::warps_for_nl(nl);
-  if (grid > needed) grid = needed;
+  const int64_t grid = invert_grid(r.dev, false, ctx->sms, n, nullptr);
   e = gm::launch_invert(r.dev, ia, (int)grid, s);
   if (e != cudaSuccess) return GM_ERR_CUDA;
   auto back = [&](void* host, const void* dev, size_t bytes) {
@@ -949,9 +956,9 @@ gm_status noalloc_scratch(int dev, void** out) {
     gm::DevCfg probe{};
     probe.nl = 32;
     probe.nterms = 10;
-    const int b32 = gm::invert_blocks_per_sm(probe, false);
+    const int b32 = gm::invert_geometry(probe, false).blocks_per_sm;
     probe.nl = 64;
-    if (b32 < 1 || gm::invert_blocks_per_sm(probe, false) < 1) {
+    if (b32 < 1 || gm::invert_geometry(probe, false).blocks_per_sm < 1) {
       cudaGetLastError();
       return GM_ERR_CUDA;
     }
@@ -1006,10 +1013,7 @@ extern "C" gm_status gm_invert_noalloc(const gm_config* cfg, const float* iquv, 
   ia.fitted = fitted;
   ia.status = status;
   ia.work = (gm::WorkCounters*)scratch;
-  const int per_sm = std::max(1, gm::invert_blocks_per_sm(d, false));
-  int64_t grid = (int64_t)per_sm * sms;
-  const int64_t needed = (npix + gm::warps_for_nl(nl) - 1) / gm::warps_for_nl(nl);
-  if (grid > needed) grid = needed;
+  const int64_t grid = invert_grid(d, false, sms, npix, nullptr);
   e = gm::launch_invert(d, ia, (int)grid, s);
   return e == cudaSuccess ? GM_OK : GM_ERR_CUDA;
 }

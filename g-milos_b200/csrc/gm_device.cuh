@@ -132,12 +132,14 @@ struct Angles {
 // macroturbulence; V = 1: 10 terms with the macroturbulence convolution
 // (a fixed v_mac > 0, or per-pixel start models); V = 2: the 11-term path
 // (v_mac and alpha both free: lm_mils_11, milosUtils.cu:713-850) with its
-// FP64 solve.
+// FP64 solve.  V = 0 solves the 10x10 system for two dampings at once, one
+// per half-warp (the second is the damping a rejected trial moves to).
 template <int V>
 struct Variant {
   static constexpr int NT = (V == 2) ? 11 : 10;         // terms of the normal equations
   static constexpr bool MAC = V != 0;                    // macroturbulence-capable
   static constexpr int ROWS = MAC ? 36 : 32;             // staged rows (+4 for the v_mac RF)
+  static constexpr int SOLVES = (V == 0) ? 2 : 1;        // 10x10 systems solved per call
 };
 
 // Per-lane results of a synthesis that the response functions reuse:
@@ -169,11 +171,12 @@ struct WarpSmem {
   static constexpr bool S11 = V == 2;
   double m[11];          // current (last accepted) model: the reference's initModel
   double t[11];          // trial model, persistent like the reference's `model`
-  float A[2][10][11];    // Jacobi working matrix (upper triangle), double-buffered
+  static constexpr int NS = Variant<V>::SOLVES;
+  float A[NS][2][10][11];   // Jacobi working matrix (upper triangle) per damping, double-buffered
   float alpha[68];       // undamped normal matrix, packed upper triangle (55 or 66)
   float beta[12];
-  float vec[2][12];      // rotated beta, double-buffered; the step lands in vec[0]
-  float cs[18][5], sn[18][5];
+  float vec[NS][2][12];  // rotated beta per damping, double-buffered; a step lands in vec[d][0]
+  float cs[NS][18][5], sn[NS][18][5];
   float red[96];
   float ic[NR];          // continuum about which each staged I row is reflected
   double gk[Variant<V>::MAC ? kMaxNl : 1];   // macroturbulence kernel (PSF folded in)
@@ -838,29 +841,40 @@ __device__ __forceinline__ float chisq(const DevCfg& c, const float (&syn)[LPL][
 // --------------------------------------------------------------- 10x10 solve
 // delta = V diag(1/w) V^T beta where (w, V) come from 18 steps of the
 // reference's parallel Jacobi (svdcordicf, svdcordic.cu:423-536; mil_svdf,
-// milosUtils.cu:328-365).  Lanes 0..14 own the 15 2x2 blocks of the upper
-// triangle; after every step the rotated blocks are written to the
+// milosUtils.cu:328-365).  A group of lanes owns the 15 2x2 blocks of the
+// upper triangle; after every step the rotated blocks are written to the
 // round-robin relabelled positions.  V is never formed: the step rotations
 // are applied to beta on the way in and replayed transposed, in reverse, on
 // the way out.  The matrix and the vector are double-buffered so a step
 // needs one warp barrier, and every lane runs the same instruction stream
-// (lanes past 14 shadow block (0, 0) and store nothing).
+// (lanes past 14 of a group shadow block (0, 0) and store nothing).  With
+// two solves per call each half-warp is a group with its own damping;
+// otherwise the group is the warp.  The step loops stay rolled: the kernel
+// is bound by instruction fetch, and a rolled loop keeps the solve's code
+// small.
 struct SolvePlan {
   int src;                      // offset of this lane's block in the working matrix
   int d00, d01, d10, d11;       // offsets its four entries move to
-  int p, q;                     // block row / column (rotation pair)
+  int p, q;                     // block row / column (rotation pair), as group lanes
   int vin, vout0, vout1;        // beta pair read / relabelled write positions
-  int init0, init1;             // packed-triangle entries this lane copies in (-1: none)
-  int ioff0, ioff1;             // and where they go
+  int base;                     // first lane of this lane's group
+  // packed-triangle entries g + e * (32 / NS) (e < 2 NS, g the group lane)
+  // this lane copies in: byte e holds the working-matrix offset, bit 7
+  // marking a diagonal entry, 0xff none
+  unsigned initpack;
 };
 
+template <int NS>
 __device__ __forceinline__ SolvePlan make_solve_plan(int lane) {
+  constexpr int G = 32 / NS;
+  const int g = lane & (G - 1);
   SolvePlan s;
   const int bp[15] = {0, 1, 2, 3, 4, 0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
   const int bq[15] = {0, 1, 2, 3, 4, 1, 2, 3, 4, 2, 3, 4, 3, 4, 4};
   const int pr[10] = {0, 2, 4, 1, 6, 3, 8, 5, 9, 7};
-  s.p = lane < 15 ? bp[lane] : 0;
-  s.q = lane < 15 ? bq[lane] : 0;
+  s.base = lane - g;
+  s.p = g < 15 ? bp[g] : 0;
+  s.q = g < 15 ? bq[g] : 0;
   const int r0 = 2 * s.p, c0 = 2 * s.q;
   s.src = r0 * 11 + c0;
   auto dst = [&](int r, int c) {
@@ -875,42 +889,48 @@ __device__ __forceinline__ SolvePlan make_solve_plan(int lane) {
   s.vout0 = pr[r0];
   s.vout1 = pr[r0 + 1];
   // packed upper-triangle index i -> (row, col)
-  s.init0 = -1;
-  s.init1 = -1;
-  s.ioff0 = 0;
-  s.ioff1 = 0;
+  s.initpack = 0xffffffffu;
   int i = 0;
   for (int r = 0; r < 10; ++r)
     for (int c = r; c < 10; ++c, ++i) {
-      if (i == lane) { s.init0 = i; s.ioff0 = r * 11 + c + (r == c ? 1000 : 0); }
-      if (i == lane + 32) { s.init1 = i; s.ioff1 = r * 11 + c + (r == c ? 1000 : 0); }
+      if (i >= g && (i - g) % G == 0 && (i - g) / G < 2 * NS) {
+        const int e = (i - g) / G;
+        const unsigned b = (unsigned)(r * 11 + c) | (r == c ? 0x80u : 0u);
+        s.initpack = (s.initpack & ~(0xffu << (8 * e))) | (b << (8 * e));
+      }
     }
   return s;
 }
 
+// Solves for damping 1 + flambda into sm.vec[0][0] and, with two solves per
+// call, for 1 + flambda2 into sm.vec[1][0].
 template <int LPL, int V>
 __device__ __forceinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, float flambda,
-                                        int lane, bool accurate) {
+                                        float flambda2, int lane, bool accurate) {
+  constexpr int NS = Variant<V>::SOLVES, G = 32 / NS;
+  const int h = NS == 2 ? lane >> 4 : 0;
+  const int g = lane & (G - 1);
   // damped matrix (diagonal x (1 + lambda), milosUtils.cu:648-652)
-  const double damp = 1.0 + (double)flambda;
-  float* A = &sm.A[0][0][0];
-  float* B = &sm.A[1][0][0];
-  if (pl.init0 >= 0) {
-    const float a = sm.alpha[pl.init0];
-    A[pl.ioff0 % 1000] = (pl.ioff0 >= 1000) ? (float)((double)a * damp) : a;
+  const double damp = 1.0 + (double)(h ? flambda2 : flambda);
+  float* A = &sm.A[h][0][0][0];
+  float* B = &sm.A[h][1][0][0];
+#pragma unroll
+  for (int e = 0; e < 2 * NS; ++e) {
+    const unsigned b = (pl.initpack >> (8 * e)) & 0xffu;
+    if (b != 0xffu) {
+      const float a = sm.alpha[g + e * G];
+      A[b & 0x7fu] = (b & 0x80u) ? (float)((double)a * damp) : a;
+    }
   }
-  if (pl.init1 >= 0) {
-    const float a = sm.alpha[pl.init1];
-    A[pl.ioff1 % 1000] = (pl.ioff1 >= 1000) ? (float)((double)a * damp) : a;
-  }
-  float* va = &sm.vec[0][0];
-  float* vb = &sm.vec[1][0];
-  if (lane < 10) va[lane] = sm.beta[lane];
+  float* va = &sm.vec[h][0][0];
+  float* vb = &sm.vec[h][1][0];
+  if (g < 10) va[g] = sm.beta[g];
   __syncwarp();
 
   const float quarter = (float)(kPi / 4);
   const float qclamp = __fdividef((float)kPi, 4.f);
-  const bool diag = lane < 5, active = lane < 15;
+  const bool diag = g < 5, active = g < 15;
+#pragma unroll 1
   for (int step = 0; step < 18; ++step) {
     const float m00 = A[pl.src], m01 = A[pl.src + 1], m11 = A[pl.src + 12];
     const float m10 = diag ? m01 : A[pl.src + 11];
@@ -926,11 +946,11 @@ __device__ __forceinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& p
     float sn, cs;
     sincos_mode(th, &sn, &cs, accurate);
     if (diag) {
-      sm.cs[step][lane] = cs;
-      sm.sn[step][lane] = sn;
+      sm.cs[h][step][g] = cs;
+      sm.sn[h][step][g] = sn;
     }
-    const float cr = __shfl_sync(kFull, cs, pl.p), sr = __shfl_sync(kFull, sn, pl.p);
-    const float cc = __shfl_sync(kFull, cs, pl.q), sc = __shfl_sync(kFull, sn, pl.q);
+    const float cr = __shfl_sync(kFull, cs, pl.base + pl.p), sr = __shfl_sync(kFull, sn, pl.base + pl.p);
+    const float cc = __shfl_sync(kFull, cs, pl.base + pl.q), sc = __shfl_sync(kFull, sn, pl.base + pl.q);
     const float t0 = m00 * cr - m10 * sr, t1 = m00 * sr + m10 * cr;
     const float u0 = m01 * cr - m11 * sr, u1 = m01 * sr + m11 * cr;
     const float n00 = t0 * cc - u0 * sc, n11 = t1 * sc + u1 * cc;
@@ -952,16 +972,17 @@ __device__ __forceinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& p
   }
   // 18 steps: the final matrix and vector are back in the first buffers, in
   // the original index order.  z = (V^T beta) / w with the |w| <= 1e-12 cut.
-  if (lane < 10) {
-    const float w = A[lane * 12];
+  if (g < 10) {
+    const float w = A[g * 12];
     const float inv = ((double)fabsf(w) > 1e-12) ? (1.f / w) : 0.f;
-    va[lane] = va[lane] * inv;
+    va[g] = va[g] * inv;
   }
   __syncwarp();
   // delta = V z: undo the steps in reverse order
+#pragma unroll 1
   for (int step = 17; step >= 0; --step) {
     const float y0 = va[pl.vout0], y1 = va[pl.vout1];
-    const float cs = sm.cs[step][pl.p], sn = sm.sn[step][pl.p];
+    const float cs = sm.cs[h][step][pl.p], sn = sm.sn[h][step][pl.p];
     if (diag) {
       vb[pl.vin] = cs * y0 + sn * y1;
       vb[pl.vin + 1] = -sn * y0 + cs * y1;
@@ -969,7 +990,7 @@ __device__ __forceinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& p
     __syncwarp();
     float* tv = va; va = vb; vb = tv;
   }
-  // 18 swaps: the result is in sm.vec[0]
+  // 18 swaps: the result is in sm.vec[h][0]
 }
 
 // --------------------------------------------------------------- 11x11 solve (FP64)

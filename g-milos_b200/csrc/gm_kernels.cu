@@ -66,7 +66,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
       for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
   }
 
-  const SolvePlan plan = make_solve_plan(lane);
+  const SolvePlan plan = make_solve_plan<Variant<V>::SOLVES>(lane);
   Solve11Plan plan11;
   if constexpr (NT == 11) plan11 = make_solve11_plan(lane);
   unsigned long long my_iter = 0, my_acc = 0;
@@ -94,11 +94,16 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
     float flambda = c.ilambda, pbf = 1.f, ochisqr = 0.f, chisqr0 = 0.f;
     int iter = 0, acc = 0;
     bool stop = false, first = true;
+    // sm.vec[1][0] holds the step for the damping that the last trial's
+    // rejection moved to (solved beside the trial's own step)
+    bool have_next = false, solved = false;
     while (true) {
       if (!first) {
         if constexpr (NT == 10) {
-          solve10<LPL, V>(sm, plan, flambda, lane, c.numerics != 0);
-          if (lane == 0) apply_delta_check<10>(c, sm.m, sm.vec[0], sm.t);
+          const bool reuse = Variant<V>::SOLVES == 2 && have_next;
+          if (!reuse) solve10<LPL, V>(sm, plan, flambda, flambda * 10.f * pbf, lane, c.numerics != 0);
+          solved = !reuse;
+          if (lane == 0) apply_delta_check<10>(c, sm.m, sm.vec[reuse ? 1 : 0][0], sm.t);
         } else {
           solve11<LPL, V>(sm, plan11, flambda, lane);
           if (lane == 0) apply_delta_check<11>(c, sm.m, sm.dd, sm.t);
@@ -111,7 +116,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
       if (!first) {
         if (iter == 0) {
           if (a.step_delta && lane < NT)
-            a.step_delta[pix * NT + lane] = (NT == 10) ? sm.vec[0][lane] : (float)sm.dd[lane];
+            a.step_delta[pix * NT + lane] = (NT == 10) ? sm.vec[0][0][lane] : (float)sm.dd[lane];
           if (a.step_trial && lane < 11) a.step_trial[pix * 11 + lane] = sm.t[lane];
           if (lane == 0 && a.step_chi2_start) a.step_chi2_start[pix] = chisqr0;
           if (lane == 0 && a.step_chi2_trial) a.step_chi2_trial[pix] = chisqr;
@@ -136,6 +141,8 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
           st |= GM_PIX_LAMBDA_EXIT;
         }
         ++iter;
+        // the rejection damping above is the second one the solve just took
+        have_next = !accept && solved;
         if (c.logclambda) pbf = log10f(chisqr) / log10f(chisqr0);
       }
       if (accept) {
@@ -378,12 +385,13 @@ cudaError_t prepare_invert() {
 }
 
 template <int LPL, int V>
-int blocks_per_sm_t() {
-  int n = 0;
-  if (prepare_invert<LPL, V>() != cudaSuccess) return 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, invert_kernel<LPL, V>, warps_per_block<LPL>() * 32,
+InvertGeometry geometry_t() {
+  // one pixel per warp
+  InvertGeometry g{0, warps_per_block<LPL>() * 32, warps_per_block<LPL>(), V};
+  if (prepare_invert<LPL, V>() != cudaSuccess) return g;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g.blocks_per_sm, invert_kernel<LPL, V>, g.threads,
                                                 smem_bytes<LPL, V>());
-  return n;
+  return g;
 }
 
 int kernel_variant(const DevCfg& cfg, bool per_pixel_init) {
@@ -391,16 +399,16 @@ int kernel_variant(const DevCfg& cfg, bool per_pixel_init) {
   return (cfg.init[MAC] > 0.0001 || per_pixel_init) ? 1 : 0;
 }
 
-int invert_blocks_per_sm(const DevCfg& cfg, bool per_pixel_init) {
+InvertGeometry invert_geometry(const DevCfg& cfg, bool per_pixel_init) {
   const int v = kernel_variant(cfg, per_pixel_init);
   if (cfg.nl <= 32) {
-    if (v == 0) return blocks_per_sm_t<1, 0>();
-    if (v == 1) return blocks_per_sm_t<1, 1>();
-    return blocks_per_sm_t<1, 2>();
+    if (v == 0) return geometry_t<1, 0>();
+    if (v == 1) return geometry_t<1, 1>();
+    return geometry_t<1, 2>();
   }
-  if (v == 0) return blocks_per_sm_t<2, 0>();
-  if (v == 1) return blocks_per_sm_t<2, 1>();
-  return blocks_per_sm_t<2, 2>();
+  if (v == 0) return geometry_t<2, 0>();
+  if (v == 1) return geometry_t<2, 1>();
+  return geometry_t<2, 2>();
 }
 
 template <int LPL, int V>

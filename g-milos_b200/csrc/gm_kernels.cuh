@@ -55,8 +55,14 @@ cudaError_t launch_synth_grid(const DevCfg& cfg, const double* models, int64_t n
 // kernel variant for a configuration (0: 10 terms, 1: 10 terms with
 // macroturbulence, 2: 11 terms); per_pixel_init: start models given per pixel
 int kernel_variant(const DevCfg& cfg, bool per_pixel_init);
-// resident blocks per SM of the inversion kernel for this configuration
-int invert_blocks_per_sm(const DevCfg& cfg, bool per_pixel_init);
+// launch geometry of the inversion kernel for a configuration
+struct InvertGeometry {
+  int blocks_per_sm;      // resident blocks per SM (0: the kernel cannot be resident)
+  int threads;            // threads per block
+  int pixels_per_block;   // pixels in flight per block
+  int variant;
+};
+InvertGeometry invert_geometry(const DevCfg& cfg, bool per_pixel_init);
 
 // FMA-issue-bound microbenchmark (kind 0: FP32, 1: FP64); each thread runs
 // kPeakChains independent FMA chains of `iters` steps.
