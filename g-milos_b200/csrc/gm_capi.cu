@@ -188,6 +188,8 @@ gm_status build_devcfg(gm_ctx* ctx, const gm_config& c, gm::DevCfg* d) {
   d->use_psf = c.use_psf ? 1 : 0;
   d->use_slight = c.use_slight ? 1 : 0;
   d->slight_per_pixel = c.slight_per_pixel ? 1 : 0;
+  d->lambda_per_pixel = c.lambda_per_pixel ? 1 : 0;
+  d->lam_map = nullptr;   // bound per call
   d->init_mode = c.init_mode == GM_INIT_CLASSICAL ? 0 : 1;
   d->miter = c.miter;
   d->logclambda = c.logclambda;
@@ -377,7 +379,7 @@ struct StepOut {
 
 static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* iquv, int64_t npix,
                              int nl, const double* init_models, const float* slight_map,
-                             float* model, double* model_f64, float* chi2, int* iters,
+                             const double* lambda_map, float* model, double* model_f64, float* chi2, int* iters,
                              int* accepted, float* fitted, uint32_t* status, void* stream,
                              const StepOut* so = nullptr) {
   if (!ctx->configured) return fail(ctx, GM_ERR_NOT_CONFIGURED, "gm_configure first");
@@ -387,9 +389,10 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   cudaSetDevice(ctx->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   const size_t cube = sizeof(float) * 4 * (size_t)nl * npix;
-  size_t need = cube + (fitted ? cube : 0) + (size_t)npix * (11 * 12 + 16);
+  size_t need = cube + (fitted ? cube : 0) + (size_t)npix * (11 * 12 + 16) +
+                (dcfg.lambda_per_pixel ? sizeof(double) * (size_t)nl * npix : 0);
   if (need > ctx->budget) return fail(ctx, GM_ERR_NOMEM, "request exceeds the context's HBM budget");
-  Arg a_in, a_init, a_sl, a_model, a_m64, a_chi, a_it, a_acc, a_fit, a_st;
+  Arg a_in, a_init, a_sl, a_lam, a_model, a_m64, a_chi, a_it, a_acc, a_fit, a_st;
   gm_status st;
   if ((st = stage_in(ctx, "iquv", iquv, cube, &a_in, s)) != GM_OK) return st;
   if ((st = stage_in(ctx, "init", init_models, sizeof(double) * 11 * npix, &a_init, s)) != GM_OK) return st;
@@ -398,6 +401,12 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
     if (!slight_map) return fail(ctx, GM_ERR_INVALID, "per-pixel stray light needs a map");
     if ((st = stage_in(ctx, "slight", slight_map, cube, &a_sl, s)) != GM_OK) return st;
     d.slight = (const float*)a_sl.dev;
+  }
+  if (d.lambda_per_pixel) {
+    if (!lambda_map) return fail(ctx, GM_ERR_INVALID, "per-pixel wavelength grids need lambda_map");
+    if ((st = stage_in(ctx, "lammap", lambda_map, sizeof(double) * (size_t)nl * npix, &a_lam, s)) != GM_OK)
+      return st;
+    d.lam_map = (const double*)a_lam.dev;
   }
   if ((st = stage_out(ctx, "model", model, sizeof(float) * 11 * npix, &a_model)) != GM_OK) return st;
   if ((st = stage_out(ctx, "model64", model_f64, sizeof(double) * 11 * npix, &a_m64)) != GM_OK) return st;
@@ -473,7 +482,7 @@ gm_status gm_invert_ex(gm_ctx* ctx, const float* iquv, int64_t npix, int nl,
   gm::DevCfg d = ctx->dev;
   if (init_models) d.init_mode = 1;
   const float* map = (ctx->cfg.use_slight && ctx->cfg.slight_per_pixel) ? ctx->cfg.slight : nullptr;
-  return invert_impl(ctx, d, iquv, npix, nl, init_models, map, model, model_f64, chi2, iters,
+  return invert_impl(ctx, d, iquv, npix, nl, init_models, map, ctx->cfg.lambda_map, model, model_f64, chi2, iters,
                      accepted, fitted, status, stream);
 }
 
@@ -499,7 +508,7 @@ gm_status gm_lm_step(gm_ctx* ctx, const float* iquv, int64_t npix, int nl, const
   so.chi2_start = chi2_start;
   so.chi2_trial = chi2_trial;
   const float* map = (ctx->cfg.use_slight && ctx->cfg.slight_per_pixel) ? ctx->cfg.slight : nullptr;
-  return invert_impl(ctx, d, iquv, npix, nl, models, map, nullptr, nullptr, nullptr, nullptr, nullptr,
+  return invert_impl(ctx, d, iquv, npix, nl, models, map, ctx->cfg.lambda_map, nullptr, nullptr, nullptr, nullptr, nullptr,
                      nullptr, nullptr, stream, &so);
 }
 
@@ -513,7 +522,7 @@ static gm_status synth_impl(gm_ctx* ctx, const float* m32, const double* m64, in
   cudaSetDevice(ctx->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   const int nl = ctx->dev.nl, nt = ctx->dev.nterms;
-  Arg a_m, a_out, a_rf, a_sl;
+  Arg a_m, a_out, a_rf, a_sl, a_lam;
   gm_status st;
   if (m32) st = stage_in(ctx, "smodels", m32, sizeof(float) * 11 * npix, &a_m, s);
   else st = stage_in(ctx, "smodels", m64, sizeof(double) * 11 * npix, &a_m, s);
@@ -527,6 +536,12 @@ static gm_status synth_impl(gm_ctx* ctx, const float* m32, const double* m64, in
   if (d.use_slight && d.slight_per_pixel) {
     if ((st = stage_in(ctx, "sslight", ctx->cfg.slight, sizeof(float) * 4 * nl * npix, &a_sl, s)) != GM_OK) return st;
     d.slight = (const float*)a_sl.dev;
+  }
+  if (d.lambda_per_pixel) {
+    if (!ctx->cfg.lambda_map) return fail(ctx, GM_ERR_INVALID, "per-pixel wavelength grids need lambda_map");
+    if ((st = stage_in(ctx, "slammap", ctx->cfg.lambda_map, sizeof(double) * (size_t)nl * npix, &a_lam, s)) != GM_OK)
+      return st;
+    d.lam_map = (const double*)a_lam.dev;
   }
   gm::SynthArgs sa{};
   sa.models_f32 = m32 ? (const float*)a_m.dev : nullptr;
@@ -590,11 +605,18 @@ gm_status gm_classical(gm_ctx* ctx, const float* iquv, int64_t npix, int nl, dou
   if (npix == 0) return GM_OK;
   cudaSetDevice(ctx->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-  Arg a_in, a_out;
+  Arg a_in, a_out, a_lam;
   gm_status st;
   if ((st = stage_in(ctx, "iquv", iquv, sizeof(float) * 4 * (size_t)nl * npix, &a_in, s)) != GM_OK) return st;
   if ((st = stage_out(ctx, "cmodels", models, sizeof(double) * 11 * npix, &a_out)) != GM_OK) return st;
-  cudaError_t e = gm::launch_classical(ctx->dev, (const float*)a_in.dev, npix, (double*)a_out.dev, s);
+  gm::DevCfg d = ctx->dev;
+  if (d.lambda_per_pixel) {
+    if (!ctx->cfg.lambda_map) return fail(ctx, GM_ERR_INVALID, "per-pixel wavelength grids need lambda_map");
+    if ((st = stage_in(ctx, "lammap", ctx->cfg.lambda_map, sizeof(double) * (size_t)nl * npix, &a_lam, s)) != GM_OK)
+      return st;
+    d.lam_map = (const double*)a_lam.dev;
+  }
+  cudaError_t e = gm::launch_classical(d, (const float*)a_in.dev, npix, (double*)a_out.dev, s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "classical-estimates launch");
   if ((st = copy_back(ctx, a_out, s)) != GM_OK) return st;
   if (a_out.host || a_in.dev != (const void*)iquv || !stream) {
@@ -713,6 +735,8 @@ gm_status gm_submit(gm_ctx* ctx, const gm_request* req, gm_ticket* ticket) {
     return fail(ctx, GM_ERR_INVALID, "bad request");
   if (ctx->dev.use_slight && ctx->dev.slight_per_pixel)
     return fail(ctx, GM_ERR_UNSUPPORTED, "serving takes one stray-light profile, not a per-pixel map");
+  if (ctx->dev.lambda_per_pixel)
+    return fail(ctx, GM_ERR_UNSUPPORTED, "serving takes one wavelength grid, not per-pixel grids");
   auto r = std::make_shared<Request>();
   r->req = *req;
   r->dev = ctx->dev;
@@ -978,6 +1002,7 @@ extern "C" gm_status gm_invert_noalloc(const gm_config* cfg, const float* iquv, 
   gm_status st = build_devcfg(nullptr, *cfg, &d);
   if (st != GM_OK) return st;
   if (nl != d.nl) return GM_ERR_INVALID;
+  if (d.lambda_per_pixel) return GM_ERR_UNSUPPORTED;
   const bool global_slight = d.use_slight && !d.slight_per_pixel;
   const size_t need = kNoallocSlightOffset + (global_slight ? sizeof(float) * 4 * (size_t)nl : 0);
   if (need > GM_NOALLOC_SCRATCH_BYTES) return GM_ERR_INVALID;

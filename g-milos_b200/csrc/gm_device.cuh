@@ -48,6 +48,8 @@ struct DevCfg {
   double lambda0, toplim, stop_dchi2;
   double init[11];
   const float* slight;   // device [4][nl] or [P][4][nl]
+  int lambda_per_pixel;  // 1: pixel p's absolute wavelengths are lam_map[p][0..nl)
+  const double* lam_map; // device [P][nl] (per-pixel grids) or null
 };
 
 // --------------------------------------------------------------- warp utils
@@ -263,13 +265,14 @@ __device__ __forceinline__ void psf_rows(WarpSmem<LPL, V>& sm, const DevCfg& c, 
 // derivative with respect to v_mac, g / v_mac * (x^2 - 1) (me_der.cu:122-129),
 // in sm.gd.  With a PSF both are then correlated with it in double, zero
 // padded about nl/2 (direct_convolution_double, convolution.cu:120-151;
-// mil_sinrf.cu:105-107, me_der.cu:131-136).
+// mil_sinrf.cu:105-107, me_der.cu:131-136).  lamp: the pixel's own
+// wavelengths, or null for the configured grid.
 template <int LPL, int V>
 __device__ __forceinline__ void mac_kernels(const DevCfg& c, WarpSmem<LPL, V>& sm, double mac,
-                                            int lane, bool deriv) {
+                                            int lane, bool deriv, const double* lamp) {
   const int nl = c.nl, half = nl >> 1;
   const double ild = (c.lambda0 * mac) / kVlight;
-  const double lc = c.lam[half];
+  const double lc = lamp ? lamp[half] : c.lam[half];
   double g[LPL], x2[LPL], part = 0.0;
 #pragma unroll
   for (int k = 0; k < LPL; ++k) {
@@ -277,7 +280,7 @@ __device__ __forceinline__ void mac_kernels(const DevCfg& c, WarpSmem<LPL, V>& s
     g[k] = 0.0;
     x2[k] = 0.0;
     if (l < nl) {
-      const double x = (c.lam[l] - lc) / ild;
+      const double x = ((lamp ? lamp[l] : c.lam[l]) - lc) / ild;
       const double term = (x * x) / 2;
       g[k] = term < 1e30 ? exp(-term) : 0.0;
       x2[k] = x * x;
@@ -370,7 +373,8 @@ template <int LPL, int V>
 __device__ __forceinline__ void synth_lane(const DevCfg& c, const double* m, const float (&dlv)[LPL],
                                            int lane, Lane<LPL, V>& st, Angles& an,
                                            float (&spec)[LPL][4], float (&pure)[LPL][4],
-                                           const float (&sl)[LPL][4], WarpSmem<LPL, V>& sm) {
+                                           const float (&sl)[LPL][4], WarpSmem<LPL, V>& sm,
+                                           const double* lamp = nullptr) {
   const float CC = (float)(kPi / 180.0), CC2 = (float)((kPi / 180.0) * 2);
   const double azi = m[AZ] * (double)CC, gmr = m[GM] * (double)CC;
   float sgm, cgm;
@@ -463,7 +467,7 @@ __device__ __forceinline__ void synth_lane(const DevCfg& c, const double* m, con
   if (mac_on) {
     // macroturbulence with the PSF folded into its kernel; the PSF is not
     // applied again (mil_sinrf.cu:101-130)
-    mac_kernels<LPL, V>(c, sm, m[MAC], lane, false);
+    mac_kernels<LPL, V>(c, sm, m[MAC], lane, false, lamp);
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
       float row[LPL];
@@ -534,7 +538,8 @@ __device__ __forceinline__ uint32_t rf_row_mask(const DevCfg& c) {
 // (FijaACeroDerivadasNoNecesarias, milosUtils.cu:243-271).
 template <int LPL, int V>
 __device__ __forceinline__ void rf_rows(const DevCfg& c, const double* m, const Lane<LPL, V>& st,
-                                        const Angles& an, int lane, WarpSmem<LPL, V>& sm) {
+                                        const Angles& an, int lane, WarpSmem<LPL, V>& sm,
+                                        const double* lamp = nullptr) {
   const float auxCte = __fdividef((float)(-c.lambda0), (float)(kVlight * m[DOPP]));
   const double aa = m[AA], dopp = m[DOPP];
   // last component of each group: its scaled splitting and strength
@@ -686,7 +691,7 @@ __device__ __forceinline__ void rf_rows(const DevCfg& c, const double* m, const 
       // macroturbulence (me_der.cu:117-156): the v_mac RF is the profile
       // before convolution through the kernel's derivative; every other
       // staged RF goes through the kernel (PSF folded into both)
-      mac_kernels<LPL, V>(c, sm, m[MAC], lane, true);
+      mac_kernels<LPL, V>(c, sm, m[MAC], lane, true, lamp);
 #pragma unroll
       for (int s = 0; s < 4; ++s) {
         float row[LPL];

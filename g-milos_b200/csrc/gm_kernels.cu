@@ -15,6 +15,26 @@ __device__ __forceinline__ void load_pixel(const float* __restrict__ p, int nl, 
   }
 }
 
+// Per-pixel wavelength grids: this pixel's offsets from row pix of the map
+// (the same double difference and float rounding the host applies to the
+// configured grid) and its absolute wavelengths; null with the configured grid.
+template <int LPL>
+__device__ __forceinline__ const double* pixel_grid(const DevCfg& c, unsigned long long pix, int lane,
+                                                    float (&dlv)[LPL], double (&dld)[LPL]) {
+  if (!c.lambda_per_pixel) return nullptr;
+  const double* lp = c.lam_map + pix * (unsigned long long)c.nl;
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+    if (l < c.nl) {
+      const double d = __ldg(lp + l) - c.lambda0;
+      dld[k] = d;
+      dlv[k] = (float)d;
+    }
+  }
+  return lp;
+}
+
 template <int LPL, int V>
 __device__ __forceinline__ void zero_padding(WarpSmem<LPL, V>& sm, int lane) {
   for (int i = lane; i < WarpSmem<LPL, V>::NR * 64 * LPL; i += 32) (&sm.rows[0][0])[i] = 0.f;
@@ -80,6 +100,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
     float ob[LPL][4];
     load_pixel<LPL>(a.iquv + off, nl, lane, ob);
     if (c.use_slight && c.slight_per_pixel) load_pixel<LPL>(c.slight + off, nl, lane, slg);
+    const double* lamp = pixel_grid<LPL>(c, pix, lane, dlv, dld);
 
     // initial model
     if (lane < 11) sm.m[lane] = a.init_models ? a.init_models[pix * 11 + lane] : c.init[lane];
@@ -110,7 +131,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
         }
         __syncwarp();
       }
-      synth_lane<LPL, V>(c, first ? sm.m : sm.t, dlv, lane, ln, an, syn, pure, slg, sm);
+      synth_lane<LPL, V>(c, first ? sm.m : sm.t, dlv, lane, ln, an, syn, pure, slg, sm, lamp);
       const float chisqr = chisq<LPL>(c, syn, ob, valid);
       bool accept = first;
       if (!first) {
@@ -148,7 +169,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
       if (accept) {
         // response functions and normal equations at the accepted model; the
         // alpha RF uses the mixed profile after the first step (milosUtils.cu:675)
-        rf_rows<LPL, V>(c, sm.m, ln, an, lane, sm);
+        rf_rows<LPL, V>(c, sm.m, ln, an, lane, sm, lamp);
         normal_eq<LPL, V>(c, sm.m, !first && c.quirks, pure, slg, syn, ob, valid, lane, sm);
         ochisqr = chisqr;
       }
@@ -206,10 +227,12 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
   zero_padding<LPL, V>(sm, lane);
   const int nl = c.nl;
   float dlv[LPL];
+  double dld[LPL];
 #pragma unroll
   for (int k = 0; k < LPL; ++k) {
     const int l = lane + 32 * k;
     dlv[k] = (l < nl) ? c.dl[l] : 0.f;
+    dld[k] = 0.0;
   }
   float slg[LPL][4];
   if (c.use_slight && !c.slight_per_pixel) load_pixel<LPL>(c.slight, nl, lane, slg);
@@ -226,10 +249,11 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
     if (c.use_slight && c.slight_per_pixel) load_pixel<LPL>(c.slight + off, nl, lane, slg);
     if (lane < 11) sm.m[lane] = a.models_f64 ? a.models_f64[pix * 11 + lane] : (double)a.models_f32[pix * 11 + lane];
     __syncwarp();
+    const double* lamp = pixel_grid<LPL>(c, (unsigned long long)pix, lane, dlv, dld);
     Lane<LPL, V> ln;
     Angles an;
     float syn[LPL][4], pure[LPL][4];
-    synth_lane<LPL, V>(c, sm.m, dlv, lane, ln, an, syn, pure, slg, sm);
+    synth_lane<LPL, V>(c, sm.m, dlv, lane, ln, an, syn, pure, slg, sm, lamp);
 #pragma unroll
     for (int k = 0; k < LPL; ++k) {
       const int l = lane + 32 * k;
@@ -238,7 +262,7 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
         for (int s = 0; s < 4; ++s) a.iquv[off + s * nl + l] = syn[k][s];
     }
     if (a.rf) {
-      rf_rows<LPL, V>(c, sm.m, ln, an, lane, sm);
+      rf_rows<LPL, V>(c, sm.m, ln, an, lane, sm, lamp);
       bool mac_on = false;
       if constexpr (Variant<V>::MAC) mac_on = sm.m[MAC] > 0.0001;
       const size_t roff = (size_t)pix * 4 * NT * nl;
@@ -278,8 +302,9 @@ __global__ void __launch_bounds__(128) classical_kernel(const DevCfg c, const fl
   }
   const int64_t nw = (int64_t)gridDim.x * 4;
   for (int64_t pix = (int64_t)blockIdx.x * 4 + w; pix < npix; pix += nw) {
-    float ob[LPL][4];
+    float ob[LPL][4], dlv[LPL];
     load_pixel<LPL>(iquv + (size_t)pix * 4 * nl, nl, lane, ob);
+    pixel_grid<LPL>(c, (unsigned long long)pix, lane, dlv, dld);
     if (lane < 11) ms[w][lane] = c.init[lane];
     __syncwarp();
     classical_warp<LPL>(c, ob, dld, valid, lane, ms[w], false);

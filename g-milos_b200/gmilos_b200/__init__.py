@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libgmilos.so")
 PKG_ROOT = os.path.dirname(HERE)
 MAX_NL = 64
 NPAR = 11
-ABI_VERSION = 1
+ABI_VERSION = 2
 PARAM_NAMES = ("eta0", "B", "vlos", "dopp", "aa", "gm", "az", "S0", "S1", "mac", "alfa")
 
 GM_OK = 0
@@ -62,7 +62,8 @@ class Config(C.Structure):
                 ("toplim", C.c_double), ("logclambda", C.c_int), ("stop_dchi2", C.c_double),
                 ("use_slight", C.c_int), ("slight_per_pixel", C.c_int),
                 ("slight", C.POINTER(C.c_float)), ("reference_quirks", C.c_int),
-                ("numerics", C.c_int)]
+                ("numerics", C.c_int), ("lambda_per_pixel", C.c_int),
+                ("lambda_map", C.POINTER(C.c_double))]
 
 
 class Request(C.Structure):
@@ -188,7 +189,12 @@ def psf_from_table(x_mA, y, offsets_mA, step_mA):
 def make_config(lam, lambda0, zeeman, psf=None, mu=1.0, weight=(1, 1, 1, 1), noise=1e-6,
                 fix=(1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0), init=None, init_mode=INIT_CLASSICAL,
                 miter=50, ilambda=0.1, toplim=1e-12, logclambda=0, stop_dchi2=0.0,
-                slight=None, slight_per_pixel=False, reference_quirks=1, numerics=0):
+                slight=None, slight_per_pixel=False, reference_quirks=1, numerics=0,
+                lambda_map=None):
+    """Engine configuration (gm_config).  lambda_map: optional per-pixel
+    wavelength grids [P][nl] (absolute, A; numpy or a CUDA tensor of float64),
+    read at each call like a per-pixel stray map; `lam` then only sizes the
+    grid and the PSF stays `psf`."""
     c = Config()
     lib().gm_config_defaults(C.byref(c))
     lam = np.asarray(lam, dtype=np.float64)
@@ -221,6 +227,18 @@ def make_config(lam, lambda0, zeeman, psf=None, mu=1.0, weight=(1, 1, 1, 1), noi
     c.reference_quirks = reference_quirks
     c.numerics = numerics
     c._slight_ref = None
+    c._lambda_ref = None
+    if lambda_map is not None:
+        c.lambda_per_pixel = 1
+        if hasattr(lambda_map, "data_ptr"):
+            c._lambda_ref = lambda_map
+            c.lambda_map = C.cast(C.c_void_p(lambda_map.data_ptr()), C.POINTER(C.c_double))
+        else:
+            arr = np.ascontiguousarray(lambda_map, dtype=np.float64)
+            if arr.ndim != 2 or arr.shape[1] != len(lam):
+                raise ValueError("lambda_map must be [P][nl]")
+            c._lambda_ref = arr
+            c.lambda_map = arr.ctypes.data_as(C.POINTER(C.c_double))
     if slight is not None:
         c.use_slight = 1
         c.slight_per_pixel = 1 if slight_per_pixel else 0

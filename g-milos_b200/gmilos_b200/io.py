@@ -56,6 +56,7 @@ def lib():
         L.gm_fits_write_models.argtypes = [cp, C.c_int, C.c_int, dp, ip, fp, C.c_int]
         L.gm_fits_read_stray.argtypes = [cp, C.c_int, C.POINTER(fp), ip, ip, ip]
         L.gm_fits_read_lambda.argtypes = [cp, dp, C.c_int, ip, ip]
+        L.gm_fits_read_lambda_map.argtypes = [cp, C.POINTER(dp), ip, ip, ip, ip, ip]
         L.gm_fits_write_image.argtypes = [cp, C.c_int, C.POINTER(C.c_int64), fp, C.POINTER(C.c_char_p), C.c_int]
         L.gm_io_free.argtypes = [vp]
         L.gm_io_free.restype = None
@@ -194,6 +195,20 @@ def read_lambda(path, cap=256):
     n, idx = C.c_int(), C.c_int()
     _check(lib().gm_fits_read_lambda(_b(path), _d(lam), cap, C.byref(n), C.byref(idx)))
     return lam[:n.value], idx.value
+
+
+def read_lambda_map(path):
+    """Wavelength FITS with one grid or per-pixel grids (gm_fits_read_lambda_map):
+    (grids [nl] or [P][nl], line index, per_pixel, rows, cols)."""
+    out = C.POINTER(C.c_double)()
+    pp, r, c, n, idx = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    _check(lib().gm_fits_read_lambda_map(_b(path), C.byref(out), C.byref(pp), C.byref(r), C.byref(c),
+                                         C.byref(n), C.byref(idx)))
+    P = r.value * c.value if pp.value else 1
+    g = np.ctypeslib.as_array(out, shape=(P * n.value,)).copy()
+    lib().gm_io_free(C.cast(out, C.c_void_p))
+    g = g.reshape(P, n.value) if pp.value else g
+    return g, idx.value, bool(pp.value), r.value, c.value
 
 
 def write_image(path, data, cards=()):

@@ -737,12 +737,52 @@ gm_status gm_fits_read_lambda(const char* path, double* lambda, int cap, int* nl
   gm_status st = fits_read(path, &img);
   if (st != GM_OK) return st;
   if (img.naxes.size() != 2 || img.naxes[1] < 2)
-    return io_fail(GM_ERR_IO, "wavelength FITS must be 2-D: line index row, wavelength row");
+    return io_fail(GM_ERR_IO, "wavelength FITS must be 2-D: line index row, wavelength row "
+                              "(per-pixel grids: gm_fits_read_lambda_map)");
   const int64_t n = img.naxes[0];
   if (n > cap) return io_fail(GM_ERR_IO, "too many wavelengths");
   *line_index = (int)img.data[(size_t)(n - 1)];
   for (int64_t i = 0; i < n; ++i) lambda[i] = img.data[(size_t)(n + i)];
   *nl = (int)n;
+  return GM_OK;
+}
+
+gm_status gm_fits_read_lambda_map(const char* path, double** out, int* per_pixel, int* rows, int* cols,
+                                  int* nl, int* line_index) {
+  *out = nullptr;
+  FitsImage img;
+  gm_status st = fits_read(path, &img);
+  if (st != GM_OK) return st;
+  const size_t na = img.naxes.size();
+  if (na == 2) {   // one grid: row 1 the line index, row 2 the wavelengths
+    const int64_t n = img.naxes[0];
+    if (img.naxes[1] < 2 || n < 2) return io_fail(GM_ERR_IO, "wavelength FITS must hold a line index and >= 2 wavelengths");
+    double* g = (double*)std::malloc(sizeof(double) * (size_t)n);
+    *line_index = (int)img.data[(size_t)(n - 1)];
+    for (int64_t i = 0; i < n; ++i) g[i] = img.data[(size_t)(n + i)];
+    *out = g;
+    *per_pixel = 0;
+    *rows = *cols = 1;
+    *nl = (int)n;
+    return GM_OK;
+  }
+  // per-pixel grids: NAXIS1 = rows, NAXIS2 = cols, NAXIS3 = 1 + nl (plane 0
+  // the line index, planes 1..nl the wavelengths), NAXIS4 = 1 if present
+  if ((na != 3 && na != 4) || (na == 4 && img.naxes[3] != 1) || img.naxes[2] < 3)
+    return io_fail(GM_ERR_IO, "per-pixel wavelength FITS must be rows x cols x (1 + nl)");
+  const int64_t R = img.naxes[0], Cc = img.naxes[1], n = img.naxes[2] - 1, P = R * Cc;
+  const int idx = (int)img.data[0];
+  for (int64_t p = 0; p < P; ++p)
+    if ((int)img.data[(size_t)p] != idx) return io_fail(GM_ERR_IO, "per-pixel wavelength FITS: one line index for all pixels");
+  double* m = (double*)std::malloc(sizeof(double) * (size_t)(P * n));
+  for (int64_t l = 0; l < n; ++l)
+    for (int64_t p = 0; p < P; ++p) m[(size_t)(p * n + l)] = img.data[(size_t)((l + 1) * P + p)];
+  *out = m;
+  *per_pixel = 1;
+  *rows = (int)R;
+  *cols = (int)Cc;
+  *nl = (int)n;
+  *line_index = idx;
   return GM_OK;
 }
 

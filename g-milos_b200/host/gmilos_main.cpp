@@ -65,10 +65,12 @@ struct Cleanup {
   gm_ctx* ctx = nullptr;
   gm_fits_cube* cube = nullptr;
   float* stray = nullptr;
+  double* lambda_map = nullptr;
   ~Cleanup() {
     if (ctx) gm_destroy(ctx);
     if (cube) gm_fits_cube_free(cube);
     if (stray) gm_io_free(stray);
+    if (lambda_map) gm_io_free(lambda_map);
   }
 };
 
@@ -111,7 +113,8 @@ int main(int argc, char** argv) {
 
   // ---- wavelengths and the line
   double lambda[GM_MAX_NL], offsets[GM_MAX_NL], quantum[6], lambda0 = 0, step_mA = 0;
-  int nl = 0, line_index = 0;
+  int nl = 0, line_index = 0, lam_rows = 1, lam_cols = 1;
+  Cleanup res;
   if (t.use_grid) {
     double first, last;
     if (gm_io_read_grid(t.grid, &line_index, &first, &step_mA, &last) != GM_OK) return die(gm_io_last_error());
@@ -119,8 +122,20 @@ int main(int argc, char** argv) {
     nl = gm_io_grid_wavelengths(lambda0, first, step_mA, last, offsets, lambda, GM_MAX_NL);
     if (nl < 2) return die("the grid must have 2.." + std::to_string(GM_MAX_NL) + " samples");
   } else {
-    if (gm_fits_read_lambda(t.wavelength, lambda, GM_MAX_NL, &nl, &line_index) != GM_OK)
+    // one grid (2-D FITS) or per-pixel grids (rows x cols x (1 + nl)); with
+    // per-pixel grids the first pixel's grid sets the PSF and the offsets
+    // written with .per outputs
+    double* grids = nullptr;
+    int per_pixel = 0;
+    if (gm_fits_read_lambda_map(t.wavelength, &grids, &per_pixel, &lam_rows, &lam_cols, &nl, &line_index) != GM_OK)
       return die(gm_io_last_error());
+    res.lambda_map = grids;
+    if (nl < 2 || nl > GM_MAX_NL) return die("the wavelength file must have 2.." + std::to_string(GM_MAX_NL) + " samples");
+    for (int i = 0; i < nl; ++i) lambda[i] = grids[i];
+    if (per_pixel) {
+      cfg.lambda_per_pixel = 1;
+      cfg.lambda_map = grids;
+    }
     if (gm_io_read_line(t.lines, line_index, &lambda0, quantum) != GM_OK) return die(gm_io_last_error());
     for (int i = 0; i < nl; ++i) offsets[i] = (lambda[i] - lambda0) * 1000.0;
     step_mA = (lambda[1] - lambda[0]) * 1000.0;
@@ -159,7 +174,6 @@ int main(int argc, char** argv) {
   cfg.init_mode = GM_INIT_CLASSICAL;
   cfg.numerics = numerics;
 
-  Cleanup res;
   // ---- stray light: one profile (.per or 2-D FITS) or a map (4-D FITS)
   int stray_rows = 0, stray_cols = 0;
   if (exists(t.stray)) {
@@ -191,6 +205,7 @@ int main(int argc, char** argv) {
   // ---- synthesis
   if (t.ncycles == 0) {
     if (cfg.slight_per_pixel) return die("synthesis takes one stray-light profile, not a map");
+    if (cfg.lambda_per_pixel) return die("synthesis takes one wavelength grid, not per-pixel grids");
     std::vector<float> spec(4 * nl);
     if (gm_synthesize_f64(res.ctx, cfg.init_model, 1, spec.data(), nullptr, nullptr) != GM_OK)
       return die(gm_last_error(res.ctx));
@@ -220,6 +235,8 @@ int main(int argc, char** argv) {
   }
   if (cfg.slight_per_pixel && (stray_rows != rows || stray_cols != cols))
     return die("the stray-light map's dimensions differ from the observed cube's");
+  if (cfg.lambda_per_pixel && (!fits_input || lam_rows != rows || lam_cols != cols))
+    return die("per-pixel wavelength grids need a FITS cube of the same rows and columns");
   if (cfg.slight_per_pixel) {
     // the per-pixel map travels with the call (gm_invert_ex reads cfg.slight)
   }

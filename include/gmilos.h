@@ -41,7 +41,7 @@ extern "C" {
 
 #define GM_MAX_NL 64          /* wavelength samples per pixel (reference: MAX_LAMBDA 50) */
 #define GM_NPAR 11
-#define GM_ABI_VERSION 1
+#define GM_ABI_VERSION 2
 
 typedef enum {
     GM_OK = 0,
@@ -110,6 +110,12 @@ typedef struct {
                                      an accepted step, milosUtils.cu:675) */
     int numerics;                 /* GM_NUMERICS_REFERENCE (default) or
                                      GM_NUMERICS_ACCURATE */
+    int lambda_per_pixel;         /* 0: every pixel on `lambda`; 1: pixel p on
+                                     lambda_map[p][0..nl) (read at each call, like
+                                     the per-pixel stray map).  The PSF taps stay
+                                     those of `psf`.  The reference's per-pixel
+                                     wavelength FITS (utilsFits.c:1488-1500). */
+    const double *lambda_map;     /* [P][nl] absolute wavelengths [A], host or device */
 } gm_config;
 
 /* Trigonometry of the 10x10 Jacobi solve and of the field angles.
@@ -163,7 +169,7 @@ gm_status gm_invert_ex(gm_ctx *ctx, const float *iquv, int64_t npix, int nl,
  * All calls share the array: calls that overlap on the GPU race, so serialise
  * them (one stream, or events).  Errors are reported by status only:
  * GM_ERR_INVALID (bad configuration, host pointer, or scratch over the
- * maximum), GM_ERR_UNSUPPORTED, GM_ERR_CUDA. */
+ * maximum), GM_ERR_UNSUPPORTED (per-pixel wavelength grids), GM_ERR_CUDA. */
 #define GM_NOALLOC_SCRATCH_BYTES 4096
 gm_status gm_invert_noalloc(const gm_config *cfg, const float *iquv, int64_t npix, int nl,
                             float *model, float *chi2, int *iters, float *fitted,
@@ -206,8 +212,11 @@ gm_status gm_synthesize_grid(gm_ctx *ctx, const double *models, int64_t npix,
  * chunks of chunk_pixels; `streams` lanes each keep one chunk on the device,
  * taken round robin from the admitted requests, so requests that arrive
  * while others run start within one chunk time and their work overlaps on
- * the device.  Per-pixel results do not depend on the mix.  No counterpart
- * in the reference (its main inverts one cube per process run). */
+ * the device.  Per-pixel results do not depend on the mix.  Requests share
+ * the configured stray-light profile and wavelength grid: a configuration
+ * with per-pixel stray maps or per-pixel grids is refused with
+ * GM_ERR_UNSUPPORTED.  No counterpart in the reference (its main inverts one
+ * cube per process run). */
 typedef uint64_t gm_ticket;
 typedef struct {
     const float *iquv;            /* [P][4][nl] host or device */

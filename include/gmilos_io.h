@@ -130,8 +130,20 @@ gm_status gm_fits_write_models(const char *path, int rows, int cols, const doubl
 gm_status gm_fits_read_stray(const char *path, int nl, float **out, int *per_pixel, int *rows,
                              int *cols);
 
-/* Wavelength file: NAXIS = 2, row 1 = line index, row 2 = wavelengths [A]. */
+/* Wavelength file: NAXIS = 2, row 1 = line index, row 2 = wavelengths [A]
+ * (readFitsLambdaToArray, utilsFits.c:1446-1487). */
 gm_status gm_fits_read_lambda(const char *path, double *lambda, int cap, int *nl, int *line_index);
+
+/* Wavelength file with one grid (2-D, as above; *per_pixel = 0, *out [nl])
+ * or per-pixel grids (*per_pixel = 1, *out [P][nl], pixel p = col * rows +
+ * row as in gm_fits_read_cube): NAXIS1 = rows, NAXIS2 = cols, NAXIS3 =
+ * 1 + nl, optional NAXIS4 = 1; plane 0 holds the line index (the same in
+ * every pixel), planes 1..nl the pixel's wavelengths [A] -- the 2-D layout
+ * with pixels added.  The reference meant its 4-D branch for this
+ * (utilsFits.c:1488-1500) but reads it into a NULL pointer.  BITPIX -64
+ * keeps the wavelengths exact.  *out is malloc'd; free with gm_io_free. */
+gm_status gm_fits_read_lambda_map(const char *path, double **out, int *per_pixel, int *rows, int *cols,
+                                  int *nl, int *line_index);
 
 /* Generic single-HDU float image (for tests and tools): naxes[0] fastest. */
 gm_status gm_fits_write_image(const char *path, int naxis, const int64_t *naxes, const float *data,

@@ -59,6 +59,17 @@ def test_config_defaults_follow_reference():
     assert c.toplim == 1e-12
     assert c.mu == 1.0
     assert c.reference_quirks == 1
+    assert c.lambda_per_pixel == 0 and not c.lambda_map
+
+
+def test_per_pixel_wavelength_map_binding():
+    lam = np.linspace(6172.9, 6173.9, 30)
+    lmap = np.repeat(lam[None], 5, 0) + np.arange(5)[:, None] * 1e-3
+    c = G.make_config(lam, 6173.3356, G.zeeman_from_levels(2, 1, 1.0, 2, 2, 0.0, 1.0), lambda_map=lmap)
+    assert c.lambda_per_pixel == 1
+    assert c.lambda_map[4 * 30 + 29] == lmap[4, 29]
+    with pytest.raises(ValueError):
+        G.make_config(lam, 6173.3356, G.zeeman_from_levels(2, 1, 1.0, 2, 2, 0.0, 1.0), lambda_map=lmap[:, :10])
 
 
 @pytest.mark.parametrize("levels", [(2, 1, 1.0, 2, 2, 0.0), (2, 2, 0.0, 3, 2, 1.0),

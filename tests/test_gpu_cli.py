@@ -35,7 +35,7 @@ FIELDS = ["Number of cycles          (*)", "Observed profiles          (*)", "St
           "Number of Streams            ", "Device number                "]
 
 
-def setup_dir(d, ncycles, observed="", stray="", init=None, stray_free=0, mac_free=0):
+def setup_dir(d, ncycles, observed="", stray="", init=None, stray_free=0, mac_free=0, wavelength="malla.grid"):
     """Line list, grid, PSF table and guess model of the known-answer case."""
     g = H.kat()
     (d / "LINES").write_text("1=FE 1   6173.3356    1.0  2.223 -2.880   5P 1.0- 5D 0.0  0.266  7.868e-15\n")
@@ -50,7 +50,7 @@ def setup_dir(d, ncycles, observed="", stray="", init=None, stray_free=0, mac_fr
     names = ["eta_0", "magnetic field", "LOS velocity", "Doppler width", "damping", "gamma", "phi", "S_0",
              "S_1", "v_mac", "filling factor"]
     (d / "guess.mod").write_text("".join("%s: %.10g\n" % (n, v) for n, v in zip(names, m)))
-    vals = [str(ncycles), observed, stray, "crisp.psf", "malla.grid", "LINES", "", "guess.mod", "", "1", "1",
+    vals = [str(ncycles), observed, stray, "crisp.psf", wavelength, "LINES", "", "guess.mod", "", "1", "1",
             "1", "1", "", "1", "1", "1", "1", "1", "1", "1", "1", "1", str(mac_free)] + [""] * 10 + \
            ["", str(stray_free), "1", "1000", "", "0.1", "0", "0", "4", "0"]
     with open(d / "run.mtrol", "w") as f:
@@ -156,3 +156,46 @@ def test_classical_estimates_mode(tmp_path):
             for k in (1, 2, 5, 6, 7):      # B, vlos, gamma, phi and S0 = B_los
                 assert got[k] == pytest.approx(ref[k], rel=1e-5, abs=1e-4), (k, got[k], ref[k])
             assert planes[11, cc, rr] == 0 and planes[12, cc, rr] == 0
+
+
+def test_fits_inversion_on_per_pixel_wavelength_grids(tmp_path):
+    """A per-pixel wavelength FITS (rows x cols x (1 + nl)): the CLI inverts
+    each pixel on its own grid, with the PSF of the first pixel's grid, as the
+    engine API does with lambda_map."""
+    from test_io import cube_file, lambda_map_planes, write_f64_image
+    g = setup_dir(tmp_path, 30, observed="cube.fits", init=H.GUESS, wavelength="lmap.fits")
+    rows, cols = 5, 4
+    P = rows * cols
+    rng = np.random.default_rng(7)
+    l0, zo = H.fe_line()
+    first, step, last = g["grid"]
+    lam0 = G.grid_lambda(l0, first, step, last)
+    grids = lam0[None] + rng.uniform(-0.02, 0.02, (P, 1))
+    write_f64_image(tmp_path / "lmap.fits", lambda_map_planes(grids, rows, cols))
+    off0 = (grids[0] - l0) * 1000.0
+    x, y = gio.read_psf_table(tmp_path / "crisp.psf")
+    psf = G.psf_from_table(x, y, off0, (grids[0][1] - grids[0][0]) * 1000.0)
+    t = H.truth_models(P, rng)
+    obs = np.stack([O.synth_f(O.make_cfg(grids[p], l0, zo, psf=psf), t[p]) for p in range(P)])
+    obs = np.ascontiguousarray(obs + rng.normal(0, 1e-3, obs.shape), dtype=np.float32)
+    cube_file(tmp_path / "cube.fits", obs, rows, cols, ("lam", "stokes", "row", "col"))
+    run_cli(tmp_path)
+    planes, _ = gio.read_image(tmp_path / "cube_mod.fits")
+    cfg = G.make_config(grids[0], l0, G.zeeman_from_levels(2, 1, 1.0, 2, 2, 0.0, 1.0), psf=psf,
+                        init=H.GUESS, miter=30, lambda_map=grids)
+    one = G.make_config(grids[0], l0, G.zeeman_from_levels(2, 1, 1.0, 2, 2, 0.0, 1.0), psf=psf,
+                        init=H.GUESS, miter=30)
+    with G.Engine(0) as e:
+        e.configure(cfg)
+        out = e.invert(obs)
+        e.configure(one)
+        single = e.invert(obs)
+    for rr in range(rows):
+        for cc in range(cols):
+            p = cc * rows + rr
+            np.testing.assert_allclose(planes[:11, cc, rr], out["model"][p], rtol=1e-6)
+            assert planes[11, cc, rr] == out["iters"][p]
+    # the map is applied per pixel: pixel 0, whose grid is the single grid,
+    # comes out bit-identical to a single-grid run; every other pixel differs
+    np.testing.assert_array_equal(out["model64"][0], single["model64"][0])
+    assert (np.abs(out["model64"][1:] - single["model64"][1:]).max(axis=1) > 0).all()

@@ -238,3 +238,54 @@ def test_fits_models_and_stray_and_lambda(tmp_path):
     got, idx = gio.read_lambda(tmp_path / "l.fits")
     assert idx == 1
     np.testing.assert_allclose(got, lam.astype(np.float32))
+
+
+def write_f64_image(path, data):
+    """BITPIX -64 image, NAXIS1 = the last numpy axis (wavelengths kept exact)."""
+    a = np.ascontiguousarray(data, dtype=">f8")
+    cards = ["SIMPLE  = %20s" % "T", "BITPIX  = %20d" % -64, "NAXIS   = %20d" % a.ndim]
+    cards += ["NAXIS%-3d= %20d" % (i + 1, n) for i, n in enumerate(reversed(a.shape))]
+    cards.append("END")
+    hdr = "".join(c.ljust(80) for c in cards)
+    hdr = hdr.ljust((len(hdr) + 2879) // 2880 * 2880)
+    body = a.tobytes()
+    body += b"\0" * ((-len(body)) % 2880)
+    with open(path, "wb") as f:
+        f.write(hdr.encode() + body)
+
+
+def lambda_map_planes(grids, rows, cols, line_index=1):
+    """[1 + nl][cols][rows] planes of a per-pixel wavelength FITS; pixel p =
+    col * rows + row as in the cube reader."""
+    P, nl = grids.shape
+    arr = np.zeros((nl + 1, cols, rows))
+    arr[0] = line_index
+    for r in range(rows):
+        for c in range(cols):
+            arr[1:, c, r] = grids[c * rows + r]
+    return arr
+
+
+def test_per_pixel_wavelength_fits(tmp_path):
+    rows, cols, nl = 3, 4, 7
+    P = rows * cols
+    rng = np.random.default_rng(11)
+    grids = 6173.0 + np.arange(nl) * 0.035 + rng.uniform(-0.02, 0.02, (P, 1))
+    arr = lambda_map_planes(grids, rows, cols)
+    write_f64_image(tmp_path / "lmap3.fits", arr)
+    write_f64_image(tmp_path / "lmap4.fits", arr[None])
+    for f in ("lmap3.fits", "lmap4.fits"):
+        g, idx, per_pixel, r, c = gio.read_lambda_map(tmp_path / f)
+        assert per_pixel and (r, c) == (rows, cols) and idx == 1
+        np.testing.assert_array_equal(g, grids)
+    # one grid, 2-D: line index row, wavelength row
+    write_f64_image(tmp_path / "l2.fits", np.stack([np.full(nl, 2.0), grids[0]]))
+    g, idx, per_pixel, r, c = gio.read_lambda_map(tmp_path / "l2.fits")
+    assert not per_pixel and idx == 2
+    np.testing.assert_array_equal(g, grids[0])
+    with pytest.raises(gio.GmError):          # the 2-D reader points to the map reader
+        gio.read_lambda(tmp_path / "lmap3.fits")
+    arr[0, 1, 2] = 2                           # one line per run
+    write_f64_image(tmp_path / "bad.fits", arr)
+    with pytest.raises(gio.GmError):
+        gio.read_lambda_map(tmp_path / "bad.fits")
