@@ -204,20 +204,8 @@ gm_status build_devcfg(gm_ctx* ctx, const gm_config& c, gm::DevCfg* d) {
     const double off = c.lambda[l] - c.lambda0;
     d->dl[l] = (float)off;
     d->dld[l] = off;
-    d->psf[l] = (float)c.psf[l];
     d->psfd[l] = c.psf[l];
     d->lam[l] = c.lambda[l];
-  }
-  // Taps whose weight is below 1e-10 of the largest contribute less than
-  // float resolution to any sample (their total is < 1e-8 of the sum): the
-  // convolution skips them.
-  double hmax = 0.0;
-  for (int l = 0; l < c.nl; ++l) hmax = std::max(hmax, std::fabs(c.psf[l]));
-  d->tap_lo = 0;
-  d->tap_hi = c.nl - 1;
-  if (c.use_psf && hmax > 0) {
-    while (d->tap_lo < d->tap_hi && std::fabs(c.psf[d->tap_lo]) <= 1e-10 * hmax) ++d->tap_lo;
-    while (d->tap_hi > d->tap_lo && std::fabs(c.psf[d->tap_hi]) <= 1e-10 * hmax) --d->tap_hi;
   }
   for (int i = 0; i < 10; ++i) {
     d->nup[i] = z.nup[i];

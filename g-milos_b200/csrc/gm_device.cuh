@@ -33,13 +33,11 @@ struct DevCfg {
   int use_psf, use_slight, slight_per_pixel;
   int init_mode, miter, logclambda, quirks;
   int numerics;          // 0: reference intrinsics, 1: accurate trigonometry
-  int tap_lo, tap_hi;    // PSF taps outside [tap_lo, tap_hi] are below float resolution
   int n_pi, n_sig;
   int fix[11];
   float dl[kMaxNl];      // (float)(lambda - lambda0), the reference's sub_aux
   double dld[kMaxNl];    // lambda - lambda0 in double (classical estimates)
-  float psf[kMaxNl];     // PSF taps
-  double psfd[kMaxNl];   // the same taps in double (folded into the macroturbulence kernel)
+  double psfd[kMaxNl];   // PSF taps (double, as the reference's psfFunction)
   double lam[kMaxNl];    // absolute wavelengths (macroturbulence kernel)
   float nup[10], nub[10], wep[10], web[10], wer[10];
   float geff, fo, mu, ilambda, noise;
@@ -163,8 +161,27 @@ struct Lane {
 constexpr int kRows = 32;
 __host__ __device__ constexpr int rf_row(int s, int t) { return s * 8 + (t == 8 ? 7 : t); }
 __host__ __device__ constexpr int mac_row(int s) { return kRows + s; }
+// A staged row holds samples [0, 32 LPL) (zero past nl); its pitch of
+// 32 LPL + 4 floats puts the 8 rows of a tensor-core fragment in distinct
+// shared-memory banks.
 template <int LPL>
-__host__ __device__ constexpr int row_off() { return 16 * LPL; }   // samples at [16 LPL, 48 LPL)
+__host__ __device__ constexpr int row_pitch() { return 32 * LPL + 4; }
+
+// Dynamic shared memory of the inversion and synthesis kernels: the block's
+// PSF taps (block_taps), then one WarpSmem per warp.
+extern __shared__ __align__(16) unsigned char gm_dyn_smem[];
+
+// The PSF taps in double, zero padded, shared by the warps of a block: tap j
+// of the nl-tap PSF at index tap_off + j of tap_span doubles.  The padding
+// lets every lane read its Toeplitz element of the convolution matrix with one
+// load and no bounds test.
+template <int LPL>
+__host__ __device__ constexpr int tap_span() { return 96 * LPL; }
+template <int LPL>
+__host__ __device__ constexpr int tap_off() { return 32 * LPL; }
+template <int LPL>
+__host__ __device__ constexpr size_t tap_bytes() { return sizeof(double) * tap_span<LPL>(); }
+__device__ __forceinline__ double* block_taps() { return reinterpret_cast<double*>(gm_dyn_smem); }
 
 // Warp-private shared memory.
 template <int LPL, int V>
@@ -188,7 +205,7 @@ struct WarpSmem {
   double V11[S11 ? 2 : 1][S11 ? 144 : 1];    // its accumulated rotations
   double b11[S11 ? 12 : 1], z11[S11 ? 12 : 1];
   double c11[S11 ? 6 : 1], s11[S11 ? 6 : 1]; // the step's rotations
-  float rows[NR][64 * LPL];   // zero-padded rows for the PSF
+  float rows[NR][row_pitch<LPL>()];   // staged rows (PSF, macroturbulence, RFs)
 };
 
 template <int LPL>
@@ -216,43 +233,85 @@ __device__ __forceinline__ void put_row(WarpSmem<LPL, V>& sm, int r, const float
 #pragma unroll
   for (int k = 0; k < LPL; ++k) {
     const int l = lane + 32 * k;
-    sm.rows[r][row_off<LPL>() + l] = (l < nl) ? (reflect ? ic - x[k] : x[k]) : 0.f;
+    sm.rows[r][l] = (l < nl) ? (reflect ? ic - x[k] : x[k]) : 0.f;
   }
 }
 
+// Load the block's padded PSF taps (all threads of the block, once).
+template <int LPL>
+__device__ __forceinline__ void load_taps(const DevCfg& c) {
+  double* taps = block_taps();
+  for (int i = threadIdx.x; i < tap_span<LPL>(); i += blockDim.x) {
+    const int j = i - tap_off<LPL>();
+    taps[i] = (c.use_psf && j >= 0 && j < c.nl) ? c.psfd[j] : 0.0;
+  }
+  __syncthreads();
+}
+
+// D += A B on the FP64 tensor cores: an 8x8 tile from an 8x4 by 4x8 product.
+// Lane l holds A[l / 4][l % 4], B[l % 4][l / 4] and D[l / 4][2 (l % 4) + i].
+__device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
 // In-place same-size correlation of the staged rows in `mask` with the
-// nl-tap PSF centred at nl/2, zero padded, two partial sums over even and
-// odd taps (direct_convolution{,_ic}, convolution.cu:153-241); rows in
-// `reflect` are reflected back about sm.ic.  The caller syncs the warp after
-// staging.  One loop over rows keeps the code small whatever the row count.
+// nl-tap PSF centred at nl/2, zero padded, in double -- the reference's
+// direct_convolution{,_ic} (convolution.cu:153-241), whose taps, padded row
+// and sums are double and whose result is rounded to float once.  Rows in
+// `reflect` are reflected back about sm.ic in double as there.  The
+// correlation is the product out = X T of the staged rows X (8-row tiles) and
+// the Toeplitz matrix T[n][m] = h[n - m + nl/2] (zero outside the taps, which
+// is the zero padding), on the FP64 tensor cores; only the order of the double
+// additions differs from the reference.  A tile holding a row outside `mask`
+// computes it but stores only the rows in `mask`.  The caller syncs the warp
+// after staging.
 template <int LPL, int V>
 __device__ __forceinline__ void psf_rows(WarpSmem<LPL, V>& sm, const DevCfg& c, uint32_t mask,
                                          uint32_t reflect, int lane) {
+  constexpr int S = 32 * LPL;                 // samples per row: the K and N extents
   const int nl = c.nl, half = nl >> 1;
-  (void)nl;
+  const int gr = lane >> 2, gc = lane & 3;   // fragment row group, column group
+  // this lane's B element of step (k0, n0): T[k0 + gc][n0 + gr]
+  const double* tb = block_taps() + tap_off<LPL>() + half + gc - gr;
   while (mask) {
-    const int r = __ffs(mask) - 1;
-    mask &= mask - 1;
-    float out[LPL];
+    const int mt = (__ffs(mask) - 1) >> 3;    // 8-row tile of the next staged row
+    const uint32_t tile = (mask >> (8 * mt)) & 0xffu;
+    mask &= ~(0xffu << (8 * mt));
+    const int r = 8 * mt + gr;
+    const float* arow = sm.rows[r];
+    const bool mine = (tile >> gr) & 1u;
+    const bool refl = (reflect >> r) & 1u;
+    const double ic = refl ? (double)sm.ic[r] : 0.0;
+    float res[LPL][4][2];
 #pragma unroll
-    for (int k = 0; k < LPL; ++k) {
-      const float* base = sm.rows[r] + row_off<LPL>() + lane + 32 * k - half;
-      float a0 = 0.f, a1 = 0.f;
-      int j = c.tap_lo;
-      for (; j < c.tap_hi; j += 2) {
-        a0 = fmaf(c.psf[j], base[j], a0);
-        a1 = fmaf(c.psf[j + 1], base[j + 1], a1);
+    for (int p = 0; p < LPL; ++p) {           // output columns in passes of 32
+      double acc[4][2];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[q][0] = acc[q][1] = 0.0;
+#pragma unroll 2
+      for (int k0 = 0; k0 < S; k0 += 4) {
+        const double a = (double)arow[k0 + gc];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dmma_884(acc[q][0], acc[q][1], a, tb[k0 - 8 * (4 * p + q)]);
       }
-      if (j == c.tap_hi) a0 = fmaf(c.psf[j], base[j], a0);
-      out[k] = a0 + a1;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) res[p][q][i] = (float)(refl ? ic - acc[q][i] : acc[q][i]);
     }
     __syncwarp();
-    const bool refl = (reflect >> r) & 1u;
-    const float ic = refl ? sm.ic[r] : 0.f;
+    if (mine) {
 #pragma unroll
-    for (int k = 0; k < LPL; ++k) {
-      const int l = lane + 32 * k;
-      sm.rows[r][row_off<LPL>() + l] = (l < nl) ? (refl ? ic - out[k] : out[k]) : 0.f;
+      for (int p = 0; p < LPL; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            const int m = 32 * p + 8 * q + 2 * gc + i;
+            sm.rows[r][m] = (m < nl) ? res[p][q][i] : 0.f;
+          }
     }
   }
   __syncwarp();
@@ -339,7 +398,7 @@ __device__ __forceinline__ void circ_rows(WarpSmem<LPL, V>& sm, const DevCfg& c,
   while (mask) {
     const int r = __ffsll((long long)mask) - 1;
     mask &= mask - 1;
-    const float* x = sm.rows[r] + row_off<LPL>();
+    const float* x = sm.rows[r];
     float out[LPL];
 #pragma unroll
     for (int k = 0; k < LPL; ++k) {
@@ -359,7 +418,7 @@ __device__ __forceinline__ void circ_rows(WarpSmem<LPL, V>& sm, const DevCfg& c,
 #pragma unroll
     for (int k = 0; k < LPL; ++k) {
       const int mo = lane + 32 * k;
-      if (mo < nl) sm.rows[r][row_off<LPL>() + mo] = out[k];
+      if (mo < nl) sm.rows[r][mo] = out[k];
     }
   }
   __syncwarp();
@@ -480,7 +539,7 @@ __device__ __forceinline__ void synth_lane(const DevCfg& c, const double* m, con
 #pragma unroll
     for (int k = 0; k < LPL; ++k)
 #pragma unroll
-      for (int s = 0; s < 4; ++s) spec[k][s] = sm.rows[s][row_off<LPL>() + lane + 32 * k];
+      for (int s = 0; s < 4; ++s) spec[k][s] = sm.rows[s][lane + 32 * k];
     __syncwarp();
   } else if (c.use_psf) {
     __syncwarp();
@@ -496,7 +555,7 @@ __device__ __forceinline__ void synth_lane(const DevCfg& c, const double* m, con
 #pragma unroll
     for (int k = 0; k < LPL; ++k)
 #pragma unroll
-      for (int s = 0; s < 4; ++s) spec[k][s] = sm.rows[s][row_off<LPL>() + lane + 32 * k];
+      for (int s = 0; s < 4; ++s) spec[k][s] = sm.rows[s][lane + 32 * k];
     __syncwarp();
   }
 #pragma unroll
@@ -678,7 +737,7 @@ __device__ __forceinline__ void rf_rows(const DevCfg& c, const double* m, const 
 #pragma unroll
       for (int s = 0; s < 4; ++s) {
         const int r = rf_row(s, il);
-        if ((mask >> r) & 1u) sm.rows[r][row_off<LPL>() + l] = (l < nl) ? o[s] : 0.f;
+        if ((mask >> r) & 1u) sm.rows[r][l] = (l < nl) ? o[s] : 0.f;
       }
     }
   }
@@ -713,8 +772,8 @@ __device__ __forceinline__ void rf_rows(const DevCfg& c, const double* m, const 
       icv[tt] = 0.f;
       if (!((mask >> r) & 1u)) continue;
       refl |= 1u << r;
-      const float f0 = sm.rows[r][row_off<LPL>()];
-      const float f1 = sm.rows[r][row_off<LPL>() + nl - 1];
+      const float f0 = sm.rows[r][0];
+      const float f1 = sm.rows[r][nl - 1];
       icv[tt] = f0 > f1 ? f0 : f1;
       if (lane == 0) sm.ic[r] = icv[tt];
     }
@@ -726,7 +785,7 @@ __device__ __forceinline__ void rf_rows(const DevCfg& c, const double* m, const 
 #pragma unroll
       for (int k = 0; k < LPL; ++k) {
         const int l = lane + 32 * k;
-        if (l < nl) sm.rows[r][row_off<LPL>() + l] = icv[tt] - sm.rows[r][row_off<LPL>() + l];
+        if (l < nl) sm.rows[r][l] = icv[tt] - sm.rows[r][l];
       }
     }
     __syncwarp();
@@ -753,20 +812,20 @@ __device__ __forceinline__ float gather_rf(const DevCfg& c, const WarpSmem<LPL, 
     // me_der wrote there (me_der.cu:140-143)
     if (c.use_slight) return asrc - sl;
     if constexpr (Variant<V>::MAC && NT == 10) {
-      if (mac_on) return sm.rows[mac_row(s)][row_off<LPL>() + l];
+      if (mac_on) return sm.rows[mac_row(s)][l];
     }
     return 0.f;
   }
   if (t == 9) {
     if constexpr (Variant<V>::MAC) {
-      if (mac_on) v = sm.rows[mac_row(s)][row_off<LPL>() + l];
+      if (mac_on) v = sm.rows[mac_row(s)][l];
     }
   } else if (t == 7) {
     v = (s == 0) ? 1.f : 0.f;
   } else if (t == 6 && (s == 0 || s == 3)) {
     v = 0.f;
   } else {
-    v = sm.rows[rf_row(s, t)][row_off<LPL>() + l];
+    v = sm.rows[rf_row(s, t)][l];
   }
   if (c.use_slight) v = (float)((double)v * alfa);
   return v;

@@ -35,19 +35,19 @@ __device__ __forceinline__ const double* pixel_grid(const DevCfg& c, unsigned lo
   return lp;
 }
 
+// Staged rows start at zero (rows that no phase stages then hold zeros in
+// the tensor-core tiles of the PSF).
 template <int LPL, int V>
-__device__ __forceinline__ void zero_padding(WarpSmem<LPL, V>& sm, int lane) {
-  for (int i = lane; i < WarpSmem<LPL, V>::NR * 64 * LPL; i += 32) (&sm.rows[0][0])[i] = 0.f;
+__device__ __forceinline__ void zero_rows(WarpSmem<LPL, V>& sm, int lane) {
+  for (int i = lane; i < WarpSmem<LPL, V>::NR * row_pitch<LPL>(); i += 32) (&sm.rows[0][0])[i] = 0.f;
   __syncwarp();
 }
 
 // Warp-private shared memory lives in the dynamic allocation (the larger
-// variants exceed the 48 KB static limit).
-extern __shared__ __align__(16) unsigned char gm_dyn_smem[];
-
+// variants exceed the 48 KB static limit), after the block's PSF taps.
 template <int LPL, int V>
 __device__ __forceinline__ WarpSmem<LPL, V>& warp_smem() {
-  return reinterpret_cast<WarpSmem<LPL, V>*>(gm_dyn_smem)[threadIdx.x >> 5];
+  return reinterpret_cast<WarpSmem<LPL, V>*>(gm_dyn_smem + tap_bytes<LPL>())[threadIdx.x >> 5];
 }
 
 template <int LPL, int V>
@@ -63,8 +63,9 @@ __global__ void __launch_bounds__(warps_per_block<LPL>() * 32, min_blocks<LPL, V
 invert_kernel(const DevCfg c, const InvertArgs a) {
   constexpr int NT = Variant<V>::NT;
   const int lane = threadIdx.x & 31;
+  load_taps<LPL>(c);
   WarpSmem<LPL, V>& sm = warp_smem<LPL, V>();
-  zero_padding<LPL, V>(sm, lane);
+  zero_rows<LPL, V>(sm, lane);
 
   const int nl = c.nl;
   float dlv[LPL];
@@ -223,8 +224,9 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
   constexpr int NT = Variant<V>::NT;
   const int WPB = warps_per_block<LPL>();
   const int lane = threadIdx.x & 31;
+  load_taps<LPL>(c);
   WarpSmem<LPL, V>& sm = warp_smem<LPL, V>();
-  zero_padding<LPL, V>(sm, lane);
+  zero_rows<LPL, V>(sm, lane);
   const int nl = c.nl;
   float dlv[LPL];
   double dld[LPL];
@@ -401,7 +403,7 @@ cudaError_t launch_peak(int kind, int blocks, int threads, int iters, void* sink
 
 // ---------------------------------------------------------------- launchers
 template <int LPL, int V>
-size_t smem_bytes() { return sizeof(WarpSmem<LPL, V>) * warps_per_block<LPL>(); }
+size_t smem_bytes() { return tap_bytes<LPL>() + sizeof(WarpSmem<LPL, V>) * warps_per_block<LPL>(); }
 
 template <int LPL, int V>
 cudaError_t prepare_invert() {
@@ -458,7 +460,7 @@ cudaError_t launch_invert(const DevCfg& cfg, const InvertArgs& a, int grid, cuda
 
 template <int LPL, int V>
 cudaError_t launch_synth_t(const DevCfg& cfg, const SynthArgs& a, int grid, cudaStream_t s) {
-  const size_t bytes = sizeof(WarpSmem<LPL, V>) * warps_per_block<LPL>();
+  const size_t bytes = tap_bytes<LPL>() + sizeof(WarpSmem<LPL, V>) * warps_per_block<LPL>();
   cudaError_t e = cudaFuncSetAttribute(synth_kernel<LPL, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)bytes);
   if (e != cudaSuccess) return e;
