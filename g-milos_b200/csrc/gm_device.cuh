@@ -62,27 +62,6 @@ __device__ __forceinline__ double warp_sum_d(double v) {
   return v;
 }
 
-// Reduce-scatter of N = 32*r per-lane partial sums by recursive halving:
-// every step each lane keeps half of its vector and adds the partner's copy
-// of that half.  After five steps lane L holds the warp-wide sums of entries
-// [r*L, r*L + r).  Cost: N - r shuffles instead of 5 N for N butterflies.
-template <int N>
-__device__ __forceinline__ void warp_reduce_scatter(float (&v)[N], int lane) {
-#pragma unroll
-  for (int s = 0; s < 5; ++s) {
-    const int w = N >> s;        // live entries per lane
-    const int h = w >> 1;
-    const int bit = 16 >> s;
-    const bool up = (lane & bit) != 0;
-#pragma unroll
-    for (int i = 0; i < h; ++i) {
-      const float send = up ? v[i] : v[i + h];
-      const float keep = up ? v[i + h] : v[i];
-      v[i] = keep + __shfl_xor_sync(kFull, send, bit);
-    }
-  }
-}
-
 // sin and cos as the reference takes them (__sincosf, absolute error of a few
 // 1e-7) or correctly rounded (accurate numerics)
 __device__ __forceinline__ void sincos_mode(float x, float* s, float* c, bool accurate) {
@@ -183,6 +162,11 @@ template <int LPL>
 __host__ __device__ constexpr size_t tap_bytes() { return sizeof(double) * tap_span<LPL>(); }
 __device__ __forceinline__ double* block_taps() { return reinterpret_cast<double*>(gm_dyn_smem); }
 
+// Extra rows of the normal equations' operand: per Stokes the column of
+// alpha's slot (asrc - slight) and the residual syn - obs, then a row of ones
+// (S0's RF of Stokes I) and a row of zeros, all zero past nl.
+constexpr int kXAlpha = 0, kXRes = 4, kXOne = 8, kXZero = 9, kXRows = 10;
+
 // Warp-private shared memory.
 template <int LPL, int V>
 struct WarpSmem {
@@ -196,7 +180,7 @@ struct WarpSmem {
   float beta[12];
   float vec[NS][2][12];  // rotated beta per damping, double-buffered; a step lands in vec[d][0]
   float cs[NS][18][5], sn[NS][18][5];
-  float red[96];
+  float xrows[kXRows][row_pitch<LPL>()];   // normal-equation operand rows (kX*)
   float ic[NR];          // continuum about which each staged I row is reflected
   double gk[Variant<V>::MAC ? kMaxNl : 1];   // macroturbulence kernel (PSF folded in)
   double gd[Variant<V>::MAC ? kMaxNl : 1];   // its derivative with respect to v_mac
@@ -835,53 +819,103 @@ __device__ __forceinline__ float gather_rf(const DevCfg& c, const WarpSmem<LPL, 
 template <int NT>
 __host__ __device__ constexpr int upk(int i, int h) { return i * NT - (i * (i - 1)) / 2 + (h - i); }
 
+// Row of the operand J' of the normal equations for term t and Stokes s:
+// the response function of parameter t < NT as gather_rf defines it (a
+// staged RF row, alpha's column, S0's constant RF, or zeros for fixed
+// parameters, FijaACeroDerivadasNoNecesarias, milosUtils.cu:243-271), the
+// residual syn - obs for t = NT, zeros beyond; `scale` is the stray-light
+// factor alpha that gather_rf applies (me_der.cu:191-211), here in double.
+template <int LPL, int V>
+__device__ __forceinline__ const float* jrow(const DevCfg& c, const WarpSmem<LPL, V>& sm, int t, int s,
+                                             bool mac_on, double alfa, double& scale) {
+  constexpr int NT = Variant<V>::NT;
+  scale = 1.0;
+  if (t == NT) return sm.xrows[kXRes + s];
+  if (t > NT) return sm.xrows[kXZero];
+  const int key = (NT == 10 && t == 9) ? 10 : t;
+  if (!c.fix[key]) return sm.xrows[kXZero];
+  if (t == NT - 1) {   // alpha's slot (me_der.cu:140-143 without stray light)
+    if (c.use_slight) return sm.xrows[kXAlpha + s];
+    if constexpr (Variant<V>::MAC && NT == 10) {
+      if (mac_on) return sm.rows[mac_row(s)];
+    }
+    return sm.xrows[kXZero];
+  }
+  if (c.use_slight) scale = alfa;
+  if (t == 9) {        // v_mac of the 11-term layout
+    if constexpr (Variant<V>::MAC) {
+      if (mac_on) return sm.rows[mac_row(s)];
+    }
+    return sm.xrows[kXZero];
+  }
+  if (t == 7) return sm.xrows[s == 0 ? kXOne : kXZero];
+  if (t == 6 && (s == 0 || s == 3)) return sm.xrows[kXZero];
+  return sm.rows[rf_row(s, t)];
+}
+
 // Normal equations alpha = sum_s w_s/sigma^2 J^T J and beta = sum_s w_s J^T
 // (syn - obs) / sigma^2 (covarmf, lib.cu:65-118; covarm, lib.cu:12-63 for
-// 11 terms) from the staged response functions, reduced across the warp;
-// results land in sm.alpha (packed) and sm.beta.  alpha's RF is taken from
-// the mixed profile `syn` when alpha_mixed (milosUtils.cu:675), else from the
-// unmixed `pure`.
+// 11 terms) as one product J' W J'^T on the FP64 tensor cores: J' holds the
+// NT response functions and, as row NT, the residual, over the 4 nl columns
+// of the Stokes profiles; W the weights w_s / sigma^2.  alpha is the leading
+// NT x NT block and beta column NT (8x8 tiles (0,0), (0,1), (1,1) of the
+// symmetric 16x16 result; for this operand layout a lane's B element of
+// J'^T is its A element of J').  The reference sums each Stokes parameter in
+// float; here the products and sums are double and alpha, beta are rounded
+// to float once.  Results land in sm.alpha (packed) and sm.beta.  alpha's RF
+// is taken from the mixed profile `syn` when alpha_mixed
+// (milosUtils.cu:675), else from the unmixed `pure`.
 template <int LPL, int V>
 __device__ __forceinline__ void normal_eq(const DevCfg& c, const double* m, bool alpha_mixed,
                                           const float (&pure)[LPL][4], const float (&sl)[LPL][4],
                                           const float (&syn)[LPL][4], const float (&ob)[LPL][4],
                                           const bool (&valid)[LPL], int lane, WarpSmem<LPL, V>& sm) {
   constexpr int NT = Variant<V>::NT;
-  constexpr int NP = NT * (NT + 1) / 2;
-  static_assert(NP + NT <= 96, "normal equations exceed the reduction width");
-  float v[96];
-#pragma unroll
-  for (int i = 0; i < 96; ++i) v[i] = 0.f;
+  constexpr int S = 32 * LPL;
+  static_assert(NT < 16, "the residual row must fit the 16-row operand");
   const double alfa = m[ALFA];
   bool mac_on = false;
   if constexpr (Variant<V>::MAC) mac_on = m[MAC] > 0.0001;
+  // stage alpha's column and the residual of this lane's samples
 #pragma unroll
   for (int k = 0; k < LPL; ++k) {
-    if (!valid[k]) continue;
     const int l = lane + 32 * k;
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
-      float J[NT];
       const float asrc = alpha_mixed ? syn[k][s] : pure[k][s];
-#pragma unroll
-      for (int t = 0; t < NT; ++t) J[t] = gather_rf<LPL, V>(c, sm, alfa, asrc, sl[k][s], l, s, t, mac_on);
-      const float wd = c.wsig[s];
-      const float r = c.weight[s] * (syn[k][s] - ob[k][s]);
-#pragma unroll
-      for (int i = 0; i < NT; ++i) {
-        const float ji = J[i];
-#pragma unroll
-        for (int h = i; h < NT; ++h) v[upk<NT>(i, h)] = fmaf(wd * ji, J[h], v[upk<NT>(i, h)]);
-        v[NP + i] = fmaf(r, ji, v[NP + i]);
-      }
+      sm.xrows[kXAlpha + s][l] = valid[k] ? asrc - sl[k][s] : 0.f;
+      sm.xrows[kXRes + s][l] = valid[k] ? syn[k][s] - ob[k][s] : 0.f;
     }
   }
-  warp_reduce_scatter<96>(v, lane);
-#pragma unroll
-  for (int i = 0; i < 3; ++i) sm.red[3 * lane + i] = v[i];
   __syncwarp();
-  for (int i = lane; i < NP; i += 32) sm.alpha[i] = sm.red[i];
-  if (lane < NT) sm.beta[lane] = __fdividef(sm.red[NP + lane], c.noise);
+  const int gr = lane >> 2, gc = lane & 3;
+  double d00[2] = {0.0, 0.0}, d01[2] = {0.0, 0.0}, d11[2] = {0.0, 0.0};
+#pragma unroll 1
+  for (int s = 0; s < 4; ++s) {
+    double sc0, sc1;
+    const float* r0 = jrow<LPL, V>(c, sm, gr, s, mac_on, alfa, sc0);
+    const float* r1 = jrow<LPL, V>(c, sm, 8 + gr, s, mac_on, alfa, sc1);
+    const double wd = (double)c.wsig[s];
+#pragma unroll 4
+    for (int k0 = 0; k0 < S; k0 += 4) {
+      const double x0 = (double)r0[k0 + gc] * sc0, x1 = (double)r1[k0 + gc] * sc1;
+      dmma_884(d00[0], d00[1], wd * x0, x0);
+      dmma_884(d01[0], d01[1], wd * x0, x1);
+      dmma_884(d11[0], d11[1], wd * x1, x1);
+    }
+  }
+  // lane holds element (gr, 2 gc + i) of each tile
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const int q = 2 * gc + i;
+    const int row[3] = {gr, gr, 8 + gr}, col[3] = {q, 8 + q, 8 + q};
+    const double val[3] = {d00[i], d01[i], d11[i]};
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      if (row[e] <= col[e] && col[e] < NT) sm.alpha[upk<NT>(row[e], col[e])] = (float)val[e];
+      else if (col[e] == NT && row[e] < NT) sm.beta[row[e]] = (float)val[e];
+    }
+  }
   __syncwarp();
 }
 

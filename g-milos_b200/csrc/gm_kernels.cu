@@ -36,10 +36,14 @@ __device__ __forceinline__ const double* pixel_grid(const DevCfg& c, unsigned lo
 }
 
 // Staged rows start at zero (rows that no phase stages then hold zeros in
-// the tensor-core tiles of the PSF).
+// the tensor-core tiles); the normal equations' row of ones is 1 up to nl.
 template <int LPL, int V>
-__device__ __forceinline__ void zero_rows(WarpSmem<LPL, V>& sm, int lane) {
+__device__ __forceinline__ void init_rows(const DevCfg& c, WarpSmem<LPL, V>& sm, int lane) {
   for (int i = lane; i < WarpSmem<LPL, V>::NR * row_pitch<LPL>(); i += 32) (&sm.rows[0][0])[i] = 0.f;
+  for (int i = lane; i < kXRows * row_pitch<LPL>(); i += 32) {
+    const int r = i / row_pitch<LPL>(), l = i - r * row_pitch<LPL>();
+    (&sm.xrows[0][0])[i] = (r == kXOne && l < c.nl) ? 1.f : 0.f;
+  }
   __syncwarp();
 }
 
@@ -65,7 +69,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
   const int lane = threadIdx.x & 31;
   load_taps<LPL>(c);
   WarpSmem<LPL, V>& sm = warp_smem<LPL, V>();
-  zero_rows<LPL, V>(sm, lane);
+  init_rows<LPL, V>(c, sm, lane);
 
   const int nl = c.nl;
   float dlv[LPL];
@@ -226,7 +230,7 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
   const int lane = threadIdx.x & 31;
   load_taps<LPL>(c);
   WarpSmem<LPL, V>& sm = warp_smem<LPL, V>();
-  zero_rows<LPL, V>(sm, lane);
+  init_rows<LPL, V>(c, sm, lane);
   const int nl = c.nl;
   float dlv[LPL];
   double dld[LPL];
