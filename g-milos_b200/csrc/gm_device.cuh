@@ -439,32 +439,34 @@ __device__ __forceinline__ void synth_lane(const DevCfg& c, const double* m, con
   const float doppf = (float)m[DOPP];
   const double aa = m[AA];
 
+  // every Zeeman component in one rolled loop (one copy of the Voigt code):
+  // group g of component ci, its index kk within the group
+  const int ncomp = c.n_pi + 2 * c.n_sig;
+#pragma unroll 1
+  for (int ci = 0; ci < ncomp; ++ci) {
+    const int g = ci < c.n_pi ? 0 : (ci < c.n_pi + c.n_sig ? 1 : 2);
+    const int kk = g == 0 ? ci : (g == 1 ? ci - c.n_pi : ci - c.n_pi - c.n_sig);
+    float nu, wex;
+    if (g == 0) { nu = parcial * c.nup[kk]; wex = c.wep[kk]; }
+    else if (g == 1) { nu = parcial * c.nub[kk]; wex = c.web[kk]; }
+    else { nu = -(parcial * c.nub[c.n_sig - 1 - kk]); wex = c.wer[kk]; }
+    const float rnu = (float)((double)nu * m[BFLD]);
 #pragma unroll
-  for (int g = 0; g < 3; ++g) {
-    const int n = (g == 0) ? c.n_pi : c.n_sig;
-    for (int kk = 0; kk < n; ++kk) {
-      float nu, wex;
-      if (g == 0) { nu = parcial * c.nup[kk]; wex = c.wep[kk]; }
-      else if (g == 1) { nu = parcial * c.nub[kk]; wex = c.web[kk]; }
-      else { nu = -(parcial * c.nub[c.n_sig - 1 - kk]); wex = c.wer[kk]; }
-      const float rnu = (float)((double)nu * m[BFLD]);
+    for (int k = 0; k < LPL; ++k) {
+      float v = __fdividef(dlv[k], doppf);
+      v = v - ulos;
+      v = v - rnu;
+      float h, f;
+      voigt(aa, v, h, f);
+      const float fh = wex * h, fs = wex * f * 2.f;
 #pragma unroll
-      for (int k = 0; k < LPL; ++k) {
-        float v = __fdividef(dlv[k], doppf);
-        v = v - ulos;
-        v = v - rnu;
-        float h, f;
-        voigt(aa, v, h, f);
-        if (kk == 0) {
-          st.fi[k][g] = wex * h;
-          st.shi[k][g] = wex * f * 2.f;
-        } else {
-          st.fi[k][g] = st.fi[k][g] + wex * h;
-          st.shi[k][g] = st.shi[k][g] + wex * f * 2.f;
-        }
-        st.lh[k][g] = h;
-        st.lf[k][g] = f;
-        st.lu[k][g] = v;
+      for (int gg = 0; gg < 3; ++gg) {
+        if (gg != g) continue;
+        st.fi[k][gg] = kk == 0 ? fh : st.fi[k][gg] + fh;
+        st.shi[k][gg] = kk == 0 ? fs : st.shi[k][gg] + fs;
+        st.lh[k][gg] = h;
+        st.lf[k][gg] = f;
+        st.lu[k][gg] = v;
       }
     }
   }
