@@ -236,6 +236,61 @@ def test_device_and_host_buffers_agree(engine):
     np.testing.assert_array_equal(m, a["model"])
 
 
+@pytest.mark.parametrize("nl,psf", [(31, True), (45, True), (60, True)])
+def test_inversion_across_grid_sizes(engine, nl, psf):
+    """Centred grids of 12 to 60 samples at 35 mA: one sample per lane up to
+    32 samples, two above (the kernel's second lane layout), against the
+    faithful oracle with the full-inversion tolerances."""
+    rng = np.random.default_rng(500 + nl)
+    ocfg, gcfg, _ = configs(nl=nl, psf=psf, numerics=1)
+    t = H.truth_models(512, rng)
+    obs = H.observations(ocfg, t, rng)
+    engine.configure(gcfg)
+    out = engine.invert(obs)
+    mr, cr, ir, ar, fr = O.lm_batch_f(ocfg, obs, nthreads=0)
+    ok = close_enough(out["model64"], out["chi2"], mr, cr)
+    no_worse = out["chi2"] <= cr * (1 + 1e-3) + 1e-6
+    print("nl %d: agree %.4f  chi2-no-worse %.4f" % (nl, ok.mean(), no_worse.mean()))
+    assert ok.mean() >= 0.95
+    assert (ok | no_worse).mean() >= 0.99
+
+
+def test_twelve_sample_grid(engine):
+    """The shortest grid of the benchmark set (12 samples, +-210 mA) cuts the
+    wings of strongly split, shifted lines, and the fit is ill-conditioned:
+    single LM steps match the faithful oracle as on 30 samples (required:
+    99th percentile of the relative step difference < 1e-4), but ~8 % of
+    trajectories part after a rounding-level difference (every kernel
+    generation here shows the same share).  Where they part, neither side may
+    end with the better chi2 systematically: on 2048 pixels the share where
+    the engine is worse may exceed the oracle's by at most 2 % (about 2.5
+    standard deviations), and the median chi2 agrees within 1 %."""
+    rng = np.random.default_rng(512)
+    ocfg, gcfg, _ = configs(nl=12, numerics=1)
+    t = H.truth_models(2048, rng)
+    obs = H.observations(ocfg, t, rng)
+    engine.configure(gcfg)
+    start = t[:256].copy()
+    start[:, 1] = np.clip(start[:, 1] * rng.uniform(0.8, 1.2, 256) + 50, 0, None)
+    start[:, 2] += rng.uniform(-0.3, 0.3, 256)
+    d, _, _, _ = engine.lm_step(obs[:256], start, 0.1)
+    rel = np.array([np.linalg.norm(d[p, :9] - O.lm_step_f(ocfg, start[p], obs[p], 0.1)[0][:9])
+                    / max(np.linalg.norm(O.lm_step_f(ocfg, start[p], obs[p], 0.1)[0][:9]), 1e-30)
+                    for p in range(256)])
+    assert np.percentile(rel, 99) < 1e-4, np.percentile(rel, [50, 99])
+    out = engine.invert(obs)
+    mr, cr, ir, ar, fr = O.lm_batch_f(ocfg, obs, nthreads=0)
+    mg, cg = out["model64"], out["chi2"]
+    agree = close_enough(mg, cg, mr, cr)
+    worse_g = ~agree & (cg > cr * (1 + 1e-3) + 1e-6)
+    worse_r = ~agree & (cr > cg * (1 + 1e-3) + 1e-6)
+    print("nl 12: agree %.4f  engine worse %.4f  oracle worse %.4f  median chi2 %.4f / %.4f"
+          % (agree.mean(), worse_g.mean(), worse_r.mean(), np.median(cg), np.median(cr)))
+    assert agree.mean() >= 0.88
+    assert worse_g.mean() <= worse_r.mean() + 0.02
+    assert np.median(cg) == pytest.approx(np.median(cr), rel=0.01)
+
+
 @pytest.mark.parametrize("fix", [(1, 1, 1, 1, 1, 1, 1, 0, 0, 0, 0),      # 7 free, S0 S1 fixed
                                  (1, 1, 1, 0, 0, 1, 1, 1, 1, 0, 0)])     # Doppler width, damping fixed
 def test_fixed_parameter_sets(engine, fix):
