@@ -312,6 +312,12 @@ def run_engine(args):
     launch_avg = float(np.mean(launch_ms))
     achieved = flops_launch / (launch_avg / 1e3) / 1e12
     fp32_peak, fp64_peak = eng.measure_peaks()
+    # special-function side: MUFU operations per sample (10 per trial, 5 per
+    # accepted step) plus the 2 sincos of the field angles per trial; the
+    # initial point counts as one trial and one accepted step
+    sfu_launch = (iters_sum + P) * (10 * nl + 4) + (acc_sum + P) * 5 * nl
+    sfu_achieved = sfu_launch / (launch_avg / 1e3) / 1e9
+    sfu_peak = eng.measure_sfu_peak()
     clocks = summarize_clocks(clk)
 
     result = {
@@ -333,7 +339,10 @@ def run_engine(args):
                      "traffic_note": "bytes per launch, scaled from an ncu capture of a 65536-pixel launch",
                      "peak_source": "measured FFMA microbenchmark (gm_measure_peaks), burst",
                      "fp64_peak": fp64_peak,
-                     "flops_per_launch": flops_launch, "launch_ms": launch_avg},
+                     "flops_per_launch": flops_launch, "launch_ms": launch_avg,
+                     "sfu": {"ops_per_launch": sfu_launch, "achieved": sfu_achieved, "peak": sfu_peak,
+                             "unit": "G MUFU ops/s", "frac": sfu_achieved / sfu_peak if sfu_peak else None,
+                             "peak_source": "measured ex2.approx chains (gm_measure_sfu_peak), burst"}},
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

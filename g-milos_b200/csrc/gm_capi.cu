@@ -650,6 +650,31 @@ gm_status gm_measure_peaks(gm_ctx* ctx, double* fp32_tflops, double* fp64_tflops
   return GM_OK;
 }
 
+gm_status gm_measure_sfu_peak(gm_ctx* ctx, double* gops) {
+  if (!ctx || !gops) return GM_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(ctx->call_mu);
+  cudaSetDevice(ctx->device);
+  void* sink = nullptr;
+  gm_status st = ensure_buf(ctx, "peaksink", sizeof(double) * 1024 * 1024, &sink);
+  if (st != GM_OK) return st;
+  const int blocks = ctx->sms * 8, threads = 256, iters = 1024;
+  double best = 0;
+  for (int rep = 0; rep < 4; ++rep) {
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    cudaError_t e = gm::launch_peak(2, blocks, threads, iters, sink, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "SFU peak kernel");
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    e = cudaEventSynchronize(ctx->ev1);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "SFU peak kernel");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    const double ops = (double)gm::kPeakChains * iters * blocks * threads;
+    best = std::max(best, ops / (ms * 1e-3) / 1e9);
+  }
+  *gops = best;
+  return GM_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------- serving

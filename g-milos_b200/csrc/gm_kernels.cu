@@ -399,9 +399,29 @@ __global__ void peak_kernel(int iters, T* sink) {
   if (s == (T)-1) sink[(blockIdx.x * blockDim.x + threadIdx.x) & 1023] = s;
 }
 
+// Special-function-unit issue bound: kPeakChains independent chains of the
+// base-2 exponential (one MUFU operation each, the PTX ex2.approx), each
+// mapping (0, 1] into [0.5, 1).
+__global__ void mufu_peak_kernel(int iters, float* sink) {
+  float a[kPeakChains];
+#pragma unroll
+  for (int c = 0; c < kPeakChains; ++c) a[c] = 0.5f + 1e-3f * (float)((threadIdx.x + c) & 255);
+  for (int i = 0; i < iters; ++i)
+#pragma unroll
+    for (int c = 0; c < kPeakChains; ++c) {
+      const float x = -a[c];
+      asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(a[c]) : "f"(x));
+    }
+  float s = 0.f;
+#pragma unroll
+  for (int c = 0; c < kPeakChains; ++c) s += a[c];
+  if (s == -1.f) sink[(blockIdx.x * blockDim.x + threadIdx.x) & 1023] = s;
+}
+
 cudaError_t launch_peak(int kind, int blocks, int threads, int iters, void* sink, cudaStream_t s) {
   if (kind == 0) peak_kernel<float><<<blocks, threads, 0, s>>>(iters, (float*)sink);
-  else peak_kernel<double><<<blocks, threads, 0, s>>>(iters, (double*)sink);
+  else if (kind == 1) peak_kernel<double><<<blocks, threads, 0, s>>>(iters, (double*)sink);
+  else mufu_peak_kernel<<<blocks, threads, 0, s>>>(iters, (float*)sink);
   return cudaGetLastError();
 }
 

@@ -64,8 +64,9 @@ struct InvertGeometry {
 };
 InvertGeometry invert_geometry(const DevCfg& cfg, bool per_pixel_init);
 
-// FMA-issue-bound microbenchmark (kind 0: FP32, 1: FP64); each thread runs
-// kPeakChains independent FMA chains of `iters` steps.
+// Issue-bound microbenchmarks (kind 0: FP32 FMA, 1: FP64 FMA, 2: MUFU
+// exponential); each thread runs kPeakChains independent chains of `iters`
+// steps.
 constexpr int kPeakChains = 8;
 cudaError_t launch_peak(int kind, int blocks, int threads, int iters, void* sink, cudaStream_t s);
 

@@ -36,7 +36,7 @@ NUMERICS_REFERENCE, NUMERICS_ACCURATE = 0, 1
 EXPORTS = ("gm_create", "gm_destroy", "gm_last_error", "gm_status_string", "gm_config_defaults",
            "gm_configure", "gm_invert", "gm_invert_ex", "gm_synthesize", "gm_synthesize_f64",
            "gm_synthesize_grid", "gm_lm_step", "gm_submit", "gm_poll", "gm_cancel", "gm_zeeman_from_levels",
-           "gm_psf_gaussian", "gm_psf_from_table", "gm_get_stats", "gm_measure_peaks",
+           "gm_psf_gaussian", "gm_psf_from_table", "gm_get_stats", "gm_measure_peaks", "gm_measure_sfu_peak",
            "gm_invert_noalloc", "gm_classical", "gm_serving_options")
 
 
@@ -115,6 +115,7 @@ def lib():
         L.gm_psf_from_table.argtypes = [vp, vp, C.c_int, vp, C.c_int, C.c_double, vp]
         L.gm_get_stats.argtypes = [vp, C.POINTER(Stats)]
         L.gm_measure_peaks.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.gm_measure_sfu_peak.argtypes = [vp, C.POINTER(C.c_double)]
         L.gm_invert_noalloc.argtypes = [C.POINTER(Config), vp, i64, C.c_int, vp, vp, vp, vp, vp, vp]
         _lib = L
     return _lib
@@ -430,6 +431,12 @@ class Engine:
         a, b = C.c_double(), C.c_double()
         _check(lib().gm_measure_peaks(self._ctx, C.byref(a), C.byref(b)), self._ctx)
         return a.value, b.value
+
+    def measure_sfu_peak(self):
+        """Special-function-unit (MUFU) throughput of this device, G ops/s."""
+        a = C.c_double()
+        _check(lib().gm_measure_sfu_peak(self._ctx, C.byref(a)), self._ctx)
+        return a.value
 
     def stats(self):
         s = Stats()

@@ -267,6 +267,10 @@ gm_status gm_get_stats(gm_ctx *ctx, gm_stats *out);
  * the engine's roofline fraction.  Measurement helper, no reference
  * counterpart. */
 gm_status gm_measure_peaks(gm_ctx *ctx, double *fp32_tflops, double *fp64_tflops);
+/* Special-function-unit throughput (MUFU operations, G ops/s) from chains of
+ * the PTX base-2 exponential; the SFU side of the roofline.  No counterpart
+ * in the reference. */
+gm_status gm_measure_sfu_peak(gm_ctx *ctx, double *gops);
 
 #ifdef __cplusplus
 }
