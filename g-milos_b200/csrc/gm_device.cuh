@@ -6,8 +6,10 @@
 // follows the reference's precision choices: FP32 with the same fast
 // intrinsics (__fdividef, __sincosf), FP64 for the Voigt polynomials and
 // wherever the reference keeps PRECISION=double (model parameters,
-// classical estimates).  file:line citations name the reference code each
-// piece reproduces.
+// classical estimates, the PSF convolution).  The two matrix products of a
+// step -- the PSF convolution of the staged rows and the normal equations --
+// run on the FP64 tensor cores (mma.sync m8n8k4).  file:line citations name
+// the reference code each piece reproduces.
 #pragma once
 
 #include <cstdint>
