@@ -73,6 +73,10 @@ struct gm_ctx {
   gm_config cfg{};
   gm::DevCfg dev{};
   gm::WorkCounters* work = nullptr;   // device scratch of the persistent launch
+  // pipelined host-memory inversions: a second stream and its work counters
+  cudaStream_t aux = nullptr;
+  cudaEvent_t evx0 = nullptr, evx1 = nullptr;
+  gm::WorkCounters* work2 = nullptr;
   DevBuf slight;                      // global stray-light profile (device copy)
   std::map<std::string, DevBuf> bufs; // staging buffers for host-memory calls
   std::string err;
@@ -305,6 +309,10 @@ gm_status gm_create(int device, size_t hbm_budget, gm_ctx** out) {
   cudaEventCreate(&ctx->ev0);
   cudaEventCreate(&ctx->ev1);
   if (cudaMalloc(&ctx->work, sizeof(gm::WorkCounters)) != cudaSuccess) return GM_ERR_NOMEM;
+  if (cudaMalloc(&ctx->work2, sizeof(gm::WorkCounters)) != cudaSuccess) return GM_ERR_NOMEM;
+  if (cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking) != cudaSuccess) return GM_ERR_CUDA;
+  cudaEventCreateWithFlags(&ctx->evx0, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&ctx->evx1, cudaEventDisableTiming);
   *out = ctx.release();
   return GM_OK;
 }
@@ -322,9 +330,14 @@ gm_status gm_destroy(gm_ctx* ctx) {
   for (auto& kv : ctx->bufs)
     if (kv.second.p) cudaFree(kv.second.p);
   if (ctx->slight.p) cudaFree(ctx->slight.p);
+  if (ctx->aux) cudaStreamSynchronize(ctx->aux);
   if (ctx->work) cudaFree(ctx->work);
+  if (ctx->work2) cudaFree(ctx->work2);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
+  if (ctx->evx0) cudaEventDestroy(ctx->evx0);
+  if (ctx->evx1) cudaEventDestroy(ctx->evx1);
+  if (ctx->aux) cudaStreamDestroy(ctx->aux);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return GM_OK;
@@ -365,6 +378,84 @@ struct StepOut {
   float* chi2_trial = nullptr;
 };
 
+// Pixels per chunk of a pipelined host-memory inversion (at least two chunks).
+constexpr int64_t kPipeChunk = 131072;
+
+// The chunked inversion of a host-memory cube: chunk k is copied up,
+// inverted and its outputs copied back on stream k % 2 (the caller's stream
+// or ctx->aux), with per-stream work counters whose cursor is reset per
+// chunk; iteration sums accumulate over the chunks.  The auxiliary stream
+// starts after the caller's prior work and the caller's stream waits for it
+// at the end, so the call stays ordered on the caller's stream.  outs[0..n)
+// are the per-pixel outputs (per-pixel size = bytes / npix).
+static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::InvertArgs& ia,
+                               const float* iquv, const Arg& a_in, const Arg* const* outs, int nouts,
+                               int64_t npix, int nl, cudaStream_t s) {
+  const size_t row = 4 * (size_t)nl;
+  cudaError_t e = cudaMemsetAsync(ctx->work, 0, sizeof(gm::WorkCounters), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->work2, 0, sizeof(gm::WorkCounters), s);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->evx0, s);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->aux, ctx->evx0, 0);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "pipeline set-up");
+  const int nch = (int)std::min<int64_t>(8, npix / kPipeChunk);
+  cudaEventRecord(ctx->ev0, s);
+  for (int k = 0; k < nch && e == cudaSuccess; ++k) {
+    const int64_t a = npix * k / nch, b = npix * (k + 1) / nch, n = b - a;
+    cudaStream_t q = (k & 1) ? ctx->aux : s;
+    gm::WorkCounters* w = (k & 1) ? ctx->work2 : ctx->work;
+    e = cudaMemcpyAsync((float*)a_in.dev + a * row, iquv + a * row, sizeof(float) * row * n,
+                        cudaMemcpyHostToDevice, q);
+    if (e == cudaSuccess) e = cudaMemsetAsync(&w->next_pixel, 0, sizeof(w->next_pixel), q);
+    if (e != cudaSuccess) break;
+    gm::DevCfg dc = d;
+    if (d.use_slight && d.slight_per_pixel) dc.slight = d.slight + a * row;
+    if (d.lambda_per_pixel) dc.lam_map = d.lam_map + a * nl;
+    gm::InvertArgs c = ia;
+    c.iquv = ia.iquv + a * row;
+    c.npix = n;
+    if (ia.init_models) c.init_models = ia.init_models + a * 11;
+    if (ia.model) c.model = ia.model + a * 11;
+    if (ia.model_f64) c.model_f64 = ia.model_f64 + a * 11;
+    if (ia.chi2) c.chi2 = ia.chi2 + a;
+    if (ia.iters) c.iters = ia.iters + a;
+    if (ia.accepted) c.accepted = ia.accepted + a;
+    if (ia.fitted) c.fitted = ia.fitted + a * row;
+    if (ia.status) c.status = ia.status + a;
+    c.work = w;
+    gm::InvertGeometry geo;
+    const int64_t grid = invert_grid(dc, c.init_models != nullptr, ctx->sms, n, &geo);
+    e = gm::launch_invert(dc, c, (int)grid, q);
+    ctx->stats.grid_blocks = (int)grid;
+    ctx->stats.block_threads = geo.threads;
+    ctx->stats.warps_per_block = geo.threads / 32;
+    for (int o = 0; o < nouts && e == cudaSuccess; ++o) {
+      const Arg& x = *outs[o];
+      if (!x.host || !x.dev) continue;
+      const size_t unit = x.bytes / (size_t)npix;
+      e = cudaMemcpyAsync((char*)x.host + a * unit, (const char*)x.dev + a * unit, unit * n,
+                          cudaMemcpyDeviceToHost, q);
+    }
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->evx1, ctx->aux);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ctx->evx1, 0);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "pipelined inversion");
+  cudaEventRecord(ctx->ev1, s);
+  ctx->stats.kernel_launches = nch;
+  ctx->stats.pixels = npix;
+  // the cube came from host memory: the call returns with its results in place
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "pipelined inversion");
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  ctx->stats.kernel_ms = ms;
+  gm::WorkCounters w0{}, w1{};
+  cudaMemcpy(&w0, ctx->work, sizeof(w0), cudaMemcpyDeviceToHost);
+  cudaMemcpy(&w1, ctx->work2, sizeof(w1), cudaMemcpyDeviceToHost);
+  ctx->stats.iterations = (int64_t)(w0.iterations + w1.iterations);
+  ctx->stats.accepted = (int64_t)(w0.accepted + w1.accepted);
+  return GM_OK;
+}
+
 static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* iquv, int64_t npix,
                              int nl, const double* init_models, const float* slight_map,
                              const double* lambda_map, float* model, double* model_f64, float* chi2, int* iters,
@@ -382,7 +473,17 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   if (need > ctx->budget) return fail(ctx, GM_ERR_NOMEM, "request exceeds the context's HBM budget");
   Arg a_in, a_init, a_sl, a_lam, a_model, a_m64, a_chi, a_it, a_acc, a_fit, a_st;
   gm_status st;
-  if ((st = stage_in(ctx, "iquv", iquv, cube, &a_in, s)) != GM_OK) return st;
+  // A large cube in host memory goes up in chunks on two alternating
+  // streams, each chunk inverted by its own launch as soon as it has
+  // arrived: the copies overlap the inversion, and a chunk's launch fills
+  // the SMs that the previous one's last pixels leave free.
+  const bool pipeline = !so && npix >= 2 * kPipeChunk && !is_device_ptr(iquv);
+  if (pipeline) {
+    if ((st = ensure_buf(ctx, "iquv", cube, &a_in.dev)) != GM_OK) return st;
+    a_in.bytes = cube;
+  } else if ((st = stage_in(ctx, "iquv", iquv, cube, &a_in, s)) != GM_OK) {
+    return st;
+  }
   if ((st = stage_in(ctx, "init", init_models, sizeof(double) * 11 * npix, &a_init, s)) != GM_OK) return st;
   gm::DevCfg d = dcfg;
   if (d.use_slight && d.slight_per_pixel) {
@@ -427,6 +528,9 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   ia.step_chi2_start = (float*)a_sc0.dev;
   ia.step_chi2_trial = (float*)a_sc1.dev;
   ia.work = ctx->work;
+  const Arg* outs[] = {&a_model, &a_m64, &a_chi, &a_it, &a_acc, &a_fit, &a_st,
+                       &a_sd, &a_strial, &a_sc0, &a_sc1};
+  if (pipeline) return invert_chunks(ctx, d, ia, iquv, a_in, outs, 7, npix, nl, s);
   cudaError_t e = cudaMemsetAsync(ctx->work, 0, sizeof(gm::WorkCounters), s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "work counter reset");
   gm::InvertGeometry geo;
@@ -440,8 +544,6 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   ctx->stats.warps_per_block = geo.threads / 32;
   ctx->stats.kernel_launches = 1;
   ctx->stats.pixels = npix;
-  const Arg* outs[] = {&a_model, &a_m64, &a_chi, &a_it, &a_acc, &a_fit, &a_st,
-                       &a_sd, &a_strial, &a_sc0, &a_sc1};
   bool any_host = false;
   for (const Arg* o : outs) {
     if ((st = copy_back(ctx, *o, s)) != GM_OK) return st;
