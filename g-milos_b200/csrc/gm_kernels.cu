@@ -55,7 +55,7 @@ __device__ __forceinline__ WarpSmem<LPL, V>& warp_smem() {
 }
 
 template <int LPL, int V>
-constexpr int min_blocks() { return LPL == 1 ? (V == 2 ? 3 : 4) : 2; }
+constexpr int min_blocks() { return LPL == 1 ? (V == 2 ? 3 : 4) : 5; }
 
 // One warp per pixel, pixels taken from a global cursor until the cube is
 // done (lm_mils, milosUtils.cu:574-710, and lm_mils_11, :713-850, with their
