@@ -390,7 +390,7 @@ constexpr int64_t kPipeChunk = 131072;
 // are the per-pixel outputs (per-pixel size = bytes / npix).
 static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::InvertArgs& ia,
                                const float* iquv, const Arg& a_in, const Arg* const* outs, int nouts,
-                               int64_t npix, int nl, cudaStream_t s) {
+                               int64_t npix, int nl, bool prepass, cudaStream_t s) {
   const size_t row = 4 * (size_t)nl;
   cudaError_t e = cudaMemsetAsync(ctx->work, 0, sizeof(gm::WorkCounters), s);
   if (e == cudaSuccess) e = cudaMemsetAsync(ctx->work2, 0, sizeof(gm::WorkCounters), s);
@@ -414,6 +414,7 @@ static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::Inver
     c.iquv = ia.iquv + a * row;
     c.npix = n;
     if (ia.init_models) c.init_models = ia.init_models + a * 11;
+    if (ia.init_status) c.init_status = ia.init_status + a;
     if (ia.model) c.model = ia.model + a * 11;
     if (ia.model_f64) c.model_f64 = ia.model_f64 + a * 11;
     if (ia.chi2) c.chi2 = ia.chi2 + a;
@@ -423,7 +424,13 @@ static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::Inver
     if (ia.status) c.status = ia.status + a;
     c.work = w;
     gm::InvertGeometry geo;
-    const int64_t grid = invert_grid(dc, c.init_models != nullptr, ctx->sms, n, &geo);
+    if (prepass) {
+      e = gm::launch_classical(dc, c.iquv, n, const_cast<double*>(c.init_models),
+                               const_cast<uint32_t*>(c.init_status), true, q);
+      if (e != cudaSuccess) break;
+      dc.init_mode = 1;
+    }
+    const int64_t grid = invert_grid(dc, c.init_models != nullptr && !c.init_status, ctx->sms, n, &geo);
     e = gm::launch_invert(dc, c, (int)grid, q);
     ctx->stats.grid_blocks = (int)grid;
     ctx->stats.block_threads = geo.threads;
@@ -468,8 +475,12 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   cudaSetDevice(ctx->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   const size_t cube = sizeof(float) * 4 * (size_t)nl * npix;
+  // classical estimates of the start models in a pre-pass kernel, so that
+  // their code stays out of the inversion kernel's instruction stream
+  const bool prepass = dcfg.init_mode == 0 && !init_models;
   size_t need = cube + (fitted ? cube : 0) + (size_t)npix * (11 * 12 + 16) +
-                (dcfg.lambda_per_pixel ? sizeof(double) * (size_t)nl * npix : 0);
+                (dcfg.lambda_per_pixel ? sizeof(double) * (size_t)nl * npix : 0) +
+                (prepass ? (size_t)npix * (11 * 8 + 4) : 0);
   if (need > ctx->budget) return fail(ctx, GM_ERR_NOMEM, "request exceeds the context's HBM budget");
   Arg a_in, a_init, a_sl, a_lam, a_model, a_m64, a_chi, a_it, a_acc, a_fit, a_st;
   gm_status st;
@@ -528,13 +539,26 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   ia.step_chi2_start = (float*)a_sc0.dev;
   ia.step_chi2_trial = (float*)a_sc1.dev;
   ia.work = ctx->work;
+  if (prepass) {
+    void *mp = nullptr, *sp = nullptr;
+    if ((st = ensure_buf(ctx, "cinit", sizeof(double) * 11 * npix, &mp)) != GM_OK) return st;
+    if ((st = ensure_buf(ctx, "cstat", sizeof(uint32_t) * npix, &sp)) != GM_OK) return st;
+    ia.init_models = (const double*)mp;
+    ia.init_status = (const uint32_t*)sp;
+  }
   const Arg* outs[] = {&a_model, &a_m64, &a_chi, &a_it, &a_acc, &a_fit, &a_st,
                        &a_sd, &a_strial, &a_sc0, &a_sc1};
-  if (pipeline) return invert_chunks(ctx, d, ia, iquv, a_in, outs, 7, npix, nl, s);
+  if (pipeline) return invert_chunks(ctx, d, ia, iquv, a_in, outs, 7, npix, nl, prepass, s);
   cudaError_t e = cudaMemsetAsync(ctx->work, 0, sizeof(gm::WorkCounters), s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "work counter reset");
+  if (prepass) {
+    e = gm::launch_classical(d, ia.iquv, npix, const_cast<double*>(ia.init_models),
+                             const_cast<uint32_t*>(ia.init_status), true, s);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "classical-estimates pre-pass");
+    d.init_mode = 1;
+  }
   gm::InvertGeometry geo;
-  const int64_t grid = invert_grid(d, ia.init_models != nullptr, ctx->sms, npix, &geo);
+  const int64_t grid = invert_grid(d, ia.init_models != nullptr && !ia.init_status, ctx->sms, npix, &geo);
   cudaEventRecord(ctx->ev0, s);
   e = gm::launch_invert(d, ia, (int)grid, s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "inversion kernel launch");
@@ -706,7 +730,7 @@ gm_status gm_classical(gm_ctx* ctx, const float* iquv, int64_t npix, int nl, dou
       return st;
     d.lam_map = (const double*)a_lam.dev;
   }
-  cudaError_t e = gm::launch_classical(d, (const float*)a_in.dev, npix, (double*)a_out.dev, s);
+  cudaError_t e = gm::launch_classical(d, (const float*)a_in.dev, npix, (double*)a_out.dev, nullptr, false, s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "classical-estimates launch");
   if ((st = copy_back(ctx, a_out, s)) != GM_OK) return st;
   if (a_out.host || a_in.dev != (const void*)iquv || !stream) {

@@ -110,7 +110,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
     // initial model
     if (lane < 11) sm.m[lane] = a.init_models ? a.init_models[pix * 11 + lane] : c.init[lane];
     __syncwarp();
-    uint32_t st = 0;
+    uint32_t st = a.init_status ? a.init_status[pix] : 0u;
     if (c.init_mode == 0) st |= classical_warp<LPL>(c, ob, dld, valid, lane, sm.m);
     __syncwarp();
 
@@ -289,12 +289,16 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
 }
 
 // Classical estimates only, one warp per pixel: the configured guess model
-// with B, vlos, gamma, phi from the weak-field / centre-of-gravity estimates
-// and S0 = B_los (the reference's classical-estimates mode,
-// gmilos.cu:383-404).
-template <int LPL>
+// with B, vlos, gamma, phi from the weak-field / centre-of-gravity estimates.
+// FOR_INIT = false: the reference's classical-estimates mode, S0 = B_los
+// (gmilos.cu:383-404).  FOR_INIT = true: the start models of an inversion,
+// exactly as the inversion kernel forms them in place (milosUtils.cu:616-628),
+// with their status bits in `status` -- a pre-pass that keeps this code out
+// of the inversion kernel's instruction stream.
+template <int LPL, bool FOR_INIT>
 __global__ void __launch_bounds__(128) classical_kernel(const DevCfg c, const float* __restrict__ iquv,
-                                                        int64_t npix, double* __restrict__ models) {
+                                                        int64_t npix, double* __restrict__ models,
+                                                        uint32_t* __restrict__ status) {
   __shared__ double ms[4][11];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int nl = c.nl;
@@ -313,20 +317,27 @@ __global__ void __launch_bounds__(128) classical_kernel(const DevCfg c, const fl
     pixel_grid<LPL>(c, (unsigned long long)pix, lane, dlv, dld);
     if (lane < 11) ms[w][lane] = c.init[lane];
     __syncwarp();
-    classical_warp<LPL>(c, ob, dld, valid, lane, ms[w], false);
+    const uint32_t st = classical_warp<LPL>(c, ob, dld, valid, lane, ms[w], FOR_INIT);
     __syncwarp();
     if (lane < 11) models[pix * 11 + lane] = ms[w][lane];
+    if (FOR_INIT && lane == 0) status[pix] = st;
     __syncwarp();
   }
 }
 
 cudaError_t launch_classical(const DevCfg& cfg, const float* iquv, int64_t npix, double* models,
-                             cudaStream_t s) {
+                             uint32_t* status, bool for_init, cudaStream_t s) {
   int64_t blocks = (npix + 3) / 4;
   if (blocks > 148 * 32) blocks = 148 * 32;
   if (blocks < 1) blocks = 1;
-  if (cfg.nl <= 32) classical_kernel<1><<<(int)blocks, 128, 0, s>>>(cfg, iquv, npix, models);
-  else classical_kernel<2><<<(int)blocks, 128, 0, s>>>(cfg, iquv, npix, models);
+  const bool l1 = cfg.nl <= 32;
+  if (for_init) {
+    if (l1) classical_kernel<1, true><<<(int)blocks, 128, 0, s>>>(cfg, iquv, npix, models, status);
+    else classical_kernel<2, true><<<(int)blocks, 128, 0, s>>>(cfg, iquv, npix, models, status);
+  } else {
+    if (l1) classical_kernel<1, false><<<(int)blocks, 128, 0, s>>>(cfg, iquv, npix, models, status);
+    else classical_kernel<2, false><<<(int)blocks, 128, 0, s>>>(cfg, iquv, npix, models, status);
+  }
   return cudaGetLastError();
 }
 
@@ -471,7 +482,7 @@ cudaError_t launch_invert_t(const DevCfg& cfg, const InvertArgs& a, int grid, cu
 }
 
 cudaError_t launch_invert(const DevCfg& cfg, const InvertArgs& a, int grid, cudaStream_t s) {
-  const int v = kernel_variant(cfg, a.init_models != nullptr);
+  const int v = kernel_variant(cfg, a.init_models != nullptr && !a.init_status);
   if (cfg.nl <= 32) {
     if (v == 0) return launch_invert_t<1, 0>(cfg, a, grid, s);
     if (v == 1) return launch_invert_t<1, 1>(cfg, a, grid, s);

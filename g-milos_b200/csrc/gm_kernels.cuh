@@ -23,6 +23,9 @@ struct InvertArgs {
   const float* iquv;          // [P][4][nl]
   int64_t npix;
   const double* init_models;  // [P][11] or null
+  const uint32_t* init_status; // [P] status bits of a classical pre-pass that
+                               // made init_models (its v_mac is the configured
+                               // one), or null
   float* model;               // [P][11] or null
   double* model_f64;          // [P][11] or null
   float* chi2;                // [P] or null
@@ -48,8 +51,10 @@ struct SynthArgs {
 // launchers (gm_kernels.cu); return the CUDA error of the launch
 cudaError_t launch_invert(const DevCfg& cfg, const InvertArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_synth(const DevCfg& cfg, const SynthArgs& a, cudaStream_t s);
+// classical estimates: for_init false -> the classical-estimates mode
+// (S0 = B_los); true -> start models of an inversion plus status bits
 cudaError_t launch_classical(const DevCfg& cfg, const float* iquv, int64_t npix, double* models,
-                             cudaStream_t s);
+                             uint32_t* status, bool for_init, cudaStream_t s);
 cudaError_t launch_synth_grid(const DevCfg& cfg, const double* models, int64_t npix,
                               const double* offsets, int ngrid, float* out, cudaStream_t s);
 // kernel variant for a configuration (0: 10 terms, 1: 10 terms with

@@ -249,6 +249,34 @@ def test_pipelined_host_inversion_equals_one_launch(engine):
     assert st["iterations"] == int(host["iters"].sum())
 
 
+def test_classical_prepass_equals_in_kernel_estimates(engine):
+    """gm_invert forms the classical start models in a pre-pass kernel;
+    gm_invert_noalloc forms them inside the inversion kernel with the same
+    device code: the inversions agree bit for bit."""
+    import ctypes as C
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(720)
+    fix = (1,) * 9 + (0, 1)
+    ocfg, gcfg, sl = configs(psf=True, stray=True, fix=fix)
+    obs = H.observations(ocfg, H.truth_models(4096, rng, alpha_range=(0.7, 1.0)), rng, slight=sl)
+    engine.configure(gcfg)
+    a = engine.invert(obs)
+    d = torch.from_numpy(obs).cuda()
+    P, nl = len(obs), obs.shape[2]
+    model = torch.empty((P, 11), dtype=torch.float32, device="cuda")
+    chi2 = torch.empty(P, dtype=torch.float32, device="cuda")
+    iters = torch.empty(P, dtype=torch.int32, device="cuda")
+    status = torch.empty(P, dtype=torch.int32, device="cuda")
+    st = G.lib().gm_invert_noalloc(C.byref(gcfg), G._ptr(d), P, nl, G._ptr(model), G._ptr(chi2), G._ptr(iters),
+                                   None, G._ptr(status), C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == G.GM_OK
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(a["model"], model.cpu().numpy())
+    np.testing.assert_array_equal(a["chi2"], chi2.cpu().numpy())
+    np.testing.assert_array_equal(a["iters"], iters.cpu().numpy())
+    np.testing.assert_array_equal(a["status"].astype(np.int64), status.cpu().numpy().astype(np.int64))
+
+
 def test_device_and_host_buffers_agree(engine):
     torch = pytest.importorskip("torch")
     rng = np.random.default_rng(700)
