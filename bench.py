@@ -44,7 +44,7 @@ MAXITER = 50
 # DRAM bytes (read + write) per pixel of the inversion kernel, measured with
 # ncu (dram__bytes_read.sum + dram__bytes_write.sum) on one 65 536-pixel
 # launch of this workload; traffic grows with the pixel count.
-DRAM_BYTES_PER_PIXEL = 484.0
+DRAM_BYTES_PER_PIXEL = 585.0
 
 # Algorithmic FLOPs per pixel (per-wavelength costs counted from the formulas)
 C_VOIGT, C_RTE, C_DVOIGT, C_DRTE = 100, 85, 23, 870
