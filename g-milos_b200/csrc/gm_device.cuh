@@ -182,7 +182,6 @@ struct WarpSmem {
   float beta[12];
   float vec[NS][2][12];  // rotated beta per damping, double-buffered; a step lands in vec[d][0]
   float cs[NS][18][5], sn[NS][18][5];
-  float xrows[kXRows][row_pitch<LPL>()];   // normal-equation operand rows (kX*)
   float ic[NR];          // continuum about which each staged I row is reflected
   double gk[Variant<V>::MAC ? kMaxNl : 1];   // macroturbulence kernel (PSF folded in)
   double gd[Variant<V>::MAC ? kMaxNl : 1];   // its derivative with respect to v_mac
@@ -192,6 +191,9 @@ struct WarpSmem {
   double b11[S11 ? 12 : 1], z11[S11 ? 12 : 1];
   double c11[S11 ? 6 : 1], s11[S11 ? 6 : 1]; // the step's rotations
   float rows[NR][row_pitch<LPL>()];   // staged rows (PSF, macroturbulence, RFs)
+  // the normal equations' operand rows (kX*), right after `rows` with the
+  // same pitch: row NR + x of the combined array is xrows[x]
+  float xrows[kXRows][row_pitch<LPL>()];
 };
 
 template <int LPL>
@@ -823,38 +825,34 @@ __device__ __forceinline__ float gather_rf(const DevCfg& c, const WarpSmem<LPL, 
 template <int NT>
 __host__ __device__ constexpr int upk(int i, int h) { return i * NT - (i * (i - 1)) / 2 + (h - i); }
 
-// Row of the operand J' of the normal equations for term t and Stokes s:
+// Row of the operand J' of the normal equations for term t and Stokes s,
+// as an index into the staged rows followed by the operand rows (NR + kX*):
 // the response function of parameter t < NT as gather_rf defines it (a
 // staged RF row, alpha's column, S0's constant RF, or zeros for fixed
 // parameters, FijaACeroDerivadasNoNecesarias, milosUtils.cu:243-271), the
-// residual syn - obs for t = NT, zeros beyond; `scale` is the stray-light
-// factor alpha that gather_rf applies (me_der.cu:191-211), here in double.
+// residual syn - obs for t = NT, zeros beyond; `scaled` tells whether the
+// stray-light factor alpha applies (me_der.cu:191-211).  t differs between
+// the lanes of a warp, so this is written with selects and the free-
+// parameter bitmask `fixmask` rather than branches and indexed constants.
 template <int LPL, int V>
-__device__ __forceinline__ const float* jrow(const DevCfg& c, const WarpSmem<LPL, V>& sm, int t, int s,
-                                             bool mac_on, double alfa, double& scale) {
-  constexpr int NT = Variant<V>::NT;
-  scale = 1.0;
-  if (t == NT) return sm.xrows[kXRes + s];
-  if (t > NT) return sm.xrows[kXZero];
+__device__ __forceinline__ int jrow(const DevCfg& c, uint32_t fixmask, int t, int s, bool mac_on,
+                                   bool& scaled) {
+  constexpr int NT = Variant<V>::NT, NR = WarpSmem<LPL, V>::NR;
+  const int zero = NR + kXZero;
   const int key = (NT == 10 && t == 9) ? 10 : t;
-  if (!c.fix[key]) return sm.xrows[kXZero];
-  if (t == NT - 1) {   // alpha's slot (me_der.cu:140-143 without stray light)
-    if (c.use_slight) return sm.xrows[kXAlpha + s];
-    if constexpr (Variant<V>::MAC && NT == 10) {
-      if (mac_on) return sm.rows[mac_row(s)];
-    }
-    return sm.xrows[kXZero];
-  }
-  if (c.use_slight) scale = alfa;
-  if (t == 9) {        // v_mac of the 11-term layout
-    if constexpr (Variant<V>::MAC) {
-      if (mac_on) return sm.rows[mac_row(s)];
-    }
-    return sm.xrows[kXZero];
-  }
-  if (t == 7) return sm.xrows[s == 0 ? kXOne : kXZero];
-  if (t == 6 && (s == 0 || s == 3)) return sm.xrows[kXZero];
-  return sm.rows[rf_row(s, t)];
+  const bool free_t = t < NT && ((fixmask >> key) & 1u);
+  int mac_r = zero;
+  if constexpr (Variant<V>::MAC) mac_r = mac_on ? mac_row(s) : zero;
+  const int alpha_r = c.use_slight ? NR + kXAlpha + s : ((Variant<V>::MAC && NT == 10) ? mac_r : zero);
+  const int tt = t < 8 ? t : 7;   // rf_row's slot of a staged parameter (t = 8 is S1's)
+  int r = (t == 6 && (s == 0 || s == 3)) ? zero : rf_row(s, t == 8 ? 8 : tt);
+  if (t == 7) r = s == 0 ? NR + kXOne : zero;
+  if (NT == 11 && t == 9) r = mac_r;
+  if (t == NT - 1) r = alpha_r;
+  if (!free_t) r = zero;
+  if (t == NT) r = NR + kXRes + s;
+  scaled = c.use_slight && t < NT - 1;
+  return r;
 }
 
 // Normal equations alpha = sum_s w_s/sigma^2 J^T J and beta = sum_s w_s J^T
@@ -893,12 +891,17 @@ __device__ __forceinline__ void normal_eq(const DevCfg& c, const double* m, bool
   }
   __syncwarp();
   const int gr = lane >> 2, gc = lane & 3;
+  uint32_t fixmask = 0;
+#pragma unroll
+  for (int i = 0; i < 11; ++i) fixmask |= (c.fix[i] ? 1u : 0u) << i;
+  const float* rows0 = &sm.rows[0][0];
   double d00[2] = {0.0, 0.0}, d01[2] = {0.0, 0.0}, d11[2] = {0.0, 0.0};
 #pragma unroll 1
   for (int s = 0; s < 4; ++s) {
-    double sc0, sc1;
-    const float* r0 = jrow<LPL, V>(c, sm, gr, s, mac_on, alfa, sc0);
-    const float* r1 = jrow<LPL, V>(c, sm, 8 + gr, s, mac_on, alfa, sc1);
+    bool s0d, s1d;
+    const float* r0 = rows0 + jrow<LPL, V>(c, fixmask, gr, s, mac_on, s0d) * row_pitch<LPL>();
+    const float* r1 = rows0 + jrow<LPL, V>(c, fixmask, 8 + gr, s, mac_on, s1d) * row_pitch<LPL>();
+    const double sc0 = s0d ? alfa : 1.0, sc1 = s1d ? alfa : 1.0;
     const double wd = (double)c.wsig[s];
 #pragma unroll 4
     for (int k0 = 0; k0 < S; k0 += 4) {
