@@ -1008,10 +1008,14 @@ __device__ __forceinline__ SolvePlan make_solve_plan(int lane) {
 }
 
 // Solves for damping 1 + flambda into sm.vec[0][0] and, with two solves per
-// call, for 1 + flambda2 into sm.vec[1][0].
-template <int LPL, int V>
-__device__ __forceinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, float flambda,
-                                        float flambda2, int lane, bool accurate) {
+// call, for 1 + flambda2 into sm.vec[1][0].  `accurate` (the numerics mode)
+// is a template parameter and the solve an out-of-line function: a runtime
+// mode flag put three branches into every step, and inlined the solve adds
+// to the register pressure of the whole LM loop (together 7.6 % of the
+// kernel's time).
+template <int LPL, int V, bool accurate>
+__device__ __noinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, float flambda,
+                                        float flambda2, int lane) {
   constexpr int NS = Variant<V>::SOLVES, G = 32 / NS;
   const int h = NS == 2 ? lane >> 4 : 0;
   const int g = lane & (G - 1);

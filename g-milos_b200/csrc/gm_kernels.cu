@@ -127,7 +127,10 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
       if (!first) {
         if constexpr (NT == 10) {
           const bool reuse = Variant<V>::SOLVES == 2 && have_next;
-          if (!reuse) solve10<LPL, V>(sm, plan, flambda, flambda * 10.f * pbf, lane, c.numerics != 0);
+          if (!reuse) {
+            if (c.numerics) solve10<LPL, V, true>(sm, plan, flambda, flambda * 10.f * pbf, lane);
+            else solve10<LPL, V, false>(sm, plan, flambda, flambda * 10.f * pbf, lane);
+          }
           solved = !reuse;
           if (lane == 0) apply_delta_check<10>(c, sm.m, sm.vec[reuse ? 1 : 0][0], sm.t);
         } else {
