@@ -61,6 +61,9 @@ typedef struct {
     int classical_init;            /* 1: classical estimates override B, vlos, gm, az */
     int alpha_rf_mixed;            /* 1: reproduce the mixed-spectrum alpha response
                                       function after an accepted step (milosUtils.cu:675) */
+    double stop_dchi2;             /* > 0: also stop when an accepted step lowers chi2 by
+                                      less than this (the engine's optional early stop;
+                                      0 = the reference's stop rules only) */
 } orc_cfg;
 
 /* ---------------- host-side atomic / instrument helpers ----------------- */

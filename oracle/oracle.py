@@ -32,7 +32,7 @@ class Cfg(C.Structure):
                 ("fix", C.c_int * NPAR), ("init", C.c_double * NPAR),
                 ("miter", C.c_int), ("ilambda", C.c_double), ("toplim", C.c_double),
                 ("logclambda", C.c_int), ("classical_init", C.c_int),
-                ("alpha_rf_mixed", C.c_int)]
+                ("alpha_rf_mixed", C.c_int), ("stop_dchi2", C.c_double)]
 
 
 def build():
@@ -146,7 +146,8 @@ def psf_gauss(fwhm_mA, lam):
 
 def make_cfg(lam, lambda0, zeeman, psf=None, mu=1.0, weight=(1, 1, 1, 1), noise=1e-6,
              fix=(1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0), init=None, miter=50, ilambda=0.1,
-             toplim=1e-12, logclambda=0, classical_init=1, alpha_rf_mixed=1, nterms=None):
+             toplim=1e-12, logclambda=0, classical_init=1, alpha_rf_mixed=1, nterms=None,
+             stop_dchi2=0.0):
     c = Cfg()
     lam = np.asarray(lam, dtype=np.float64)
     c.nl = len(lam)
@@ -176,6 +177,7 @@ def make_cfg(lam, lambda0, zeeman, psf=None, mu=1.0, weight=(1, 1, 1, 1), noise=
     c.logclambda = logclambda
     c.classical_init = classical_init
     c.alpha_rf_mixed = alpha_rf_mixed
+    c.stop_dchi2 = stop_dchi2
     return c
 
 

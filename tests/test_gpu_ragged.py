@@ -1,0 +1,80 @@
+"""Ragged batches (gmilos_b200.batch.invert_rois): ROIs of many sizes on
+centred 35 mA grids of 12 to 60 samples, with the per-pixel early stop on
+an accepted chi2 gain below 1e-4.  The batch's results equal each ROI
+inverted alone bit for bit (pixels are independent), and sampled pixels
+match the faithful oracle with the full-inversion tolerances."""
+import numpy as np
+import pytest
+
+import gmilos_b200 as G
+from gmilos_b200 import batch
+import helpers as H
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+ZG = G.zeeman_from_levels(2, 1, 1.0, 2, 2, 0.0, 1.0)
+STOP = 1e-4
+
+
+def rois(seed, n=12):
+    rng = np.random.default_rng(seed)
+    l0, zo = H.fe_line()
+    out = []
+    for k in range(n):
+        nl = int(rng.choice([12, 20, 30, 31, 45, 60]))
+        side = int(rng.integers(2, 24))
+        lam, _ = H.grid(nl)
+        ocfg = O.make_cfg(lam, l0, zo, psf=O.psf_gauss(100.0, lam), init=H.GUESS)
+        t = H.truth_models(side * side, rng)
+        out.append((H.observations(ocfg, t, rng), lam))
+    return out
+
+
+def config_for(lam, numerics=0):
+    l0, _ = H.fe_line()
+    return G.make_config(lam, l0, ZG, psf=O.psf_gauss(100.0, lam), init=H.GUESS, stop_dchi2=STOP,
+                         numerics=numerics)
+
+
+def test_batch_equals_rois_alone():
+    rs = rois(31)
+    with G.Engine(0) as e:
+        got, summary = batch.invert_rois(e, rs, config_for)
+        assert summary["launches"] == len({batch.grid_key(l) for _, l in rs})
+        assert summary["pixels"] == sum(len(a) for a, _ in rs)
+        assert 0.1 < summary["lane_occupancy"] <= 1.0
+        for (a, lam), g in zip(rs, got):
+            e.configure(config_for(lam))
+            alone = e.invert(a)
+            for k in ("model", "chi2", "iters", "status"):
+                np.testing.assert_array_equal(g[k], alone[k], err_msg=k)
+
+
+def test_batch_against_the_oracle():
+    rs = rois(32)
+    with G.Engine(0) as e:
+        got, _ = batch.invert_rois(e, rs, lambda lam: config_for(lam, numerics=1))
+    l0, zo = H.fe_line()
+    ok = []
+    for (a, lam), g in zip(rs, got):
+        ocfg = O.make_cfg(lam, l0, zo, psf=O.psf_gauss(100.0, lam), init=H.GUESS, stop_dchi2=STOP)
+        for p in range(0, len(a), max(1, len(a) // 8)):
+            mr, cr, _, _, _ = O.lm_f(ocfg, a[p])
+            mg, cg = g["model64"][p], g["chi2"][p]
+            ok.append(cg <= cr * (1 + 1e-3) + 1e-6 or
+                      (abs(mg[1] - mr[1]) < 1.0 and H.angle_diff(mg[5], mr[5], 360) < 0.1
+                       and abs(mg[2] - mr[2]) < 0.005))
+    assert np.mean(ok) >= 0.97, np.mean(ok)
+
+
+def test_early_stop_shortens_the_fits():
+    rs = rois(33, n=4)
+    with G.Engine(0) as e:
+        with_stop, _ = batch.invert_rois(e, rs, config_for)
+        l0, _ = H.fe_line()
+        plain, _ = batch.invert_rois(e, rs, lambda lam: G.make_config(lam, l0, ZG, psf=O.psf_gauss(100.0, lam),
+                                                                         init=H.GUESS))
+    a = np.concatenate([r["iters"] for r in with_stop])
+    b = np.concatenate([r["iters"] for r in plain])
+    assert a.mean() < b.mean()
