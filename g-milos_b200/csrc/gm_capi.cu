@@ -5,6 +5,7 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -57,6 +58,12 @@ struct ServeLane {
   cudaStream_t stream = nullptr;
   gm::WorkCounters* work = nullptr;
   cudaEvent_t done = nullptr;
+  // one chunk's wave-kernel state, then its classical start models and
+  // status bits (null: the fused kernel serves this lane)
+  void* scratch = nullptr;
+  size_t wave_bytes = 0;
+  int nl = 0, miter = 0;
+  int64_t chunk = 0;
   std::shared_ptr<Request> req;
   bool busy = false;
 };
@@ -380,6 +387,37 @@ struct StepOut {
 
 // Pixels per chunk of a pipelined host-memory inversion (at least two chunks).
 constexpr int64_t kPipeChunk = 131072;
+// Pixels per chunk of the wave-synchronous inversion (its LM state and
+// staging take about 3.6 KB per pixel at nl <= 32, 6.6 KB above): large
+// chunks make each wave's launches long against their tails.  Below
+// kWaveMinChunk pixels within the budget the fused kernel runs instead.
+constexpr int64_t kWaveChunk = 1 << 20;
+constexpr int64_t kWaveMinChunk = 16384;
+
+// The wave-synchronous kernels cover the launch unless the environment
+// variable GMILOS_INVERT_KERNEL=fused selects the single persistent kernel
+// (both give the same results; the switch serves comparisons).
+static bool want_waves(const gm::DevCfg& d, const gm::InvertArgs& ia) {
+  const char* k = std::getenv("GMILOS_INVERT_KERNEL");
+  if (k && std::strcmp(k, "fused") == 0) return false;
+  return gm::waves_cover(d, ia);
+}
+
+// Pixels per wave chunk for a call of npix pixels that already needs `need`
+// bytes of the budget, with `sets` chunks in flight; 0: the fused kernel.
+static int64_t wave_chunk_for(const gm_ctx* ctx, const gm::DevCfg& d, size_t need, int64_t npix, int sets) {
+  int64_t ch = std::min<int64_t>(npix, kWaveChunk);
+  while (ch > 0 && need + sets * gm::wave_buffer_bytes(d.nl, d.miter, ch) > ctx->budget) ch /= 2;
+  return ch > 0 && ch >= std::min<int64_t>(npix, kWaveMinChunk) ? ch : 0;
+}
+
+static gm_status wave_buffers(gm_ctx* ctx, const char* name, const gm::DevCfg& d, int64_t chunk,
+                              gm::WaveBuffers* out) {
+  void* p = nullptr;
+  gm_status st = ensure_buf(ctx, name, gm::wave_buffer_bytes(d.nl, d.miter, chunk), &p);
+  if (st == GM_OK) *out = gm::wave_buffers(p, d.nl, d.miter, chunk);
+  return st;
+}
 
 // The chunked inversion of a host-memory cube: chunk k is copied up,
 // inverted and its outputs copied back on stream k % 2 (the caller's stream
@@ -390,14 +428,26 @@ constexpr int64_t kPipeChunk = 131072;
 // are the per-pixel outputs (per-pixel size = bytes / npix).
 static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::InvertArgs& ia,
                                const float* iquv, const Arg& a_in, const Arg* const* outs, int nouts,
-                               int64_t npix, int nl, bool prepass, cudaStream_t s) {
+                               int64_t npix, int nl, bool prepass, size_t need, cudaStream_t s) {
   const size_t row = 4 * (size_t)nl;
+  const int nch = (int)std::min<int64_t>(8, npix / kPipeChunk);
+  gm::DevCfg d1 = d;
+  if (prepass) d1.init_mode = 1;
+  const int64_t most = (npix + nch - 1) / nch;
+  // one wave chunk per pipeline chunk and stream
+  const bool waves = want_waves(d1, ia) && wave_chunk_for(ctx, d1, need, most, 2) == most;
+  gm::WaveBuffers wb[2];
+  if (waves) {
+    gm_status st = wave_buffers(ctx, "waves0", d1, most, &wb[0]);
+    if (st == GM_OK) st = wave_buffers(ctx, "waves1", d1, most, &wb[1]);
+    if (st != GM_OK) return st;
+  }
+  int launches = 0;
   cudaError_t e = cudaMemsetAsync(ctx->work, 0, sizeof(gm::WorkCounters), s);
   if (e == cudaSuccess) e = cudaMemsetAsync(ctx->work2, 0, sizeof(gm::WorkCounters), s);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->evx0, s);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->aux, ctx->evx0, 0);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "pipeline set-up");
-  const int nch = (int)std::min<int64_t>(8, npix / kPipeChunk);
   cudaEventRecord(ctx->ev0, s);
   for (int k = 0; k < nch && e == cudaSuccess; ++k) {
     const int64_t a = npix * k / nch, b = npix * (k + 1) / nch, n = b - a;
@@ -407,21 +457,8 @@ static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::Inver
                         cudaMemcpyHostToDevice, q);
     if (e == cudaSuccess) e = cudaMemsetAsync(&w->next_pixel, 0, sizeof(w->next_pixel), q);
     if (e != cudaSuccess) break;
-    gm::DevCfg dc = d;
-    if (d.use_slight && d.slight_per_pixel) dc.slight = d.slight + a * row;
-    if (d.lambda_per_pixel) dc.lam_map = d.lam_map + a * nl;
-    gm::InvertArgs c = ia;
-    c.iquv = ia.iquv + a * row;
-    c.npix = n;
-    if (ia.init_models) c.init_models = ia.init_models + a * 11;
-    if (ia.init_status) c.init_status = ia.init_status + a;
-    if (ia.model) c.model = ia.model + a * 11;
-    if (ia.model_f64) c.model_f64 = ia.model_f64 + a * 11;
-    if (ia.chi2) c.chi2 = ia.chi2 + a;
-    if (ia.iters) c.iters = ia.iters + a;
-    if (ia.accepted) c.accepted = ia.accepted + a;
-    if (ia.fitted) c.fitted = ia.fitted + a * row;
-    if (ia.status) c.status = ia.status + a;
+    gm::DevCfg dc = gm::offset_cfg(d, a);
+    gm::InvertArgs c = gm::offset_args(ia, a, n, nl, d.nterms);
     c.work = w;
     gm::InvertGeometry geo;
     if (prepass) {
@@ -431,7 +468,14 @@ static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::Inver
       dc.init_mode = 1;
     }
     const int64_t grid = invert_grid(dc, c.init_models != nullptr && !c.init_status, ctx->sms, n, &geo);
-    e = gm::launch_invert(dc, c, (int)grid, q);
+    if (waves) {
+      int nk = 0;
+      e = gm::launch_invert_waves(dc, c, wb[k & 1], q, &nk);
+      launches += nk + (prepass ? 1 : 0);
+    } else {
+      e = gm::launch_invert(dc, c, (int)grid, q);
+      launches += 1 + (prepass ? 1 : 0);
+    }
     ctx->stats.grid_blocks = (int)grid;
     ctx->stats.block_threads = geo.threads;
     ctx->stats.warps_per_block = geo.threads / 32;
@@ -447,7 +491,7 @@ static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::Inver
   if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ctx->evx1, 0);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "pipelined inversion");
   cudaEventRecord(ctx->ev1, s);
-  ctx->stats.kernel_launches = nch;
+  ctx->stats.kernel_launches = launches;
   ctx->stats.pixels = npix;
   // the cube came from host memory: the call returns with its results in place
   e = cudaStreamSynchronize(s);
@@ -548,7 +592,7 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   }
   const Arg* outs[] = {&a_model, &a_m64, &a_chi, &a_it, &a_acc, &a_fit, &a_st,
                        &a_sd, &a_strial, &a_sc0, &a_sc1};
-  if (pipeline) return invert_chunks(ctx, d, ia, iquv, a_in, outs, 7, npix, nl, prepass, s);
+  if (pipeline) return invert_chunks(ctx, d, ia, iquv, a_in, outs, 7, npix, nl, prepass, need, s);
   cudaError_t e = cudaMemsetAsync(ctx->work, 0, sizeof(gm::WorkCounters), s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "work counter reset");
   if (prepass) {
@@ -559,14 +603,19 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   }
   gm::InvertGeometry geo;
   const int64_t grid = invert_grid(d, ia.init_models != nullptr && !ia.init_status, ctx->sms, npix, &geo);
+  const int64_t wchunk = want_waves(d, ia) ? wave_chunk_for(ctx, d, need, npix, 1) : 0;
+  const bool waves = wchunk > 0;
+  gm::WaveBuffers wb{};
+  if (waves && (st = wave_buffers(ctx, "waves0", d, wchunk, &wb)) != GM_OK) return st;
+  int launches = 1;
   cudaEventRecord(ctx->ev0, s);
-  e = gm::launch_invert(d, ia, (int)grid, s);
+  e = waves ? gm::launch_invert_waves(d, ia, wb, s, &launches) : gm::launch_invert(d, ia, (int)grid, s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "inversion kernel launch");
   cudaEventRecord(ctx->ev1, s);
   ctx->stats.grid_blocks = (int)grid;
   ctx->stats.block_threads = geo.threads;
   ctx->stats.warps_per_block = geo.threads / 32;
-  ctx->stats.kernel_launches = 1;
+  ctx->stats.kernel_launches = launches + (prepass ? 1 : 0);
   ctx->stats.pixels = npix;
   bool any_host = false;
   for (const Arg* o : outs) {
@@ -951,8 +1000,25 @@ gm_status launch_chunk(gm_ctx* ctx, ServeLane& L, const std::shared_ptr<Request>
   ia.iters = r.d_iters ? r.d_iters + off : nullptr;
   ia.status = r.d_status ? r.d_status + off : nullptr;
   ia.work = L.work;
-  const int64_t grid = invert_grid(r.dev, false, ctx->sms, n, nullptr);
-  e = gm::launch_invert(r.dev, ia, (int)grid, s);
+  // the path of gm_invert: classical start models in a pre-pass, then the
+  // wave-synchronous kernels where they cover the configuration
+  gm::DevCfg d = r.dev;
+  const bool lane_ok = L.scratch && L.nl == d.nl && L.miter == d.miter && n <= L.chunk;
+  if (lane_ok && d.init_mode == 0) {
+    double* cm = reinterpret_cast<double*>(static_cast<char*>(L.scratch) + L.wave_bytes);
+    uint32_t* cs = reinterpret_cast<uint32_t*>(cm + 11 * L.chunk);
+    e = gm::launch_classical(d, ia.iquv, n, cm, cs, true, s);
+    if (e != cudaSuccess) return GM_ERR_CUDA;
+    ia.init_models = cm;
+    ia.init_status = cs;
+    d.init_mode = 1;
+  }
+  if (lane_ok && want_waves(d, ia)) {
+    e = gm::launch_invert_waves(d, ia, gm::wave_buffers(L.scratch, d.nl, d.miter, L.chunk), s, nullptr);
+  } else {
+    const int64_t grid = invert_grid(d, ia.init_models != nullptr && !ia.init_status, ctx->sms, n, nullptr);
+    e = gm::launch_invert(d, ia, (int)grid, s);
+  }
   if (e != cudaSuccess) return GM_ERR_CUDA;
   auto back = [&](void* host, const void* dev, size_t bytes) {
     if (e == cudaSuccess && host && host != dev) e = cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, s);
@@ -998,6 +1064,15 @@ void serve_loop(gm_ctx* ctx) {
       cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking);
       cudaMalloc(&L.work, sizeof(gm::WorkCounters));
       cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming);
+      L.nl = ctx->dev.nl;
+      L.miter = ctx->dev.miter;
+      L.chunk = ctx->serve_chunk;
+      L.wave_bytes = (gm::wave_buffer_bytes(L.nl, L.miter, L.chunk) + 255) & ~(size_t)255;
+      if (cudaMalloc(&L.scratch, L.wave_bytes + (sizeof(double) * 11 + sizeof(uint32_t)) * (size_t)L.chunk) !=
+          cudaSuccess) {
+        cudaGetLastError();
+        L.scratch = nullptr;
+      }
     }
   }
   for (;;) {
@@ -1082,6 +1157,7 @@ void serve_loop(gm_ctx* ctx) {
   for (ServeLane& L : ctx->lanes) {
     cudaStreamSynchronize(L.stream);
     cudaFree(L.work);
+    if (L.scratch) cudaFree(L.scratch);
     cudaEventDestroy(L.done);
     cudaStreamDestroy(L.stream);
   }

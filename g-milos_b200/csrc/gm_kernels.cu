@@ -1,4 +1,6 @@
 // gm_kernels.cu -- persistent LM inversion kernel, synthesis kernels.
+#include <cstddef>
+
 #include "gm_kernels.cuh"
 
 namespace gm {
@@ -220,6 +222,341 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
   if (lane == 0 && (my_iter | my_acc)) {
     atomicAdd(&a.work->iterations, my_iter);
     atomicAdd(&a.work->accepted, my_acc);
+  }
+}
+
+// ------------------------------------------------- wave-synchronous inversion
+// The same LM iteration as invert_kernel, split at its two halves and run
+// for every pixel of a chunk in lockstep waves (10-term path without
+// macroturbulence, the reference's default configuration).  Wave w launches
+// trial_kernel over the pixels still iterating -- the step solve (both
+// dampings), the step limits, the trial synthesis with PSF and stray light,
+// chi2 and the damping schedule -- then accept_kernel over the pixels whose
+// trial was accepted: response functions, their PSF and the normal
+// equations.  Each kernel executes about a third of invert_kernel's code,
+// so the warps of an SM share one hot instruction working set, and each has
+// its own register budget (the trial half runs 20 warps per SM).  A pixel's
+// LM state lives in a PixLM record between the kernels; the per-lane Voigt
+// and Zeeman terms, angles and profiles of an accepted trial reach the
+// accept kernel through a staging row block, so nothing is recomputed and
+// every pixel performs exactly invert_kernel's arithmetic.
+
+template <int LPL>
+constexpr int trial_min_blocks() { return LPL == 1 ? 7 : 8; }
+template <int LPL>
+constexpr int accept_min_blocks() { return LPL == 1 ? 5 : 5; }
+
+// The trial half touches the warp's shared memory only up to the first
+// 8-row tile of staged rows (the synthesis PSF stages rows 0-3), so its
+// warps are packed at that stride: half the footprint, more warps per SM.
+template <int LPL>
+__host__ __device__ constexpr size_t trial_warp_bytes() {
+  using WS = WarpSmem<LPL, 0>;
+  return (offsetof(WS, rows) + 8 * row_pitch<LPL>() * sizeof(float) + 15) & ~(size_t)15;
+}
+template <int LPL>
+__device__ __forceinline__ WarpSmem<LPL, 0>& trial_smem() {
+  return *reinterpret_cast<WarpSmem<LPL, 0>*>(gm_dyn_smem + tap_bytes<LPL>() +
+                                               (threadIdx.x >> 5) * trial_warp_bytes<LPL>());
+}
+
+// Staged rows of an accepted trial (one float per lane each): per sample
+// slot k the 15 Lane terms, then syn and pure; the last row holds the angles.
+template <int LPL>
+__device__ __forceinline__ void stage_put(float* __restrict__ q, const Lane<LPL, 0>& ln, const Angles& an,
+                                          const float (&syn)[LPL][4], const float (&pure)[LPL][4], int lane) {
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    float* r = q + k * 23 * 32 + lane;
+#pragma unroll
+    for (int g = 0; g < 3; ++g) {
+      r[(0 + g) * 32] = ln.fi[k][g];
+      r[(3 + g) * 32] = ln.shi[k][g];
+      r[(6 + g) * 32] = ln.lh[k][g];
+      r[(9 + g) * 32] = ln.lf[k][g];
+      r[(12 + g) * 32] = ln.lu[k][g];
+    }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      r[(15 + s) * 32] = syn[k][s];
+      r[(19 + s) * 32] = pure[k][s];
+    }
+  }
+  if (lane == 0) {
+    float* r = q + LPL * 23 * 32;
+    r[0] = an.cosi; r[1] = an.sinis; r[2] = an.sina; r[3] = an.cosa; r[4] = an.sinda;
+    r[5] = an.cosda; r[6] = an.sindi; r[7] = an.cosdi; r[8] = an.cosis_2;
+  }
+}
+
+template <int LPL>
+__device__ __forceinline__ void stage_get(const float* __restrict__ q, Lane<LPL, 0>& ln, Angles& an,
+                                          float (&syn)[LPL][4], float (&pure)[LPL][4], int lane) {
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const float* r = q + k * 23 * 32 + lane;
+#pragma unroll
+    for (int g = 0; g < 3; ++g) {
+      ln.fi[k][g] = r[(0 + g) * 32];
+      ln.shi[k][g] = r[(3 + g) * 32];
+      ln.lh[k][g] = r[(6 + g) * 32];
+      ln.lf[k][g] = r[(9 + g) * 32];
+      ln.lu[k][g] = r[(12 + g) * 32];
+    }
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      syn[k][s] = r[(15 + s) * 32];
+      pure[k][s] = r[(19 + s) * 32];
+    }
+  }
+  const float* r = q + LPL * 23 * 32;
+  an.cosi = r[0]; an.sinis = r[1]; an.sina = r[2]; an.cosa = r[3]; an.sinda = r[4];
+  an.cosda = r[5]; an.sindi = r[6]; an.cosdi = r[7]; an.cosis_2 = r[8];
+}
+
+// Outputs of a pixel that stopped (as invert_kernel writes them).
+template <int LPL>
+__device__ __forceinline__ void finish_pixel(const InvertArgs& a, const double* m, float ochisqr, int iter,
+                                             int acc, uint32_t st, const float (&syn)[LPL][4],
+                                             uint64_t pix, int nl, int lane) {
+  if (lane < 11) {
+    if (a.model) a.model[pix * 11 + lane] = (float)m[lane];
+    if (a.model_f64) a.model_f64[pix * 11 + lane] = m[lane];
+  }
+  if (lane == 0) {
+    if (a.chi2) a.chi2[pix] = ochisqr;
+    if (a.iters) a.iters[pix] = iter;
+    if (a.accepted) a.accepted[pix] = acc;
+    if (a.status) a.status[pix] = st;
+  }
+  if (a.fitted) {
+    const size_t off = (size_t)pix * 4 * nl;
+#pragma unroll
+    for (int k = 0; k < LPL; ++k) {
+      const int l = lane + 32 * k;
+      if (l < nl)
+#pragma unroll
+        for (int s = 0; s < 4; ++s) a.fitted[off + s * nl + l] = syn[k][s];
+    }
+  }
+}
+
+// One trial of every pixel in the wave's active list (wave 0: the start
+// models, every pixel of the chunk).  The body is invert_kernel's loop
+// body from the solve to the damping schedule (milosUtils.cu:630-700).
+template <int LPL>
+__global__ void __launch_bounds__(warps_per_block<LPL>() * 32, trial_min_blocks<LPL>())
+trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
+  const int lane = threadIdx.x & 31;
+  load_taps<LPL>(c);
+  WarpSmem<LPL, 0>& sm = trial_smem<LPL>();
+  for (int i = lane; i < 8 * row_pitch<LPL>(); i += 32) (&sm.rows[0][0])[i] = 0.f;
+  __syncwarp();
+  const int nl = c.nl;
+  float dlv[LPL];
+  double dld[LPL];
+  bool valid[LPL];
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+    valid[k] = l < nl;
+    dlv[k] = valid[k] ? c.dl[l] : 0.f;
+    dld[k] = valid[k] ? c.dld[l] : 0.0;
+  }
+  float slg[LPL][4];
+  if (c.use_slight && !c.slight_per_pixel) load_pixel<LPL>(c.slight, nl, lane, slg);
+  else {
+#pragma unroll
+    for (int k = 0; k < LPL; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
+  }
+  const SolvePlan plan = make_solve_plan<2>(lane);
+  const uint32_t n = wave == 0 ? (uint32_t)a.npix : w.cnt[wave - 1].n_next;
+  const uint32_t* in = (wave & 1) ? w.act1 : w.act0;
+  uint32_t* next = (wave & 1) ? w.act0 : w.act1;
+  unsigned long long my_iter = 0, my_acc = 0;
+  while (true) {
+    uint32_t j = 0;
+    if (lane == 0) j = atomicAdd(&w.cnt[wave].cur_trial, 1u);
+    j = __shfl_sync(kFull, j, 0);
+    if (j >= n) break;
+    const uint32_t pix = wave == 0 ? j : in[j];
+    PixLM& P = w.state[pix];
+    const size_t off = (size_t)pix * 4 * nl;
+    float ob[LPL][4];
+    load_pixel<LPL>(a.iquv + off, nl, lane, ob);
+    if (c.use_slight && c.slight_per_pixel) load_pixel<LPL>(c.slight + off, nl, lane, slg);
+    const double* lamp = pixel_grid<LPL>(c, pix, lane, dlv, dld);
+
+    float flambda, pbf, ochisqr, chisqr0;
+    int iter, acc;
+    uint32_t st;
+    bool solved = false;
+    if (wave == 0) {
+      if (lane < 11) sm.m[lane] = a.init_models ? a.init_models[(size_t)pix * 11 + lane] : c.init[lane];
+      st = a.init_status ? a.init_status[pix] : 0u;
+      flambda = c.ilambda;
+      pbf = 1.f;
+      ochisqr = chisqr0 = 0.f;
+      iter = acc = 0;
+      __syncwarp();
+    } else {
+      const bool reuse = P.flags & 1u;
+      if (lane < 11) {
+        sm.m[lane] = P.m[lane];
+        sm.t[lane] = P.t[lane];
+      }
+      flambda = P.flambda;
+      pbf = P.pbf;
+      ochisqr = P.ochisqr;
+      chisqr0 = P.chisqr0;
+      iter = P.iter;
+      acc = P.acc;
+      st = P.st;
+      if (reuse) {
+        if (lane < 10) sm.vec[1][0][lane] = P.vnext[lane];
+      } else {
+        for (int i = lane; i < 55; i += 32) sm.alpha[i] = P.alpha[i];
+        if (lane < 10) sm.beta[lane] = P.beta[lane];
+      }
+      __syncwarp();
+      if (!reuse) {
+        if (c.numerics) solve10<LPL, 0, true>(sm, plan, flambda, flambda * 10.f * pbf, lane);
+        else solve10<LPL, 0, false>(sm, plan, flambda, flambda * 10.f * pbf, lane);
+      }
+      solved = !reuse;
+      if (lane == 0) apply_delta_check<10>(c, sm.m, sm.vec[reuse ? 1 : 0][0], sm.t);
+      __syncwarp();
+    }
+    Lane<LPL, 0> ln;
+    Angles an;
+    float syn[LPL][4], pure[LPL][4];
+    synth_lane<LPL, 0>(c, wave == 0 ? sm.m : sm.t, dlv, lane, ln, an, syn, pure, slg, sm, lamp);
+    const float chisqr = chisq<LPL>(c, syn, ob, valid);
+    bool accept = true, stop = false, have_next = false;
+    if (wave == 0) {
+      ochisqr = chisqr;
+      chisqr0 = chisqr;
+      if (lane < 11) sm.t[lane] = sm.m[lane];
+    } else {
+      // stop rules and damping schedule (milosUtils.cu:667-696)
+      if ((double)fabsf(((ochisqr) - (chisqr)) * 100 / (chisqr)) < c.toplim || (chisqr) < 0.0001f) {
+        stop = true;
+        st |= GM_PIX_CHI2_EXIT;
+      }
+      accept = (chisqr) - (ochisqr) < 0.f;
+      if (accept) {
+        flambda = flambda / (5.f * pbf);
+        if (c.stop_dchi2 > 0.0 && (double)(ochisqr - chisqr) < c.stop_dchi2) stop = true;
+        if (lane < 11) sm.m[lane] = sm.t[lane];
+        ++acc;
+      } else {
+        flambda = flambda * 10.f * pbf;
+      }
+      if (flambda > 1e+7f || flambda < 1e-25f) {
+        stop = true;
+        st |= GM_PIX_LAMBDA_EXIT;
+      }
+      ++iter;
+      have_next = !accept && solved;
+      if (c.logclambda) pbf = log10f(chisqr) / log10f(chisqr0);
+      if (accept) ochisqr = chisqr;
+    }
+    __syncwarp();
+    if (wave > 0 && (iter >= c.miter || stop)) {
+      if (!stop) st |= GM_PIX_MAXITER;
+      if (!isfinite(ochisqr)) st |= GM_PIX_NONFINITE;
+      finish_pixel<LPL>(a, sm.m, ochisqr, iter, acc, st, syn, pix, nl, lane);
+      my_iter += iter;
+      my_acc += acc;
+    } else {
+      if (lane < 11) {
+        P.m[lane] = sm.m[lane];
+        P.t[lane] = sm.t[lane];
+      }
+      if (solved && lane < 10) P.vnext[lane] = sm.vec[1][0][lane];
+      uint32_t slot = 0, aslot = 0;
+      if (lane == 0) {
+        P.flambda = flambda;
+        P.pbf = pbf;
+        P.ochisqr = ochisqr;
+        P.chisqr0 = chisqr0;
+        P.iter = iter;
+        P.acc = acc;
+        P.st = st;
+        P.flags = have_next ? 1u : 0u;
+        slot = atomicAdd(&w.cnt[wave].n_next, 1u);
+        if (accept) aslot = atomicAdd(&w.cnt[wave].n_acc, 1u);
+      }
+      slot = __shfl_sync(kFull, slot, 0);
+      aslot = __shfl_sync(kFull, aslot, 0);
+      if (lane == 0) next[slot] = pix;
+      if (accept) {
+        stage_put<LPL>(w.stage + (size_t)pix * stage_floats<LPL>(), ln, an, syn, pure, lane);
+        if (lane == 0) w.accl[aslot] = pix;
+      }
+    }
+    __syncwarp();
+  }
+  if (lane == 0 && (my_iter | my_acc)) {
+    atomicAdd(&a.work->iterations, my_iter);
+    atomicAdd(&a.work->accepted, my_acc);
+  }
+}
+
+// Response functions and normal equations of every pixel whose trial of
+// this wave was accepted (the accept branch of invert_kernel's loop).
+template <int LPL>
+__global__ void __launch_bounds__(warps_per_block<LPL>() * 32, accept_min_blocks<LPL>())
+accept_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
+  const int lane = threadIdx.x & 31;
+  load_taps<LPL>(c);
+  WarpSmem<LPL, 0>& sm = warp_smem<LPL, 0>();
+  init_rows<LPL, 0>(c, sm, lane);
+  const int nl = c.nl;
+  float dlv[LPL];
+  double dld[LPL];
+  bool valid[LPL];
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    valid[k] = lane + 32 * k < nl;
+    dlv[k] = 0.f;
+    dld[k] = 0.0;
+  }
+  float slg[LPL][4];
+  if (c.use_slight && !c.slight_per_pixel) load_pixel<LPL>(c.slight, nl, lane, slg);
+  else {
+#pragma unroll
+    for (int k = 0; k < LPL; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
+  }
+  const uint32_t n = w.cnt[wave].n_acc;
+  const bool alpha_mixed = wave > 0 && c.quirks;
+  while (true) {
+    uint32_t j = 0;
+    if (lane == 0) j = atomicAdd(&w.cnt[wave].cur_acc, 1u);
+    j = __shfl_sync(kFull, j, 0);
+    if (j >= n) break;
+    const uint32_t pix = w.accl[j];
+    PixLM& P = w.state[pix];
+    const size_t off = (size_t)pix * 4 * nl;
+    float ob[LPL][4];
+    load_pixel<LPL>(a.iquv + off, nl, lane, ob);
+    if (c.use_slight && c.slight_per_pixel) load_pixel<LPL>(c.slight + off, nl, lane, slg);
+    const double* lamp = pixel_grid<LPL>(c, pix, lane, dlv, dld);
+    if (lane < 11) sm.m[lane] = P.m[lane];
+    Lane<LPL, 0> ln;
+    Angles an;
+    float syn[LPL][4], pure[LPL][4];
+    stage_get<LPL>(w.stage + (size_t)pix * stage_floats<LPL>(), ln, an, syn, pure, lane);
+    __syncwarp();
+    rf_rows<LPL, 0>(c, sm.m, ln, an, lane, sm, lamp);
+    normal_eq<LPL, 0>(c, sm.m, alpha_mixed, pure, slg, syn, ob, valid, lane, sm);
+    for (int i = lane; i < 55; i += 32) P.alpha[i] = sm.alpha[i];
+    if (lane < 10) P.beta[lane] = sm.beta[lane];
+    __syncwarp();
   }
 }
 
@@ -494,6 +831,86 @@ cudaError_t launch_invert(const DevCfg& cfg, const InvertArgs& a, int grid, cuda
   if (v == 0) return launch_invert_t<2, 0>(cfg, a, grid, s);
   if (v == 1) return launch_invert_t<2, 1>(cfg, a, grid, s);
   return launch_invert_t<2, 2>(cfg, a, grid, s);
+}
+
+// ---------------------------------------------- wave-synchronous launcher
+size_t wave_buffer_bytes(int nl, int miter, int64_t chunk) {
+  const int lpl = nl <= 32 ? 1 : 2;
+  const int waves = 1 + (miter > 1 ? miter : 1);
+  return (size_t)chunk * (sizeof(PixLM) + sizeof(float) * stage_floats_for(lpl) + 3 * sizeof(uint32_t)) +
+         sizeof(WaveCounters) * (size_t)waves + 256;
+}
+
+WaveBuffers wave_buffers(void* base, int nl, int miter, int64_t chunk) {
+  const int lpl = nl <= 32 ? 1 : 2;
+  const int waves = 1 + (miter > 1 ? miter : 1);
+  char* p = static_cast<char*>(base);
+  WaveBuffers b{};
+  b.chunk = chunk;
+  b.w.state = reinterpret_cast<PixLM*>(p);
+  p += sizeof(PixLM) * (size_t)chunk;
+  b.w.stage = reinterpret_cast<float*>(p);
+  p += sizeof(float) * stage_floats_for(lpl) * (size_t)chunk;
+  b.w.cnt = reinterpret_cast<WaveCounters*>(p);
+  p += (sizeof(WaveCounters) * (size_t)waves + 255) & ~(size_t)255;
+  b.w.act0 = reinterpret_cast<uint32_t*>(p);
+  b.w.act1 = b.w.act0 + chunk;
+  b.w.accl = b.w.act1 + chunk;
+  return b;
+}
+
+bool waves_cover(const DevCfg& cfg, const InvertArgs& a) {
+  return kernel_variant(cfg, a.init_models != nullptr && !a.init_status) == 0 && cfg.init_mode != 0 &&
+         !a.step_delta && !a.step_trial && !a.step_chi2_start && !a.step_chi2_trial;
+}
+
+template <int LPL>
+cudaError_t launch_waves_t(const DevCfg& cfg, const InvertArgs& a, const WaveBuffers& b, cudaStream_t s,
+                           int* launches) {
+  const size_t smem = smem_bytes<LPL, 0>();
+  const size_t tsmem = tap_bytes<LPL>() + trial_warp_bytes<LPL>() * warps_per_block<LPL>();
+  cudaError_t e = cudaFuncSetAttribute(trial_kernel<LPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(accept_kernel<LPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int threads = warps_per_block<LPL>() * 32;
+  int dev = 0, sms = 0, bt = 0, ba = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, trial_kernel<LPL>, threads, tsmem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ba, accept_kernel<LPL>, threads, smem);
+  if (bt < 1 || ba < 1) return cudaErrorInvalidConfiguration;
+  const int waves = 1 + (cfg.miter > 1 ? cfg.miter : 1);
+  int count = 0;
+  for (int64_t first = 0; first < a.npix; first += b.chunk) {
+    const int64_t n = a.npix - first < b.chunk ? a.npix - first : b.chunk;
+    const DevCfg dc = offset_cfg(cfg, first);
+    const InvertArgs c = offset_args(a, first, n, cfg.nl, cfg.nterms);
+    const int64_t need = (n + warps_per_block<LPL>() - 1) / warps_per_block<LPL>();
+    const int gt = (int)(need < (int64_t)bt * sms ? need : (int64_t)bt * sms);
+    const int ga = (int)(need < (int64_t)ba * sms ? need : (int64_t)ba * sms);
+    e = cudaMemsetAsync(b.w.cnt, 0, sizeof(WaveCounters) * (size_t)waves, s);
+    if (e != cudaSuccess) return e;
+    for (int wv = 0; wv < waves; ++wv) {
+      trial_kernel<LPL><<<gt, threads, tsmem, s>>>(dc, c, b.w, wv);
+      ++count;
+      // the last wave's pixels all stop: nothing to accept
+      if (wv + 1 < waves) {
+        accept_kernel<LPL><<<ga, threads, smem, s>>>(dc, c, b.w, wv);
+        ++count;
+      }
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (launches) *launches = count;
+  return cudaSuccess;
+}
+
+cudaError_t launch_invert_waves(const DevCfg& cfg, const InvertArgs& a, const WaveBuffers& b, cudaStream_t s,
+                                int* launches) {
+  if (!waves_cover(cfg, a) || b.chunk < 1 || b.chunk > 0x7fffffff) return cudaErrorInvalidValue;
+  return cfg.nl <= 32 ? launch_waves_t<1>(cfg, a, b, s, launches) : launch_waves_t<2>(cfg, a, b, s, launches);
 }
 
 template <int LPL, int V>

@@ -40,6 +40,79 @@ struct InvertArgs {
   WorkCounters* work;         // zeroed before the launch
 };
 
+// Wave-synchronous inversion (launch_invert_waves): the LM state of one
+// pixel between the trial and the accept kernel of a wave.
+struct PixLM {
+  double m[11], t[11];         // accepted and trial models
+  float alpha[56], beta[10];   // normal equations of the accepted model (packed alpha)
+  float vnext[10];             // step for the damping a rejection moves to
+  float flambda, pbf, ochisqr, chisqr0;
+  int iter, acc;
+  uint32_t st, flags;          // status bits; flags bit 0: vnext holds the next step
+};
+static_assert(sizeof(PixLM) == 512, "PixLM is one 512-byte record");
+
+// Per wave: the trial kernel's cursor, the pixels it passes to the next wave
+// and to the accept kernel, and the accept kernel's cursor.
+struct WaveCounters {
+  unsigned int cur_trial, n_next, n_acc, cur_acc;
+};
+
+// Floats of one pixel's staged trial (accepted trial -> accept kernel): 23
+// rows of 32 lanes per sample slot and a row of angles.
+__host__ __device__ constexpr int stage_floats_for(int lpl) { return (23 * lpl + 1) * 32; }
+template <int LPL>
+__host__ __device__ constexpr int stage_floats() { return stage_floats_for(LPL); }
+
+struct WaveArgs {
+  PixLM* state;                // [chunk]
+  float* stage;                // [chunk][stage_floats]
+  uint32_t* act0;              // pixels iterating in even / odd waves
+  uint32_t* act1;
+  uint32_t* accl;              // pixels accepted in the current wave
+  WaveCounters* cnt;           // [waves], zeroed per chunk
+};
+
+// Device memory of a wave-synchronous inversion, carved from one buffer.
+struct WaveBuffers {
+  WaveArgs w;
+  int64_t chunk;               // pixels per chunk
+};
+size_t wave_buffer_bytes(int nl, int miter, int64_t chunk);
+WaveBuffers wave_buffers(void* base, int nl, int miter, int64_t chunk);
+// Whether the wave path covers a launch: the 10-term path without
+// macroturbulence, start models given or configured (no in-kernel
+// classical estimates), no first-step outputs.
+bool waves_cover(const DevCfg& cfg, const InvertArgs& a);
+
+// Arguments of the pixels [first, first + n) of a launch.
+inline InvertArgs offset_args(const InvertArgs& ia, int64_t first, int64_t n, int nl, int nterms) {
+  const size_t row = 4 * (size_t)nl;
+  InvertArgs c = ia;
+  c.iquv = ia.iquv + first * row;
+  c.npix = n;
+  if (ia.init_models) c.init_models = ia.init_models + first * 11;
+  if (ia.init_status) c.init_status = ia.init_status + first;
+  if (ia.model) c.model = ia.model + first * 11;
+  if (ia.model_f64) c.model_f64 = ia.model_f64 + first * 11;
+  if (ia.chi2) c.chi2 = ia.chi2 + first;
+  if (ia.iters) c.iters = ia.iters + first;
+  if (ia.accepted) c.accepted = ia.accepted + first;
+  if (ia.fitted) c.fitted = ia.fitted + first * row;
+  if (ia.status) c.status = ia.status + first;
+  if (ia.step_delta) c.step_delta = ia.step_delta + first * nterms;
+  if (ia.step_trial) c.step_trial = ia.step_trial + first * 11;
+  if (ia.step_chi2_start) c.step_chi2_start = ia.step_chi2_start + first;
+  if (ia.step_chi2_trial) c.step_chi2_trial = ia.step_chi2_trial + first;
+  return c;
+}
+inline DevCfg offset_cfg(const DevCfg& d, int64_t first) {
+  DevCfg dc = d;
+  if (d.use_slight && d.slight_per_pixel) dc.slight = d.slight + first * 4 * (int64_t)d.nl;
+  if (d.lambda_per_pixel) dc.lam_map = d.lam_map + first * (int64_t)d.nl;
+  return dc;
+}
+
 struct SynthArgs {
   const float* models_f32;    // [P][11] (one of the two)
   const double* models_f64;
@@ -50,6 +123,10 @@ struct SynthArgs {
 
 // launchers (gm_kernels.cu); return the CUDA error of the launch
 cudaError_t launch_invert(const DevCfg& cfg, const InvertArgs& a, int grid, cudaStream_t s);
+// The wave-synchronous inversion of a.npix pixels in chunks of b.chunk on
+// stream s (waves_cover must hold); *launches receives the kernel count.
+cudaError_t launch_invert_waves(const DevCfg& cfg, const InvertArgs& a, const WaveBuffers& b, cudaStream_t s,
+                                int* launches);
 cudaError_t launch_synth(const DevCfg& cfg, const SynthArgs& a, cudaStream_t s);
 // classical estimates: for_init false -> the classical-estimates mode
 // (S0 = B_los); true -> start models of an inversion plus status bits
