@@ -41,9 +41,10 @@ FIX = (1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 1)          # 9 ME parameters + alpha
 STRAY_MODEL = (10.0, 0.0, 0.0, 0.03, 0.1, 0.0, 0.0, 0.3, 0.7, 0.0, 1.0)
 MAXITER = 50
 
-# DRAM bytes (read + write) per pixel of the inversion kernel, measured with
-# ncu (dram__bytes_read.sum + dram__bytes_write.sum) on one 65 536-pixel
-# launch of this workload; traffic grows with the pixel count.
+# DRAM bytes (read + write) per pixel of one inversion (classical pre-pass
+# and every trial / accept wave), measured with ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum summed over the launches) on a 65 536-pixel inversion
+# of this workload; traffic grows with the pixel count.
 DRAM_BYTES_PER_PIXEL = 585.0
 
 # Algorithmic FLOPs per pixel (per-wavelength costs counted from the formulas)
@@ -272,6 +273,7 @@ def run_engine(args):
         evs[k][1].record(stream)
     t_end.record(stream)
     torch.cuda.synchronize()
+    launches_per_step = int(eng.stats()["kernel_launches"])
     if world > 1:
         dist.barrier()
     stop.set()
@@ -332,11 +334,15 @@ def run_engine(args):
                    "mean_iterations": iters_sum / P, "mean_accepted": acc_sum / P,
                    "l2_policy": "inputs 480 MB per GPU > 126 MB L2, no flush", "parallelism": "replicas (weak scaling, no collective)"},
         "e2e": {"value": e2e_value, "unit": "pixels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak if fp32_peak else None,
                      "traffic": DRAM_BYTES_PER_PIXEL * P,
-                     "traffic_note": "bytes per launch, scaled from an ncu capture of a 65536-pixel launch",
+                     "traffic_note": "bytes per inversion (pre-pass + trial/accept waves), scaled from an ncu "
+                                     "capture of a 65536-pixel inversion",
+                     "kernels": "one step = classical pre-pass + %d trial_kernel / accept_kernel launches "
+                                "(wave-synchronous LM); achieved = algorithmic FLOPs / the step's device time"
+                                % (launches_per_step - 1),
                      "peak_source": "measured FFMA microbenchmark (gm_measure_peaks), burst",
                      "fp64_peak": fp64_peak,
                      "flops_per_launch": flops_launch, "launch_ms": launch_avg,

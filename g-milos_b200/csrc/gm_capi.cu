@@ -385,7 +385,7 @@ struct StepOut {
   float* chi2_trial = nullptr;
 };
 
-// Pixels per chunk of a pipelined host-memory inversion (at least two chunks).
+// Smallest pipelined host-memory inversion: two chunks of kPipeChunk pixels.
 constexpr int64_t kPipeChunk = 131072;
 // Pixels per chunk of the wave-synchronous inversion (its LM state and
 // staging take about 3.6 KB per pixel at nl <= 32, 6.6 KB above): large
@@ -430,7 +430,9 @@ static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::Inver
                                const float* iquv, const Arg& a_in, const Arg* const* outs, int nouts,
                                int64_t npix, int nl, bool prepass, size_t need, cudaStream_t s) {
   const size_t row = 4 * (size_t)nl;
-  const int nch = (int)std::min<int64_t>(8, npix / kPipeChunk);
+  // two chunks or more, of at least four times kPipeChunk when there are
+  // more than two: the wave kernels prefer long launches
+  const int nch = (int)std::max<int64_t>(2, std::min<int64_t>(8, npix / (4 * kPipeChunk)));
   gm::DevCfg d1 = d;
   if (prepass) d1.init_mode = 1;
   const int64_t most = (npix + nch - 1) / nch;

@@ -1017,6 +1017,15 @@ template <int LPL, int V, bool accurate>
 __device__ __noinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, float flambda,
                                         float flambda2, int lane) {
   constexpr int NS = Variant<V>::SOLVES, G = 32 / NS;
+  // The plan's indices (all below 256) packed one byte each into three
+  // registers: read through the reference, every store to the shared-memory
+  // blocks might alias the plan and each step would reload it from local
+  // memory, and unpacked the eleven values spill (+3.6 % pixels/s packed).
+  const unsigned w0 = (unsigned)pl.src | (unsigned)pl.d00 << 8 | (unsigned)pl.d01 << 16 | (unsigned)pl.d10 << 24;
+  const unsigned w1 = (unsigned)pl.d11 | (unsigned)pl.vin << 8 | (unsigned)pl.vout0 << 16 | (unsigned)pl.vout1 << 24;
+  const unsigned w2 = (unsigned)pl.p | (unsigned)(pl.base + pl.p) << 8 | (unsigned)(pl.base + pl.q) << 16;
+  const unsigned initpack = pl.initpack;
+  auto at = [](unsigned w, int i) { return (int)((w >> (8 * i)) & 0xffu); };
   const int h = NS == 2 ? lane >> 4 : 0;
   const int g = lane & (G - 1);
   // damped matrix (diagonal x (1 + lambda), milosUtils.cu:648-652)
@@ -1025,7 +1034,7 @@ __device__ __noinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, 
   float* B = &sm.A[h][1][0][0];
 #pragma unroll
   for (int e = 0; e < 2 * NS; ++e) {
-    const unsigned b = (pl.initpack >> (8 * e)) & 0xffu;
+    const unsigned b = (initpack >> (8 * e)) & 0xffu;
     if (b != 0xffu) {
       const float a = sm.alpha[g + e * G];
       A[b & 0x7fu] = (b & 0x80u) ? (float)((double)a * damp) : a;
@@ -1041,9 +1050,9 @@ __device__ __noinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, 
   const bool diag = g < 5, active = g < 15;
 #pragma unroll 1
   for (int step = 0; step < 18; ++step) {
-    const float m00 = A[pl.src], m01 = A[pl.src + 1], m11 = A[pl.src + 12];
-    const float m10 = diag ? m01 : A[pl.src + 11];
-    const float b0 = va[pl.vin], b1 = va[pl.vin + 1];
+    const float m00 = A[at(w0, 0)], m01 = A[at(w0, 0) + 1], m11 = A[at(w0, 0) + 12];
+    const float m10 = diag ? m01 : A[at(w0, 0) + 11];
+    const float b0 = va[at(w1, 1)], b1 = va[at(w1, 1) + 1];
     float th;
     if (m00 == m11) {
       th = quarter;
@@ -1058,22 +1067,22 @@ __device__ __noinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, 
       sm.cs[h][step][g] = cs;
       sm.sn[h][step][g] = sn;
     }
-    const float cr = __shfl_sync(kFull, cs, pl.base + pl.p), sr = __shfl_sync(kFull, sn, pl.base + pl.p);
-    const float cc = __shfl_sync(kFull, cs, pl.base + pl.q), sc = __shfl_sync(kFull, sn, pl.base + pl.q);
+    const float cr = __shfl_sync(kFull, cs, at(w2, 1)), sr = __shfl_sync(kFull, sn, at(w2, 1));
+    const float cc = __shfl_sync(kFull, cs, at(w2, 2)), sc = __shfl_sync(kFull, sn, at(w2, 2));
     const float t0 = m00 * cr - m10 * sr, t1 = m00 * sr + m10 * cr;
     const float u0 = m01 * cr - m11 * sr, u1 = m01 * sr + m11 * cr;
     const float n00 = t0 * cc - u0 * sc, n11 = t1 * sc + u1 * cc;
     const float n01 = diag ? 0.f : t0 * sc + u0 * cc;
     const float n10 = diag ? 0.f : t1 * cc - u1 * sc;
     if (active) {
-      B[pl.d00] = n00;
-      B[pl.d01] = n01;
-      B[pl.d10] = n10;
-      B[pl.d11] = n11;
+      B[at(w0, 1)] = n00;
+      B[at(w0, 2)] = n01;
+      B[at(w0, 3)] = n10;
+      B[at(w1, 0)] = n11;
     }
     if (diag) {
-      vb[pl.vout0] = cs * b0 - sn * b1;
-      vb[pl.vout1] = sn * b0 + cs * b1;
+      vb[at(w1, 2)] = cs * b0 - sn * b1;
+      vb[at(w1, 3)] = sn * b0 + cs * b1;
     }
     __syncwarp();
     float* tA = A; A = B; B = tA;
@@ -1090,11 +1099,11 @@ __device__ __noinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, 
   // delta = V z: undo the steps in reverse order
 #pragma unroll 1
   for (int step = 17; step >= 0; --step) {
-    const float y0 = va[pl.vout0], y1 = va[pl.vout1];
-    const float cs = sm.cs[h][step][pl.p], sn = sm.sn[h][step][pl.p];
+    const float y0 = va[at(w1, 2)], y1 = va[at(w1, 3)];
+    const float cs = sm.cs[h][step][at(w2, 0)], sn = sm.sn[h][step][at(w2, 0)];
     if (diag) {
-      vb[pl.vin] = cs * y0 + sn * y1;
-      vb[pl.vin + 1] = -sn * y0 + cs * y1;
+      vb[at(w1, 1)] = cs * y0 + sn * y1;
+      vb[at(w1, 1) + 1] = -sn * y0 + cs * y1;
     }
     __syncwarp();
     float* tv = va; va = vb; vb = tv;

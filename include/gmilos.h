@@ -142,7 +142,20 @@ gm_status gm_configure(gm_ctx *ctx, const gm_config *cfg);
 /* ---------------- the two reference paths -------------------------------- */
 /* Invert P pixels (replaces lm_mils / lm_mils_11).  fitted (optional) receives
  * the last trial synthesis per pixel, as the reference's spectraAdjusted
- * (milosUtils.cu:658).  status (optional) receives GM_PIX_* bits. */
+ * (milosUtils.cu:658).  status (optional) receives GM_PIX_* bits.
+ *
+ * Kernels: the 10-term path without macroturbulence (the reference's default
+ * configuration) runs wave-synchronously -- per LM trial, one kernel for the
+ * trials of every pixel still iterating and one for the response functions and
+ * normal equations of the accepted ones, over chunks of up to 2^20 pixels
+ * whose LM state (about 3.6 KB per pixel at nl <= 32, 6.6 KB above) the
+ * context keeps in device memory within its HBM budget.  The other variants,
+ * and calls whose budget leaves room for fewer than 16384 pixels of state, run
+ * one fused persistent kernel.  Both execute the same LM arithmetic; compiled
+ * as different kernels they round differently at the float level, so their
+ * trajectories agree to rounding.  The environment variable
+ * GMILOS_INVERT_KERNEL=fused selects the fused kernel for every call (for
+ * comparisons). */
 gm_status gm_invert(gm_ctx *ctx, const float *iquv, int64_t npix, int nl,
                     float *model, float *chi2, int *iters, float *fitted,
                     uint32_t *status, void *stream);
@@ -154,8 +167,9 @@ gm_status gm_invert_ex(gm_ctx *ctx, const float *iquv, int64_t npix, int nl,
                        float *chi2, int *iters, int *accepted, float *fitted,
                        uint32_t *status, void *stream);
 
-/* Inversion for callers that cannot allocate device memory.  No counterpart
- * in the reference.  Some callers cannot call cudaMalloc while they run: code
+/* Inversion for callers that cannot allocate device memory (the fused kernel,
+ * its results those of gm_invert with GMILOS_INVERT_KERNEL=fused).  No
+ * counterpart in the reference.  Some callers cannot call cudaMalloc while they run: code
  * inside a CUDA-graph capture or a real-time pipeline that must not block on
  * the allocator, or a host framework that owns every device byte itself.
  * This entry point allocates nothing: it takes the configuration directly
@@ -212,7 +226,10 @@ gm_status gm_synthesize_grid(gm_ctx *ctx, const double *models, int64_t npix,
  * chunks of chunk_pixels; `streams` lanes each keep one chunk on the device,
  * taken round robin from the admitted requests, so requests that arrive
  * while others run start within one chunk time and their work overlaps on
- * the device.  Per-pixel results do not depend on the mix.  Requests share
+ * the device.  Each lane keeps one chunk of wave-kernel state and classical
+ * start models on the device (about 240 MB per lane at the default chunk and
+ * nl <= 32), so a served pixel runs the kernels of gm_invert and its result
+ * is the one gm_invert gives, whatever the mix.  Requests share
  * the configured stray-light profile and wavelength grid: a configuration
  * with per-pixel stray maps or per-pixel grids is refused with
  * GM_ERR_UNSUPPORTED.  No counterpart in the reference (its main inverts one
