@@ -249,25 +249,27 @@ constexpr int accept_min_blocks() { return LPL == 1 ? 5 : 5; }
 // The trial half touches the warp's shared memory only up to the first
 // 8-row tile of staged rows (the synthesis PSF stages rows 0-3), so its
 // warps are packed at that stride: half the footprint, more warps per SM.
-template <int LPL>
+template <int LPL, int V>
 __host__ __device__ constexpr size_t trial_warp_bytes() {
-  using WS = WarpSmem<LPL, 0>;
+  using WS = WarpSmem<LPL, V>;
   return (offsetof(WS, rows) + 8 * row_pitch<LPL>() * sizeof(float) + 15) & ~(size_t)15;
 }
-template <int LPL>
-__device__ __forceinline__ WarpSmem<LPL, 0>& trial_smem() {
-  return *reinterpret_cast<WarpSmem<LPL, 0>*>(gm_dyn_smem + tap_bytes<LPL>() +
-                                               (threadIdx.x >> 5) * trial_warp_bytes<LPL>());
+template <int LPL, int V>
+__device__ __forceinline__ WarpSmem<LPL, V>& trial_smem() {
+  return *reinterpret_cast<WarpSmem<LPL, V>*>(gm_dyn_smem + tap_bytes<LPL>() +
+                                               (threadIdx.x >> 5) * trial_warp_bytes<LPL, V>());
 }
 
 // Staged rows of an accepted trial (one float per lane each): per sample
-// slot k the 15 Lane terms, then syn and pure; the last row holds the angles.
-template <int LPL>
-__device__ __forceinline__ void stage_put(float* __restrict__ q, const Lane<LPL, 0>& ln, const Angles& an,
+// slot k the 15 Lane terms, syn and pure, and with macroturbulence the
+// profile before its convolution; the last row holds the angles.
+template <int LPL, int V>
+__device__ __forceinline__ void stage_put(float* __restrict__ q, const Lane<LPL, V>& ln, const Angles& an,
                                           const float (&syn)[LPL][4], const float (&pure)[LPL][4], int lane) {
+  constexpr int R = stage_rows_per_slot(Variant<V>::MAC);
 #pragma unroll
   for (int k = 0; k < LPL; ++k) {
-    float* r = q + k * 23 * 32 + lane;
+    float* r = q + k * R * 32 + lane;
 #pragma unroll
     for (int g = 0; g < 3; ++g) {
       r[(0 + g) * 32] = ln.fi[k][g];
@@ -280,21 +282,23 @@ __device__ __forceinline__ void stage_put(float* __restrict__ q, const Lane<LPL,
     for (int s = 0; s < 4; ++s) {
       r[(15 + s) * 32] = syn[k][s];
       r[(19 + s) * 32] = pure[k][s];
+      if constexpr (Variant<V>::MAC) r[(23 + s) * 32] = ln.mc[k][s];
     }
   }
   if (lane == 0) {
-    float* r = q + LPL * 23 * 32;
+    float* r = q + LPL * R * 32;
     r[0] = an.cosi; r[1] = an.sinis; r[2] = an.sina; r[3] = an.cosa; r[4] = an.sinda;
     r[5] = an.cosda; r[6] = an.sindi; r[7] = an.cosdi; r[8] = an.cosis_2;
   }
 }
 
-template <int LPL>
-__device__ __forceinline__ void stage_get(const float* __restrict__ q, Lane<LPL, 0>& ln, Angles& an,
+template <int LPL, int V>
+__device__ __forceinline__ void stage_get(const float* __restrict__ q, Lane<LPL, V>& ln, Angles& an,
                                           float (&syn)[LPL][4], float (&pure)[LPL][4], int lane) {
+  constexpr int R = stage_rows_per_slot(Variant<V>::MAC);
 #pragma unroll
   for (int k = 0; k < LPL; ++k) {
-    const float* r = q + k * 23 * 32 + lane;
+    const float* r = q + k * R * 32 + lane;
 #pragma unroll
     for (int g = 0; g < 3; ++g) {
       ln.fi[k][g] = r[(0 + g) * 32];
@@ -307,9 +311,10 @@ __device__ __forceinline__ void stage_get(const float* __restrict__ q, Lane<LPL,
     for (int s = 0; s < 4; ++s) {
       syn[k][s] = r[(15 + s) * 32];
       pure[k][s] = r[(19 + s) * 32];
+      if constexpr (Variant<V>::MAC) ln.mc[k][s] = r[(23 + s) * 32];
     }
   }
-  const float* r = q + LPL * 23 * 32;
+  const float* r = q + LPL * R * 32;
   an.cosi = r[0]; an.sinis = r[1]; an.sina = r[2]; an.cosa = r[3]; an.sinda = r[4];
   an.cosda = r[5]; an.sindi = r[6]; an.cosdi = r[7]; an.cosis_2 = r[8];
 }
@@ -344,12 +349,14 @@ __device__ __forceinline__ void finish_pixel(const InvertArgs& a, const double* 
 // One trial of every pixel in the wave's active list (wave 0: the start
 // models, every pixel of the chunk).  The body is invert_kernel's loop
 // body from the solve to the damping schedule (milosUtils.cu:630-700).
-template <int LPL>
+template <int LPL, int V>
 __global__ void __launch_bounds__(warps_per_block<LPL>() * 32, trial_min_blocks<LPL>())
 trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
+  static_assert(V == 0 || V == 1, "the 10-term variants");
+  constexpr int NS = Variant<V>::SOLVES;
   const int lane = threadIdx.x & 31;
   load_taps<LPL>(c);
-  WarpSmem<LPL, 0>& sm = trial_smem<LPL>();
+  WarpSmem<LPL, V>& sm = trial_smem<LPL, V>();
   for (int i = lane; i < 8 * row_pitch<LPL>(); i += 32) (&sm.rows[0][0])[i] = 0.f;
   __syncwarp();
   const int nl = c.nl;
@@ -371,7 +378,7 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
 #pragma unroll
       for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
   }
-  const SolvePlan plan = make_solve_plan<2>(lane);
+  const SolvePlan plan = make_solve_plan<NS>(lane);
   const uint32_t n = wave == 0 ? (uint32_t)a.npix : w.cnt[wave - 1].n_next;
   const uint32_t* in = (wave & 1) ? w.act1 : w.act0;
   uint32_t* next = (wave & 1) ? w.act0 : w.act1;
@@ -402,7 +409,7 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
       iter = acc = 0;
       __syncwarp();
     } else {
-      const bool reuse = P.flags & 1u;
+      const bool reuse = NS == 2 && (P.flags & 1u);
       if (lane < 11) {
         sm.m[lane] = P.m[lane];
         sm.t[lane] = P.t[lane];
@@ -422,17 +429,17 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
       }
       __syncwarp();
       if (!reuse) {
-        if (c.numerics) solve10<LPL, 0, true>(sm, plan, flambda, flambda * 10.f * pbf, lane);
-        else solve10<LPL, 0, false>(sm, plan, flambda, flambda * 10.f * pbf, lane);
+        if (c.numerics) solve10<LPL, V, true>(sm, plan, flambda, flambda * 10.f * pbf, lane);
+        else solve10<LPL, V, false>(sm, plan, flambda, flambda * 10.f * pbf, lane);
       }
       solved = !reuse;
       if (lane == 0) apply_delta_check<10>(c, sm.m, sm.vec[reuse ? 1 : 0][0], sm.t);
       __syncwarp();
     }
-    Lane<LPL, 0> ln;
+    Lane<LPL, V> ln;
     Angles an;
     float syn[LPL][4], pure[LPL][4];
-    synth_lane<LPL, 0>(c, wave == 0 ? sm.m : sm.t, dlv, lane, ln, an, syn, pure, slg, sm, lamp);
+    synth_lane<LPL, V>(c, wave == 0 ? sm.m : sm.t, dlv, lane, ln, an, syn, pure, slg, sm, lamp);
     const float chisqr = chisq<LPL>(c, syn, ob, valid);
     bool accept = true, stop = false, have_next = false;
     if (wave == 0) {
@@ -459,7 +466,7 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
         st |= GM_PIX_LAMBDA_EXIT;
       }
       ++iter;
-      have_next = !accept && solved;
+      have_next = NS == 2 && !accept && solved;
       if (c.logclambda) pbf = log10f(chisqr) / log10f(chisqr0);
       if (accept) ochisqr = chisqr;
     }
@@ -475,7 +482,7 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
         P.m[lane] = sm.m[lane];
         P.t[lane] = sm.t[lane];
       }
-      if (solved && lane < 10) P.vnext[lane] = sm.vec[1][0][lane];
+      if (NS == 2 && solved && lane < 10) P.vnext[lane] = sm.vec[NS - 1][0][lane];
       uint32_t slot = 0, aslot = 0;
       if (lane == 0) {
         P.flambda = flambda;
@@ -493,7 +500,7 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
       aslot = __shfl_sync(kFull, aslot, 0);
       if (lane == 0) next[slot] = pix;
       if (accept) {
-        stage_put<LPL>(w.stage + (size_t)pix * stage_floats<LPL>(), ln, an, syn, pure, lane);
+        stage_put<LPL, V>(w.stage + (size_t)pix * stage_floats<LPL>(), ln, an, syn, pure, lane);
         if (lane == 0) w.accl[aslot] = pix;
       }
     }
@@ -507,13 +514,13 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
 
 // Response functions and normal equations of every pixel whose trial of
 // this wave was accepted (the accept branch of invert_kernel's loop).
-template <int LPL>
+template <int LPL, int V>
 __global__ void __launch_bounds__(warps_per_block<LPL>() * 32, accept_min_blocks<LPL>())
 accept_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
   const int lane = threadIdx.x & 31;
   load_taps<LPL>(c);
-  WarpSmem<LPL, 0>& sm = warp_smem<LPL, 0>();
-  init_rows<LPL, 0>(c, sm, lane);
+  WarpSmem<LPL, V>& sm = warp_smem<LPL, V>();
+  init_rows<LPL, V>(c, sm, lane);
   const int nl = c.nl;
   float dlv[LPL];
   double dld[LPL];
@@ -547,13 +554,13 @@ accept_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
     if (c.use_slight && c.slight_per_pixel) load_pixel<LPL>(c.slight + off, nl, lane, slg);
     const double* lamp = pixel_grid<LPL>(c, pix, lane, dlv, dld);
     if (lane < 11) sm.m[lane] = P.m[lane];
-    Lane<LPL, 0> ln;
+    Lane<LPL, V> ln;
     Angles an;
     float syn[LPL][4], pure[LPL][4];
-    stage_get<LPL>(w.stage + (size_t)pix * stage_floats<LPL>(), ln, an, syn, pure, lane);
+    stage_get<LPL, V>(w.stage + (size_t)pix * stage_floats<LPL>(), ln, an, syn, pure, lane);
     __syncwarp();
-    rf_rows<LPL, 0>(c, sm.m, ln, an, lane, sm, lamp);
-    normal_eq<LPL, 0>(c, sm.m, alpha_mixed, pure, slg, syn, ob, valid, lane, sm);
+    rf_rows<LPL, V>(c, sm.m, ln, an, lane, sm, lamp);
+    normal_eq<LPL, V>(c, sm.m, alpha_mixed, pure, slg, syn, ob, valid, lane, sm);
     for (int i = lane; i < 55; i += 32) P.alpha[i] = sm.alpha[i];
     if (lane < 10) P.beta[lane] = sm.beta[lane];
     __syncwarp();
@@ -860,25 +867,26 @@ WaveBuffers wave_buffers(void* base, int nl, int miter, int64_t chunk) {
 }
 
 bool waves_cover(const DevCfg& cfg, const InvertArgs& a) {
-  return kernel_variant(cfg, a.init_models != nullptr && !a.init_status) == 0 && cfg.init_mode != 0 &&
+  return kernel_variant(cfg, a.init_models != nullptr && !a.init_status) <= 1 && cfg.init_mode != 0 &&
          !a.step_delta && !a.step_trial && !a.step_chi2_start && !a.step_chi2_trial;
 }
 
-template <int LPL>
+template <int LPL, int V>
 cudaError_t launch_waves_t(const DevCfg& cfg, const InvertArgs& a, const WaveBuffers& b, cudaStream_t s,
                            int* launches) {
-  const size_t smem = smem_bytes<LPL, 0>();
-  const size_t tsmem = tap_bytes<LPL>() + trial_warp_bytes<LPL>() * warps_per_block<LPL>();
-  cudaError_t e = cudaFuncSetAttribute(trial_kernel<LPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
+  const size_t smem = smem_bytes<LPL, V>();
+  const size_t tsmem = tap_bytes<LPL>() + trial_warp_bytes<LPL, V>() * warps_per_block<LPL>();
+  cudaError_t e =
+      cudaFuncSetAttribute(trial_kernel<LPL, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(accept_kernel<LPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(accept_kernel<LPL, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int threads = warps_per_block<LPL>() * 32;
   int dev = 0, sms = 0, bt = 0, ba = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, trial_kernel<LPL>, threads, tsmem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ba, accept_kernel<LPL>, threads, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, trial_kernel<LPL, V>, threads, tsmem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ba, accept_kernel<LPL, V>, threads, smem);
   if (bt < 1 || ba < 1) return cudaErrorInvalidConfiguration;
   const int waves = 1 + (cfg.miter > 1 ? cfg.miter : 1);
   int count = 0;
@@ -892,11 +900,11 @@ cudaError_t launch_waves_t(const DevCfg& cfg, const InvertArgs& a, const WaveBuf
     e = cudaMemsetAsync(b.w.cnt, 0, sizeof(WaveCounters) * (size_t)waves, s);
     if (e != cudaSuccess) return e;
     for (int wv = 0; wv < waves; ++wv) {
-      trial_kernel<LPL><<<gt, threads, tsmem, s>>>(dc, c, b.w, wv);
+      trial_kernel<LPL, V><<<gt, threads, tsmem, s>>>(dc, c, b.w, wv);
       ++count;
       // the last wave's pixels all stop: nothing to accept
       if (wv + 1 < waves) {
-        accept_kernel<LPL><<<ga, threads, smem, s>>>(dc, c, b.w, wv);
+        accept_kernel<LPL, V><<<ga, threads, smem, s>>>(dc, c, b.w, wv);
         ++count;
       }
     }
@@ -910,7 +918,10 @@ cudaError_t launch_waves_t(const DevCfg& cfg, const InvertArgs& a, const WaveBuf
 cudaError_t launch_invert_waves(const DevCfg& cfg, const InvertArgs& a, const WaveBuffers& b, cudaStream_t s,
                                 int* launches) {
   if (!waves_cover(cfg, a) || b.chunk < 1 || b.chunk > 0x7fffffff) return cudaErrorInvalidValue;
-  return cfg.nl <= 32 ? launch_waves_t<1>(cfg, a, b, s, launches) : launch_waves_t<2>(cfg, a, b, s, launches);
+  const int v = kernel_variant(cfg, a.init_models != nullptr && !a.init_status);
+  if (cfg.nl <= 32)
+    return v == 0 ? launch_waves_t<1, 0>(cfg, a, b, s, launches) : launch_waves_t<1, 1>(cfg, a, b, s, launches);
+  return v == 0 ? launch_waves_t<2, 0>(cfg, a, b, s, launches) : launch_waves_t<2, 1>(cfg, a, b, s, launches);
 }
 
 template <int LPL, int V>

@@ -59,8 +59,10 @@ struct WaveCounters {
 };
 
 // Floats of one pixel's staged trial (accepted trial -> accept kernel): 23
-// rows of 32 lanes per sample slot and a row of angles.
-__host__ __device__ constexpr int stage_floats_for(int lpl) { return (23 * lpl + 1) * 32; }
+// rows of 32 lanes per sample slot (27 with macroturbulence) and a row of
+// angles; every variant's block is sized for the larger.
+__host__ __device__ constexpr int stage_rows_per_slot(bool mac) { return mac ? 27 : 23; }
+__host__ __device__ constexpr int stage_floats_for(int lpl) { return (stage_rows_per_slot(true) * lpl + 1) * 32; }
 template <int LPL>
 __host__ __device__ constexpr int stage_floats() { return stage_floats_for(LPL); }
 
@@ -80,8 +82,8 @@ struct WaveBuffers {
 };
 size_t wave_buffer_bytes(int nl, int miter, int64_t chunk);
 WaveBuffers wave_buffers(void* base, int nl, int miter, int64_t chunk);
-// Whether the wave path covers a launch: the 10-term path without
-// macroturbulence, start models given or configured (no in-kernel
+// Whether the wave path covers a launch: the 10-term paths (with or without
+// macroturbulence), start models given or configured (no in-kernel
 // classical estimates), no first-step outputs.
 bool waves_cover(const DevCfg& cfg, const InvertArgs& a);
 

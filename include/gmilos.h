@@ -144,14 +144,14 @@ gm_status gm_configure(gm_ctx *ctx, const gm_config *cfg);
  * the last trial synthesis per pixel, as the reference's spectraAdjusted
  * (milosUtils.cu:658).  status (optional) receives GM_PIX_* bits.
  *
- * Kernels: the 10-term path without macroturbulence (the reference's default
- * configuration) runs wave-synchronously -- per LM trial, one kernel for the
+ * Kernels: the 10-term paths (with or without macroturbulence; the
+ * reference's lm_mils) run wave-synchronously -- per LM trial, one kernel for the
  * trials of every pixel still iterating and one for the response functions and
  * normal equations of the accepted ones, over chunks of up to 2^20 pixels
- * whose LM state (about 3.6 KB per pixel at nl <= 32, 6.6 KB above) the
- * context keeps in device memory within its HBM budget.  The other variants,
- * and calls whose budget leaves room for fewer than 16384 pixels of state, run
- * one fused persistent kernel.  Both execute the same LM arithmetic; compiled
+ * whose LM state (about 4 KB per pixel at nl <= 32, 7.4 KB above) the
+ * context keeps in device memory within its HBM budget.  The 11-term path
+ * (lm_mils_11), first-step outputs (gm_lm_step) and calls whose budget leaves
+ * room for fewer than 16384 pixels of state run one fused persistent kernel.  Both execute the same LM arithmetic; compiled
  * as different kernels they round differently at the float level, so their
  * trajectories agree to rounding.  The environment variable
  * GMILOS_INVERT_KERNEL=fused selects the fused kernel for every call (for
@@ -227,7 +227,7 @@ gm_status gm_synthesize_grid(gm_ctx *ctx, const double *models, int64_t npix,
  * taken round robin from the admitted requests, so requests that arrive
  * while others run start within one chunk time and their work overlaps on
  * the device.  Each lane keeps one chunk of wave-kernel state and classical
- * start models on the device (about 240 MB per lane at the default chunk and
+ * start models on the device (about 270 MB per lane at the default chunk and
  * nl <= 32), so a served pixel runs the kernels of gm_invert and its result
  * is the one gm_invert gives, whatever the mix.  Requests share
  * the configured stray-light profile and wavelength grid: a configuration
