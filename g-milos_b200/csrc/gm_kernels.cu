@@ -241,10 +241,12 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
 // accept kernel through a staging row block, so nothing is recomputed and
 // every pixel performs exactly invert_kernel's arithmetic.
 
-template <int LPL>
-constexpr int trial_min_blocks() { return LPL == 1 ? 7 : 8; }
-template <int LPL>
-constexpr int accept_min_blocks() { return LPL == 1 ? 5 : 5; }
+// Resident blocks per SM: registers for the 10-term variants; the 11-term
+// variant's FP64 Jacobi matrices make shared memory the limit.
+template <int LPL, int V>
+constexpr int trial_min_blocks() { return V == 2 ? (LPL == 1 ? 5 : 8) : (LPL == 1 ? 7 : 8); }
+template <int LPL, int V>
+constexpr int accept_min_blocks() { return V == 2 ? (LPL == 1 ? 3 : 4) : 5; }
 
 // The trial half touches the warp's shared memory only up to the first
 // 8-row tile of staged rows (the synthesis PSF stages rows 0-3), so its
@@ -350,10 +352,9 @@ __device__ __forceinline__ void finish_pixel(const InvertArgs& a, const double* 
 // models, every pixel of the chunk).  The body is invert_kernel's loop
 // body from the solve to the damping schedule (milosUtils.cu:630-700).
 template <int LPL, int V>
-__global__ void __launch_bounds__(warps_per_block<LPL>() * 32, trial_min_blocks<LPL>())
+__global__ void __launch_bounds__(warps_per_block<LPL>() * 32, trial_min_blocks<LPL, V>())
 trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
-  static_assert(V == 0 || V == 1, "the 10-term variants");
-  constexpr int NS = Variant<V>::SOLVES;
+  constexpr int NS = Variant<V>::SOLVES, NT = Variant<V>::NT, NA = NT * (NT + 1) / 2;
   const int lane = threadIdx.x & 31;
   load_taps<LPL>(c);
   WarpSmem<LPL, V>& sm = trial_smem<LPL, V>();
@@ -379,6 +380,8 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
       for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
   }
   const SolvePlan plan = make_solve_plan<NS>(lane);
+  Solve11Plan plan11;
+  if constexpr (NT == 11) plan11 = make_solve11_plan(lane);
   const uint32_t n = wave == 0 ? (uint32_t)a.npix : w.cnt[wave - 1].n_next;
   const uint32_t* in = (wave & 1) ? w.act1 : w.act0;
   uint32_t* next = (wave & 1) ? w.act0 : w.act1;
@@ -424,16 +427,21 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
       if (reuse) {
         if (lane < 10) sm.vec[1][0][lane] = P.vnext[lane];
       } else {
-        for (int i = lane; i < 55; i += 32) sm.alpha[i] = P.alpha[i];
-        if (lane < 10) sm.beta[lane] = P.beta[lane];
+        for (int i = lane; i < NA; i += 32) sm.alpha[i] = P.alpha[i];
+        if (lane < NT) sm.beta[lane] = P.beta[lane];
       }
       __syncwarp();
-      if (!reuse) {
-        if (c.numerics) solve10<LPL, V, true>(sm, plan, flambda, flambda * 10.f * pbf, lane);
-        else solve10<LPL, V, false>(sm, plan, flambda, flambda * 10.f * pbf, lane);
+      if constexpr (NT == 11) {
+        solve11<LPL, V>(sm, plan11, flambda, lane);
+        if (lane == 0) apply_delta_check<11>(c, sm.m, sm.dd, sm.t);
+      } else {
+        if (!reuse) {
+          if (c.numerics) solve10<LPL, V, true>(sm, plan, flambda, flambda * 10.f * pbf, lane);
+          else solve10<LPL, V, false>(sm, plan, flambda, flambda * 10.f * pbf, lane);
+        }
+        if (lane == 0) apply_delta_check<10>(c, sm.m, sm.vec[reuse ? 1 : 0][0], sm.t);
       }
       solved = !reuse;
-      if (lane == 0) apply_delta_check<10>(c, sm.m, sm.vec[reuse ? 1 : 0][0], sm.t);
       __syncwarp();
     }
     Lane<LPL, V> ln;
@@ -515,7 +523,7 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
 // Response functions and normal equations of every pixel whose trial of
 // this wave was accepted (the accept branch of invert_kernel's loop).
 template <int LPL, int V>
-__global__ void __launch_bounds__(warps_per_block<LPL>() * 32, accept_min_blocks<LPL>())
+__global__ void __launch_bounds__(warps_per_block<LPL>() * 32, accept_min_blocks<LPL, V>())
 accept_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
   const int lane = threadIdx.x & 31;
   load_taps<LPL>(c);
@@ -561,8 +569,9 @@ accept_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
     __syncwarp();
     rf_rows<LPL, V>(c, sm.m, ln, an, lane, sm, lamp);
     normal_eq<LPL, V>(c, sm.m, alpha_mixed, pure, slg, syn, ob, valid, lane, sm);
-    for (int i = lane; i < 55; i += 32) P.alpha[i] = sm.alpha[i];
-    if (lane < 10) P.beta[lane] = sm.beta[lane];
+    constexpr int NT = Variant<V>::NT;
+    for (int i = lane; i < NT * (NT + 1) / 2; i += 32) P.alpha[i] = sm.alpha[i];
+    if (lane < NT) P.beta[lane] = sm.beta[lane];
     __syncwarp();
   }
 }
@@ -867,8 +876,7 @@ WaveBuffers wave_buffers(void* base, int nl, int miter, int64_t chunk) {
 }
 
 bool waves_cover(const DevCfg& cfg, const InvertArgs& a) {
-  return kernel_variant(cfg, a.init_models != nullptr && !a.init_status) <= 1 && cfg.init_mode != 0 &&
-         !a.step_delta && !a.step_trial && !a.step_chi2_start && !a.step_chi2_trial;
+  return cfg.init_mode != 0 && !a.step_delta && !a.step_trial && !a.step_chi2_start && !a.step_chi2_trial;
 }
 
 template <int LPL, int V>
@@ -919,9 +927,14 @@ cudaError_t launch_invert_waves(const DevCfg& cfg, const InvertArgs& a, const Wa
                                 int* launches) {
   if (!waves_cover(cfg, a) || b.chunk < 1 || b.chunk > 0x7fffffff) return cudaErrorInvalidValue;
   const int v = kernel_variant(cfg, a.init_models != nullptr && !a.init_status);
-  if (cfg.nl <= 32)
-    return v == 0 ? launch_waves_t<1, 0>(cfg, a, b, s, launches) : launch_waves_t<1, 1>(cfg, a, b, s, launches);
-  return v == 0 ? launch_waves_t<2, 0>(cfg, a, b, s, launches) : launch_waves_t<2, 1>(cfg, a, b, s, launches);
+  if (cfg.nl <= 32) {
+    if (v == 0) return launch_waves_t<1, 0>(cfg, a, b, s, launches);
+    if (v == 1) return launch_waves_t<1, 1>(cfg, a, b, s, launches);
+    return launch_waves_t<1, 2>(cfg, a, b, s, launches);
+  }
+  if (v == 0) return launch_waves_t<2, 0>(cfg, a, b, s, launches);
+  if (v == 1) return launch_waves_t<2, 1>(cfg, a, b, s, launches);
+  return launch_waves_t<2, 2>(cfg, a, b, s, launches);
 }
 
 template <int LPL, int V>

@@ -44,13 +44,13 @@ struct InvertArgs {
 // pixel between the trial and the accept kernel of a wave.
 struct PixLM {
   double m[11], t[11];         // accepted and trial models
-  float alpha[56], beta[10];   // normal equations of the accepted model (packed alpha)
-  float vnext[10];             // step for the damping a rejection moves to
+  float alpha[68], beta[12];   // normal equations of the accepted model (packed alpha, 55 or 66)
+  float vnext[12];             // step for the damping a rejection moves to (10 terms)
   float flambda, pbf, ochisqr, chisqr0;
   int iter, acc;
   uint32_t st, flags;          // status bits; flags bit 0: vnext holds the next step
 };
-static_assert(sizeof(PixLM) == 512, "PixLM is one 512-byte record");
+static_assert(sizeof(PixLM) == 576, "PixLM is one 576-byte record");
 
 // Per wave: the trial kernel's cursor, the pixels it passes to the next wave
 // and to the accept kernel, and the accept kernel's cursor.
@@ -82,9 +82,9 @@ struct WaveBuffers {
 };
 size_t wave_buffer_bytes(int nl, int miter, int64_t chunk);
 WaveBuffers wave_buffers(void* base, int nl, int miter, int64_t chunk);
-// Whether the wave path covers a launch: the 10-term paths (with or without
-// macroturbulence), start models given or configured (no in-kernel
-// classical estimates), no first-step outputs.
+// Whether the wave path covers a launch: every variant, with start models
+// given or configured (no in-kernel classical estimates) and no first-step
+// outputs.
 bool waves_cover(const DevCfg& cfg, const InvertArgs& a);
 
 // Arguments of the pixels [first, first + n) of a launch.

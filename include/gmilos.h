@@ -144,14 +144,14 @@ gm_status gm_configure(gm_ctx *ctx, const gm_config *cfg);
  * the last trial synthesis per pixel, as the reference's spectraAdjusted
  * (milosUtils.cu:658).  status (optional) receives GM_PIX_* bits.
  *
- * Kernels: the 10-term paths (with or without macroturbulence; the
- * reference's lm_mils) run wave-synchronously -- per LM trial, one kernel for the
+ * Kernels: inversions run wave-synchronously -- per LM trial, one kernel for the
  * trials of every pixel still iterating and one for the response functions and
  * normal equations of the accepted ones, over chunks of up to 2^20 pixels
  * whose LM state (about 4 KB per pixel at nl <= 32, 7.4 KB above) the
- * context keeps in device memory within its HBM budget.  The 11-term path
- * (lm_mils_11), first-step outputs (gm_lm_step) and calls whose budget leaves
- * room for fewer than 16384 pixels of state run one fused persistent kernel.  Both execute the same LM arithmetic; compiled
+ * context keeps in device memory within its HBM budget.  First-step outputs
+ * (gm_lm_step), in-kernel classical estimates (gm_invert_noalloc) and calls
+ * whose budget leaves room for fewer than 16384 pixels of state run one fused
+ * persistent kernel.  Both execute the same LM arithmetic; compiled
  * as different kernels they round differently at the float level, so their
  * trajectories agree to rounding.  The environment variable
  * GMILOS_INVERT_KERNEL=fused selects the fused kernel for every call (for

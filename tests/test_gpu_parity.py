@@ -214,6 +214,26 @@ def test_wave_and_fused_kernels_agree(engine, monkeypatch, nl):
     assert np.median(w["chi2"]) == pytest.approx(np.median(f["chi2"]), rel=1e-2)
 
 
+def test_wave_state_within_the_hbm_budget():
+    """The wave kernels keep about 4 KB of LM state per pixel of a chunk in
+    the context's budget; a budget with room for fewer than 16 384 pixels
+    of it runs the fused kernel instead (pre-pass + one launch), and both
+    give equally good fits."""
+    rng = np.random.default_rng(740)
+    ocfg, gcfg, _ = configs(psf=True)
+    obs = H.observations(ocfg, H.truth_models(20000, rng), rng)
+    res = {}
+    for budget in (60 << 20, 300 << 20):
+        with G.Engine(0, hbm_budget=budget) as e:
+            e.configure(gcfg)
+            out = e.invert(obs)
+            res[budget] = (out, e.stats()["kernel_launches"])
+    (f, lf), (w, lw) = res[60 << 20], res[300 << 20]
+    assert lf == 2 and lw == 2 * 51
+    assert np.median(w["chi2"]) == pytest.approx(np.median(f["chi2"]), rel=1e-2)
+    assert abs(w["iters"].mean() - f["iters"].mean()) < 0.5
+
+
 def test_inversion_edge_cases(engine):
     rng = np.random.default_rng(500)
     ocfg, gcfg, _ = configs(numerics=1)
