@@ -45,7 +45,7 @@ MAXITER = 50
 # and every trial / accept wave), measured with ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum summed over the launches) on a 65 536-pixel inversion
 # of this workload; traffic grows with the pixel count.
-DRAM_BYTES_PER_PIXEL = 585.0
+DRAM_BYTES_PER_PIXEL = 222113.0
 
 # Algorithmic FLOPs per pixel (per-wavelength costs counted from the formulas)
 C_VOIGT, C_RTE, C_DVOIGT, C_DRTE = 100, 85, 23, 870
