@@ -84,6 +84,11 @@ struct gm_ctx {
   cudaStream_t aux = nullptr;
   cudaEvent_t evx0 = nullptr, evx1 = nullptr;
   gm::WorkCounters* work2 = nullptr;
+  // the device scratch (work counters, pre-pass output, wave state) is
+  // reused by every inversion: the next one, on whatever stream, waits for
+  // the last one's work
+  cudaEvent_t ev_scratch = nullptr;
+  bool scratch_pending = false;
   DevBuf slight;                      // global stray-light profile (device copy)
   std::map<std::string, DevBuf> bufs; // staging buffers for host-memory calls
   std::string err;
@@ -320,6 +325,7 @@ gm_status gm_create(int device, size_t hbm_budget, gm_ctx** out) {
   if (cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking) != cudaSuccess) return GM_ERR_CUDA;
   cudaEventCreateWithFlags(&ctx->evx0, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&ctx->evx1, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&ctx->ev_scratch, cudaEventDisableTiming);
   *out = ctx.release();
   return GM_OK;
 }
@@ -344,6 +350,7 @@ gm_status gm_destroy(gm_ctx* ctx) {
   cudaEventDestroy(ctx->ev1);
   if (ctx->evx0) cudaEventDestroy(ctx->evx0);
   if (ctx->evx1) cudaEventDestroy(ctx->evx1);
+  if (ctx->ev_scratch) cudaEventDestroy(ctx->ev_scratch);
   if (ctx->aux) cudaStreamDestroy(ctx->aux);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -520,6 +527,7 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   if (npix == 0) return GM_OK;
   cudaSetDevice(ctx->device);
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  if (ctx->scratch_pending) cudaStreamWaitEvent(s, ctx->ev_scratch, 0);
   const size_t cube = sizeof(float) * 4 * (size_t)nl * npix;
   // classical estimates of the start models in a pre-pass kernel, so that
   // their code stays out of the inversion kernel's instruction stream
@@ -625,6 +633,8 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
     any_host |= (o->host != nullptr);
   }
   any_host |= (a_in.dev != (void*)iquv);
+  cudaEventRecord(ctx->ev_scratch, s);
+  ctx->scratch_pending = true;
   if (any_host || !stream) {
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "inversion");

@@ -19,7 +19,9 @@
  *    calls on device buffers are stream-ordered and return after launch;
  *  - one context per host thread, or serialise calls on a shared context
  *    (the serving entry points gm_submit / gm_poll / gm_cancel are
- *    internally locked and may be called from any thread).
+ *    internally locked and may be called from any thread); inversions of a
+ *    context on different streams run one after another on the device, as
+ *    they share its scratch.
  *
  * Layouts (all float32 unless stated; pixel-major like the reference's
  * spectroImagen, gmilos.cu:1200):

@@ -234,6 +234,32 @@ def test_wave_state_within_the_hbm_budget():
     assert abs(w["iters"].mean() - f["iters"].mean()) < 0.5
 
 
+def test_calls_on_two_streams_take_the_scratch_in_turn(engine):
+    """Device-buffer calls return at launch; two calls on different streams
+    share the context's scratch (counters, wave state), so the second waits
+    for the first on the device: both results equal the calls run alone."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(750)
+    ocfg, gcfg, _ = configs(psf=True)
+    engine.configure(gcfg)
+    cubes = [torch.from_numpy(H.observations(ocfg, H.truth_models(20000, rng), rng)).cuda() for _ in range(2)]
+    alone = [engine.invert(c) for c in cubes]
+    torch.cuda.synchronize()
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    outs = []
+    for c, st in zip(cubes, streams):
+        o = {"model": torch.empty((len(c), 11), dtype=torch.float32, device="cuda"), "model64": None,
+             "chi2": torch.empty(len(c), dtype=torch.float32, device="cuda"),
+             "iters": torch.empty(len(c), dtype=torch.int32, device="cuda"),
+             "accepted": None, "status": None, "fitted": None}
+        engine.invert(c, out=o, stream=st.cuda_stream)
+        outs.append(o)
+    torch.cuda.synchronize()
+    for o, a in zip(outs, alone):
+        for k in ("model", "chi2", "iters"):
+            np.testing.assert_array_equal(o[k].cpu().numpy(), a[k].cpu().numpy(), err_msg=k)
+
+
 def test_inversion_edge_cases(engine):
     rng = np.random.default_rng(500)
     ocfg, gcfg, _ = configs(numerics=1)
