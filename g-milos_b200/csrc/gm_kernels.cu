@@ -226,20 +226,22 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
 }
 
 // ------------------------------------------------- wave-synchronous inversion
-// The same LM iteration as invert_kernel, split at its two halves and run
-// for every pixel of a chunk in lockstep waves (10-term path without
-// macroturbulence, the reference's default configuration).  Wave w launches
-// trial_kernel over the pixels still iterating -- the step solve (both
-// dampings), the step limits, the trial synthesis with PSF and stray light,
-// chi2 and the damping schedule -- then accept_kernel over the pixels whose
-// trial was accepted: response functions, their PSF and the normal
-// equations.  Each kernel executes about a third of invert_kernel's code,
-// so the warps of an SM share one hot instruction working set, and each has
-// its own register budget (the trial half runs 20 warps per SM).  A pixel's
+// The same LM iteration as invert_kernel (lm_mils, milosUtils.cu:574-710,
+// and lm_mils_11, :713-850), split at its two halves and run for every pixel
+// of a chunk in lockstep waves.  Wave w launches trial_kernel over the
+// pixels still iterating -- the step solve, the step limits, the trial
+// synthesis with PSF and stray light, chi2 and the damping schedule -- then
+// accept_kernel over the pixels whose trial was accepted: response
+// functions, their PSF and the normal equations.  Each kernel executes
+// about a third of invert_kernel's code, so the warps of an SM share one hot
+// instruction working set, and each has its own register budget (at nl <=
+// 32 the trial half runs 28 warps per SM, the accept half 20).  A pixel's
 // LM state lives in a PixLM record between the kernels; the per-lane Voigt
 // and Zeeman terms, angles and profiles of an accepted trial reach the
-// accept kernel through a staging row block, so nothing is recomputed and
-// every pixel performs exactly invert_kernel's arithmetic.
+// accept kernel through a staging row block, so nothing is recomputed: each
+// pixel runs invert_kernel's operations in its order (compiled as other
+// kernels, the multiply-adds the compiler fuses differ, so results agree
+// with invert_kernel's to rounding, not bit for bit).
 
 // Resident blocks per SM: registers for the 10-term variants; the 11-term
 // variant's FP64 Jacobi matrices make shared memory the limit.
