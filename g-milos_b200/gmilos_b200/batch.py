@@ -1,9 +1,9 @@
 """Ragged batches: regions of interest of any size and wavelength grid.
 
-Pixels are independent, so a batch of ROIs inverts as one launch per
+Pixels are independent, so a batch of ROIs inverts as one engine call per
 distinct wavelength grid over the concatenated pixels of the ROIs on that
-grid: the persistent kernel's work-stealing cursor takes pixels of all of
-them alike, so ROI sizes do not matter.  The reference inverts one cube per
+grid: the kernels' work-stealing cursors take pixels of all of them alike,
+so ROI sizes do not matter.  The reference inverts one cube per
 run (gmilos.cu:1008-1249); this is the host-side loop a caller of it would
 write, done once.
 """
@@ -18,7 +18,8 @@ def invert_rois(engine, rois, config_for_grid, fitted=False):
     """Invert a ragged batch.  rois: list of (iquv [P_i][4][nl_i] float32,
     lambda [nl_i] absolute wavelengths); config_for_grid(lam) returns the
     engine configuration (make_config) for one grid.  Returns one output
-    dict per ROI (engine.invert's keys) and a summary: launches, pixels and
+    dict per ROI (engine.invert's keys) and a summary: engine calls
+    ("launches", one per grid), pixels and
     the lane occupancy (wavelength samples over lane slots, 32 per lane row
     of up to 32 samples, 64 above)."""
     groups = {}
