@@ -837,6 +837,11 @@ gm_status gm_measure_peaks(gm_ctx* ctx, double* fp32_tflops, double* fp64_tflops
   return GM_OK;
 }
 
+size_t gm_wave_state_bytes(int nl, int miter, int64_t pixels) {
+  if (nl < 1 || nl > GM_MAX_NL || pixels < 0) return 0;
+  return gm::wave_buffer_bytes(nl, miter, pixels);
+}
+
 gm_status gm_measure_sfu_peak(gm_ctx* ctx, double* gops) {
   if (!ctx || !gops) return GM_ERR_INVALID;
   std::lock_guard<std::mutex> lk(ctx->call_mu);

@@ -37,7 +37,7 @@ EXPORTS = ("gm_create", "gm_destroy", "gm_last_error", "gm_status_string", "gm_c
            "gm_configure", "gm_invert", "gm_invert_ex", "gm_synthesize", "gm_synthesize_f64",
            "gm_synthesize_grid", "gm_lm_step", "gm_submit", "gm_poll", "gm_cancel", "gm_zeeman_from_levels",
            "gm_psf_gaussian", "gm_psf_from_table", "gm_get_stats", "gm_measure_peaks", "gm_measure_sfu_peak",
-           "gm_invert_noalloc", "gm_classical", "gm_serving_options")
+           "gm_invert_noalloc", "gm_classical", "gm_serving_options", "gm_wave_state_bytes")
 
 
 class GmError(RuntimeError):
@@ -117,6 +117,8 @@ def lib():
         L.gm_measure_peaks.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.gm_measure_sfu_peak.argtypes = [vp, C.POINTER(C.c_double)]
         L.gm_invert_noalloc.argtypes = [C.POINTER(Config), vp, i64, C.c_int, vp, vp, vp, vp, vp, vp]
+        L.gm_wave_state_bytes.argtypes = [C.c_int, C.c_int, i64]
+        L.gm_wave_state_bytes.restype = C.c_size_t
         _lib = L
     return _lib
 
@@ -176,6 +178,12 @@ def psf_gaussian(fwhm_mA, lam):
     out = np.zeros(len(lam))
     _check(lib().gm_psf_gaussian(fwhm_mA, _ptr(lam), len(lam), _ptr(out)))
     return out
+
+
+def wave_state_bytes(nl, miter, pixels):
+    """Device bytes of wave-kernel LM state for a chunk of `pixels` pixels
+    (gm_wave_state_bytes): what an HBM budget must leave room for."""
+    return int(lib().gm_wave_state_bytes(int(nl), int(miter), int(pixels)))
 
 
 def psf_from_table(x_mA, y, offsets_mA, step_mA):

@@ -291,6 +291,14 @@ gm_status gm_measure_peaks(gm_ctx *ctx, double *fp32_tflops, double *fp64_tflops
  * in the reference. */
 gm_status gm_measure_sfu_peak(gm_ctx *ctx, double *gops);
 
+/* Device bytes of wave-synchronous inversion state for a chunk of `pixels`
+ * pixels on a grid of nl samples with at most miter iterations: what an
+ * inversion of that many pixels (one chunk) adds to its cube and outputs,
+ * and what a context's HBM budget must leave room for (at least 16384 pixels'
+ * worth, else the fused kernel runs).  0 for nl outside 1..GM_MAX_NL or a
+ * negative count.  No counterpart in the reference; needs no device. */
+size_t gm_wave_state_bytes(int nl, int miter, int64_t pixels);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,23 @@ def test_library_exports_every_file_format_function():
         assert re.search(r"\bT %s\b" % n, out), n
 
 
+def test_wave_state_bytes():
+    """Per pixel of a chunk: the 576-byte LM record, the staging block of
+    (27 LPL + 1) x 32 floats and three list entries; 16 bytes of counters per
+    wave (1 + max(miter, 1) waves) and 256 bytes of alignment slack."""
+    per1 = 576 + 4 * (27 * 1 + 1) * 32 + 12
+    per2 = 576 + 4 * (27 * 2 + 1) * 32 + 12
+    assert G.wave_state_bytes(30, 50, 1000) == 1000 * per1 + 16 * 51 + 256
+    assert G.wave_state_bytes(32, 50, 1000) == 1000 * per1 + 16 * 51 + 256
+    assert G.wave_state_bytes(33, 50, 1000) == 1000 * per2 + 16 * 51 + 256
+    assert G.wave_state_bytes(30, 0, 10) == 10 * per1 + 16 * 2 + 256
+    assert G.wave_state_bytes(30, 50, 0) == 16 * 51 + 256
+    for bad in ((0, 50, 10), (G.MAX_NL + 1, 50, 10), (30, 50, -1)):
+        assert G.wave_state_bytes(*bad) == 0
+    # a full 2^20-pixel chunk at nl <= 32: about 4.2 KB per pixel
+    assert 4.1e3 < G.wave_state_bytes(30, 50, 1 << 20) / (1 << 20) < 4.3e3
+
+
 def test_status_strings():
     lib = G.lib()
     assert lib.gm_status_string(0) == b"ok"
