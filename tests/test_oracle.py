@@ -215,6 +215,30 @@ def test_lm_single_equals_batch():
         np.testing.assert_array_equal(f, fb[p])
 
 
+def test_early_stop_rule():
+    """stop_dchi2 > 0 (the ragged-batch option, not in the reference) ends a
+    pixel at the first accepted step that improves chi2 by less than the
+    threshold: it never lengthens a fit, a pixel it does not cut follows the
+    reference trajectory exactly, and a threshold of 0 is the reference."""
+    rng = np.random.default_rng(29)
+    l0, z = H.fe_line()
+    lam, _ = H.grid()
+    t = H.truth_models(64, rng)
+    base = O.make_cfg(lam, l0, z, init=H.GUESS)
+    obs = H.observations(base, t, rng)
+    m0, c0, i0, a0, _ = O.lm_batch_f(base, obs, nthreads=0)
+    mz, cz, iz, az, _ = O.lm_batch_f(O.make_cfg(lam, l0, z, init=H.GUESS, stop_dchi2=0.0), obs, nthreads=0)
+    np.testing.assert_array_equal(mz, m0)
+    np.testing.assert_array_equal(iz, i0)
+    me, ce, ie, ae, _ = O.lm_batch_f(O.make_cfg(lam, l0, z, init=H.GUESS, stop_dchi2=1e-4), obs, nthreads=0)
+    assert (ie <= i0).all()
+    cut = ie < i0
+    assert cut.mean() > 0.5, cut.mean()
+    np.testing.assert_array_equal(me[~cut], m0[~cut])
+    # a cut fit ends on an accepted step
+    assert (ae[cut] >= 1).all() and (ae[cut] <= a0[cut]).all()
+
+
 def test_lm_step_decreases_chi2_with_large_damping():
     rng = np.random.default_rng(23)
     l0, z = H.fe_line()
