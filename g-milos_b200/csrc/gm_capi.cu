@@ -395,15 +395,17 @@ struct StepOut {
 // Smallest pipelined host-memory inversion: two chunks of kPipeChunk pixels.
 constexpr int64_t kPipeChunk = 131072;
 // Pixels per chunk of the wave-synchronous inversion (its LM state and
-// staging take about 3.6 KB per pixel at nl <= 32, 6.6 KB above): large
-// chunks make each wave's launches long against their tails.  Below
+// staging take about 4.2 KB per pixel at nl <= 32, 7.6 KB above,
+// gm_wave_state_bytes): large chunks make each wave's launches long against
+// their tails.  Below
 // kWaveMinChunk pixels within the budget the fused kernel runs instead.
 constexpr int64_t kWaveChunk = 1 << 20;
 constexpr int64_t kWaveMinChunk = 16384;
 
 // The wave-synchronous kernels cover the launch unless the environment
 // variable GMILOS_INVERT_KERNEL=fused selects the single persistent kernel
-// (both give the same results; the switch serves comparisons).
+// (the two agree to rounding; the switch serves comparisons and the
+// bit-for-bit tests against gm_invert_noalloc).
 static bool want_waves(const gm::DevCfg& d, const gm::InvertArgs& ia) {
   const char* k = std::getenv("GMILOS_INVERT_KERNEL");
   if (k && std::strcmp(k, "fused") == 0) return false;
