@@ -798,7 +798,19 @@ cudaError_t launch_peak(int kind, int blocks, int threads, int iters, void* sink
 
 // ---------------------------------------------------------------- launchers
 template <int LPL, int V>
-size_t smem_bytes() { return tap_bytes<LPL>() + sizeof(WarpSmem<LPL, V>) * warps_per_block<LPL>(); }
+constexpr size_t smem_bytes() { return tap_bytes<LPL>() + sizeof(WarpSmem<LPL, V>) * warps_per_block<LPL>(); }
+
+// The wave kernels' launch bounds assume their blocks per SM; their shared
+// memory (plus the 1 KB the SM reserves per block) must fit those too.
+constexpr size_t kSmemPerSm = 228 * 1024;
+template <int LPL, int V>
+constexpr bool wave_blocks_fit() {
+  return (tap_bytes<LPL>() + trial_warp_bytes<LPL, V>() * warps_per_block<LPL>() + 1024) *
+                 trial_min_blocks<LPL, V>() <= kSmemPerSm &&
+         (smem_bytes<LPL, V>() + 1024) * accept_min_blocks<LPL, V>() <= kSmemPerSm;
+}
+static_assert(wave_blocks_fit<1, 0>() && wave_blocks_fit<1, 1>() && wave_blocks_fit<1, 2>(), "nl <= 32");
+static_assert(wave_blocks_fit<2, 0>() && wave_blocks_fit<2, 1>() && wave_blocks_fit<2, 2>(), "nl <= 64");
 
 template <int LPL, int V>
 cudaError_t prepare_invert() {
