@@ -364,6 +364,15 @@ def run_engine(args):
                 rep = rg["report"]
                 cmp_ = _fit_comparison(outs["model"][:n].double().cpu().numpy(), outs["chi2"][:n].cpu().numpy(),
                                        outs["iters"][:n].cpu().numpy(), rg["model"], rg["chi2"], rg["iters"])
+                host_vs_gpu = None
+                if ref.available():
+                    # the reference's own host build on the same pixels: how
+                    # far two builds of the reference itself agree
+                    s, _ = _ref_setup(lam, psf)
+                    mh, ch, ih, _ = ref.invert_cpu(s, obs[:n].cpu().numpy(), slight=slight,
+                                                   nthreads=os.cpu_count())
+                    host_vs_gpu = _fit_comparison(mh, ch, ih, rg["model"], rg["chi2"], rg["iters"],
+                                                  names=("host_build", "gpu_build"))
                 result["reference_gpu"] = {
                     "what": "the reference's own lm_mils built for sm_100a (child launches run in-thread), "
                             "its launch geometry, streams and device heap, same cube",
@@ -373,11 +382,14 @@ def run_engine(args):
                                  "streams": rep["nstreams"], "registers": rep["regs"],
                                  "stack_bytes": rep["local_bytes"]},
                     "speedup_value": value / rg["value"], "speedup_e2e": e2e_value / rg["e2e"],
-                    "fit_vs_engine": cmp_}
+                    "fit_vs_engine": cmp_,
+                    "reference_host_vs_gpu": host_vs_gpu}
             except Exception as exc:  # the comparison must not take the bench line down
                 result["reference_gpu"] = {"unavailable": str(exc)[:200]}
         else:
             result["reference_gpu"] = {"unavailable": "oracle/_ref/libgmref_gpu.so not built"}
+    if rank == 0 and world == 1 and args.config1:
+        result["config1"] = config1_block(eng, args, torch)
     if rank == 0:
         print(json.dumps(result), flush=True)
     eng.close()
@@ -437,6 +449,75 @@ def serving_latency(eng, obs_h, args):
             "requests": n, "pixels": int(npix.sum())}
 
 
+FIX9 = (1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0)         # the 9 ME parameters
+
+
+def config1_block(eng, args, torch, reps=10):
+    """The reference's CPU-runnable case as specified: a 64 x 64 px cube x 4
+    Stokes x 30 lambda on the same grid and line, truth drawn from the same
+    ranges, noise 1e-3 Ic, no PSF, no stray light, 9 free parameters, at
+    most 50 iterations.  The engine inverts it device-resident (CUDA-event
+    time) and end to end from host memory (gm_invert); the reference's own
+    per-pixel routines, built host-side, invert the whole cube on every host
+    thread.  Both fits are compared pixel by pixel."""
+    import gmilos_b200 as G
+    import ref
+    lam, off = grid()
+    zee = G.zeeman_from_levels(2, 1, 1.0, 2, 2, 0.0, 1.0)
+    cfg = G.make_config(lam, LAMBDA0, zee, fix=FIX9, init=GUESS, miter=MAXITER)
+    eng.configure(cfg)
+    rng = np.random.default_rng(args.seed + 64)
+    P = 64 * 64
+    truth = truth_models(P, rng)
+    truth[:, 10] = 1.0
+    obs = eng.synthesize(truth)
+    obs = np.ascontiguousarray(obs + rng.normal(0, NOISE, obs.shape).astype(np.float32))
+    obs_d = torch.from_numpy(obs).cuda()
+    stream = torch.cuda.current_stream()
+    out = None
+    for _ in range(3):
+        out = eng.invert(obs_d, out=out, stream=stream.cuda_stream)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    evs[0].record(stream)
+    for _ in range(reps):
+        eng.invert(obs_d, out=out, stream=stream.cuda_stream)
+    evs[1].record(stream)
+    torch.cuda.synchronize()
+    dev_ms = evs[0].elapsed_time(evs[1]) / reps
+    obs_h = torch.from_numpy(obs).pin_memory()
+    model_h = torch.empty((P, 11), dtype=torch.float32).pin_memory()
+    chi_h = torch.empty(P, dtype=torch.float32).pin_memory()
+    it_h = torch.empty(P, dtype=torch.int32).pin_memory()
+    e2e = []
+    for k in range(reps + 1):
+        t0 = time.perf_counter()
+        eng.invert_plain(obs_h.numpy(), model_h.numpy(), chi2=chi_h.numpy(), iters=it_h.numpy())
+        if k:
+            e2e.append(time.perf_counter() - t0)
+    res = {"workload": "64x64 px x 4 Stokes x 30 lambda, no PSF, no stray light, 9 free, <= 50 iterations, "
+                       "noise 1e-3 Ic",
+           "engine": {"value": P / (dev_ms / 1e3), "unit": "pixels/s", "ms": dev_ms,
+                      "e2e": P / float(np.mean(e2e)), "mean_iterations": float(out["iters"].float().mean())}}
+    if ref.available():
+        import oracle as O
+        l0, z = O.fe6173()
+        s = ref.setup_from_cfg(O.make_cfg(lam, l0, z, fix=FIX9, init=GUESS, miter=MAXITER))
+        nthreads = os.cpu_count()
+        times = []
+        for k in range(3):
+            t0 = time.perf_counter()
+            mr, cr, ir, _ = ref.invert_cpu(s, obs, nthreads=nthreads)
+            times.append(time.perf_counter() - t0)
+        cpu_value = P / float(np.mean(times))
+        res["reference_cpu"] = {"value": cpu_value, "unit": "pixels/s", "cores": nthreads,
+                                "kind": "reference", "sample": "the whole 4096-pixel cube, 3 runs"}
+        res["speedup_e2e_vs_reference_cpu"] = res["engine"]["e2e"] / cpu_value
+        res["fit_vs_reference"] = _fit_comparison(out["model64"].cpu().numpy(), out["chi2"].cpu().numpy(),
+                                                  out["iters"].cpu().numpy(), mr, cr, ir)
+    return res
+
+
 # ----------------------------------------------------------------- reference arms
 def _ref_setup(lam, psf):
     """The reference's configuration for this workload (oracle/ref.py)."""
@@ -488,7 +569,9 @@ def reference_gpu(obs, slight, psf, lam, nstreams=16):
             "model": m, "chi2": chi, "iters": it}
 
 
-def _fit_comparison(mg, cg, ig, mr, cr, ir):
+def _fit_comparison(mg, cg, ig, mr, cr, ir, names=("engine", "reference")):
+    """Agreement of two fits of the same pixels (|dB| < 1 G, angles < 0.1 deg,
+    vlos < 5 m/s) and, where they part, on which side chi2 is worse."""
     agree = ((np.abs(mg[:, 1] - mr[:, 1]) < 1.0)
              & (np.minimum(np.abs(mg[:, 5] - mr[:, 5]) % 360, 360 - np.abs(mg[:, 5] - mr[:, 5]) % 360) < 0.1)
              & (np.minimum(np.abs(mg[:, 6] - mr[:, 6]) % 180, 180 - np.abs(mg[:, 6] - mr[:, 6]) % 180) < 0.1)
@@ -496,8 +579,8 @@ def _fit_comparison(mg, cg, ig, mr, cr, ir):
     return {"median_chi2": [float(np.median(cg)), float(np.median(cr))],
             "mean_iterations": [float(np.mean(ig)), float(np.mean(ir))],
             "agree": float(agree.mean()),
-            "engine_chi2_worse": float((~agree & (cg > cr * (1 + 1e-3) + 1e-6)).mean()),
-            "reference_chi2_worse": float((~agree & (cr > cg * (1 + 1e-3) + 1e-6)).mean())}
+            names[0] + "_chi2_worse": float((~agree & (cg > cr * (1 + 1e-3) + 1e-6)).mean()),
+            names[1] + "_chi2_worse": float((~agree & (cr > cg * (1 + 1e-3) + 1e-6)).mean())}
 
 
 def _reference_sample(args):
@@ -605,6 +688,8 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=1.0, help="mean arrivals per second")
     ap.add_argument("--serve-side-min", type=int, default=256)
     ap.add_argument("--serve-side-max", type=int, default=2048)
+    ap.add_argument("--no-config1", dest="config1", action="store_false",
+                    help="skip the 64x64 no-PSF case (engine and the reference's CPU routines)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -212,6 +212,8 @@ gm_status build_devcfg(gm_ctx* ctx, const gm_config& c, gm::DevCfg* d) {
   d->quirks = c.reference_quirks;
   if (c.numerics != GM_NUMERICS_REFERENCE && c.numerics != GM_NUMERICS_ACCURATE)
     return fail(ctx, GM_ERR_INVALID, "numerics must be GM_NUMERICS_REFERENCE or GM_NUMERICS_ACCURATE");
+  if (c.kernel != GM_KERNEL_AUTO && c.kernel != GM_KERNEL_FUSED)
+    return fail(ctx, GM_ERR_INVALID, "kernel must be GM_KERNEL_AUTO or GM_KERNEL_FUSED");
   d->numerics = c.numerics;
   d->n_pi = z.n_pi;
   d->n_sig = z.n_sig;
@@ -402,13 +404,12 @@ constexpr int64_t kPipeChunk = 131072;
 constexpr int64_t kWaveChunk = 1 << 20;
 constexpr int64_t kWaveMinChunk = 16384;
 
-// The wave-synchronous kernels cover the launch unless the environment
-// variable GMILOS_INVERT_KERNEL=fused selects the single persistent kernel
-// (the two agree to rounding; the switch serves comparisons and the
+// The wave-synchronous kernels cover the launch unless the configuration
+// selects the single persistent kernel (gm_config.kernel = GM_KERNEL_FUSED:
+// the two agree to rounding; the choice serves comparisons and the
 // bit-for-bit tests against gm_invert_noalloc).
-static bool want_waves(const gm::DevCfg& d, const gm::InvertArgs& ia) {
-  const char* k = std::getenv("GMILOS_INVERT_KERNEL");
-  if (k && std::strcmp(k, "fused") == 0) return false;
+static bool want_waves(const gm_ctx* ctx, const gm::DevCfg& d, const gm::InvertArgs& ia) {
+  if (ctx->cfg.kernel == GM_KERNEL_FUSED) return false;
   return gm::waves_cover(d, ia);
 }
 
@@ -446,7 +447,7 @@ static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::Inver
   if (prepass) d1.init_mode = 1;
   const int64_t most = (npix + nch - 1) / nch;
   // one wave chunk per pipeline chunk and stream
-  const bool waves = want_waves(d1, ia) && wave_chunk_for(ctx, d1, need, most, 2) == most;
+  const bool waves = want_waves(ctx, d1, ia) && wave_chunk_for(ctx, d1, need, most, 2) == most;
   gm::WaveBuffers wb[2];
   if (waves) {
     gm_status st = wave_buffers(ctx, "waves0", d1, most, &wb[0]);
@@ -615,7 +616,7 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   }
   gm::InvertGeometry geo;
   const int64_t grid = invert_grid(d, ia.init_models != nullptr && !ia.init_status, ctx->sms, npix, &geo);
-  const int64_t wchunk = want_waves(d, ia) ? wave_chunk_for(ctx, d, need, npix, 1) : 0;
+  const int64_t wchunk = want_waves(ctx, d, ia) ? wave_chunk_for(ctx, d, need, npix, 1) : 0;
   const bool waves = wchunk > 0;
   gm::WaveBuffers wb{};
   if (waves && (st = wave_buffers(ctx, "waves0", d, wchunk, &wb)) != GM_OK) return st;
@@ -1032,7 +1033,7 @@ gm_status launch_chunk(gm_ctx* ctx, ServeLane& L, const std::shared_ptr<Request>
     ia.init_status = cs;
     d.init_mode = 1;
   }
-  if (lane_ok && want_waves(d, ia)) {
+  if (lane_ok && want_waves(ctx, d, ia)) {
     e = gm::launch_invert_waves(d, ia, gm::wave_buffers(L.scratch, d.nl, d.miter, L.chunk), s, nullptr);
   } else {
     const int64_t grid = invert_grid(d, ia.init_models != nullptr && !ia.init_status, ctx->sms, n, nullptr);
@@ -1199,8 +1200,9 @@ std::mutex g_noalloc_mu;
 void* g_noalloc_addr[kNoallocMaxDevices] = {};
 
 // Device address of the scratch array on the current device.  The first call
-// per device (with that device current) looks it up and loads the inversion
-// kernel, so later calls do neither.
+// per device (with that device current) looks it up and loads every variant
+// of the inversion kernel (grids of <= 32 and <= 64 samples; 10 terms, 10
+// terms with macroturbulence, 11 terms), so later calls do neither.
 gm_status noalloc_scratch(int dev, void** out) {
   if (dev < 0 || dev >= kNoallocMaxDevices) return GM_ERR_INVALID;
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
@@ -1211,14 +1213,17 @@ gm_status noalloc_scratch(int dev, void** out) {
       cudaGetLastError();
       return GM_ERR_CUDA;
     }
-    gm::DevCfg probe{};
-    probe.nl = 32;
-    probe.nterms = 10;
-    const int b32 = gm::invert_geometry(probe, false).blocks_per_sm;
-    probe.nl = 64;
-    if (b32 < 1 || gm::invert_geometry(probe, false).blocks_per_sm < 1) {
-      cudaGetLastError();
-      return GM_ERR_CUDA;
+    for (int nl : {32, 64}) {
+      for (int v = 0; v < 3; ++v) {
+        gm::DevCfg probe{};
+        probe.nl = nl;
+        probe.nterms = v == 2 ? 11 : 10;
+        probe.init[gm::MAC] = v == 1 ? 1.0 : 0.0;
+        if (gm::invert_geometry(probe, false).blocks_per_sm < 1) {
+          cudaGetLastError();
+          return GM_ERR_CUDA;
+        }
+      }
     }
     g_noalloc_addr[dev] = p;
   }

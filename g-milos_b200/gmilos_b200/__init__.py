@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libgmilos.so")
 PKG_ROOT = os.path.dirname(HERE)
 MAX_NL = 64
 NPAR = 11
-ABI_VERSION = 2
+ABI_VERSION = 3
 PARAM_NAMES = ("eta0", "B", "vlos", "dopp", "aa", "gm", "az", "S0", "S1", "mac", "alfa")
 
 GM_OK = 0
@@ -31,6 +31,7 @@ PIX_BAD_INPUT = 0x20
 
 INIT_CLASSICAL, INIT_GIVEN, INIT_PER_PIXEL = 0, 1, 2
 NUMERICS_REFERENCE, NUMERICS_ACCURATE = 0, 1
+KERNEL_AUTO, KERNEL_FUSED = 0, 1
 
 # Symbols include/gmilos.h declares (checked by the tests against the .so).
 EXPORTS = ("gm_create", "gm_destroy", "gm_last_error", "gm_status_string", "gm_config_defaults",
@@ -63,7 +64,7 @@ class Config(C.Structure):
                 ("use_slight", C.c_int), ("slight_per_pixel", C.c_int),
                 ("slight", C.POINTER(C.c_float)), ("reference_quirks", C.c_int),
                 ("numerics", C.c_int), ("lambda_per_pixel", C.c_int),
-                ("lambda_map", C.POINTER(C.c_double))]
+                ("lambda_map", C.POINTER(C.c_double)), ("kernel", C.c_int)]
 
 
 class Request(C.Structure):
@@ -199,11 +200,13 @@ def make_config(lam, lambda0, zeeman, psf=None, mu=1.0, weight=(1, 1, 1, 1), noi
                 fix=(1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0), init=None, init_mode=INIT_CLASSICAL,
                 miter=50, ilambda=0.1, toplim=1e-12, logclambda=0, stop_dchi2=0.0,
                 slight=None, slight_per_pixel=False, reference_quirks=1, numerics=0,
-                lambda_map=None):
+                lambda_map=None, kernel=KERNEL_AUTO):
     """Engine configuration (gm_config).  lambda_map: optional per-pixel
     wavelength grids [P][nl] (absolute, A; numpy or a CUDA tensor of float64),
     read at each call like a per-pixel stray map; `lam` then only sizes the
-    grid and the PSF stays `psf`."""
+    grid and the PSF stays `psf`.  kernel: KERNEL_AUTO (wave-synchronous
+    kernels where they cover the call) or KERNEL_FUSED (the fused kernel for
+    every call)."""
     c = Config()
     lib().gm_config_defaults(C.byref(c))
     lam = np.asarray(lam, dtype=np.float64)
@@ -235,6 +238,7 @@ def make_config(lam, lambda0, zeeman, psf=None, mu=1.0, weight=(1, 1, 1, 1), noi
     c.stop_dchi2 = stop_dchi2
     c.reference_quirks = reference_quirks
     c.numerics = numerics
+    c.kernel = kernel
     c._slight_ref = None
     c._lambda_ref = None
     if lambda_map is not None:

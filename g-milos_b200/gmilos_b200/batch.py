@@ -10,8 +10,24 @@ write, done once.
 import numpy as np
 
 
-def grid_key(lam):
-    return tuple(np.round(np.asarray(lam, dtype=np.float64), 9))
+GRID_ATOL = 1e-9   # A: grids closer than this everywhere are the same grid
+
+
+def group_grids(lams, atol=GRID_ATOL):
+    """Group wavelength grids that agree to `atol` at every sample (same
+    length).  Returns one group index per grid; a group is inverted on its
+    first member's exact wavelengths."""
+    firsts, idx = [], []
+    for lam in lams:
+        lam = np.asarray(lam, dtype=np.float64)
+        for g, f in enumerate(firsts):
+            if len(f) == len(lam) and np.allclose(lam, f, rtol=0.0, atol=atol):
+                idx.append(g)
+                break
+        else:
+            firsts.append(lam)
+            idx.append(len(firsts) - 1)
+    return idx
 
 
 def invert_rois(engine, rois, config_for_grid, fitted=False):
@@ -23,11 +39,12 @@ def invert_rois(engine, rois, config_for_grid, fitted=False):
     the lane occupancy (wavelength samples over lane slots, 32 per lane row
     of up to 32 samples, 64 above)."""
     groups = {}
+    gidx = group_grids([lam for _, lam in rois])
     for i, (iquv, lam) in enumerate(rois):
         a = np.ascontiguousarray(iquv, dtype=np.float32)
         if a.ndim != 3 or a.shape[1] != 4 or a.shape[2] != len(lam):
             raise ValueError("ROI %d: iquv must be [P][4][nl] on its own grid" % i)
-        groups.setdefault(grid_key(lam), []).append((i, a, lam))
+        groups.setdefault(gidx[i], []).append((i, a, lam))
     out = [None] * len(rois)
     pixels = 0
     slots = 0.0

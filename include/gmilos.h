@@ -43,7 +43,7 @@ extern "C" {
 
 #define GM_MAX_NL 64          /* wavelength samples per pixel (reference: MAX_LAMBDA 50) */
 #define GM_NPAR 11
-#define GM_ABI_VERSION 2
+#define GM_ABI_VERSION 3
 
 typedef enum {
     GM_OK = 0,
@@ -118,7 +118,17 @@ typedef struct {
                                      those of `psf`.  The reference's per-pixel
                                      wavelength FITS (utilsFits.c:1488-1500). */
     const double *lambda_map;     /* [P][nl] absolute wavelengths [A], host or device */
+    int kernel;                   /* GM_KERNEL_AUTO (default): the wave-synchronous
+                                     kernels where they cover the call, else the
+                                     fused kernel; GM_KERNEL_FUSED: the fused
+                                     persistent kernel for every call (the kernel
+                                     of gm_invert_noalloc) */
 } gm_config;
+
+/* Inversion kernels (gm_config.kernel).  Both execute the same LM arithmetic;
+ * compiled as different kernels they round differently at the float level. */
+#define GM_KERNEL_AUTO 0
+#define GM_KERNEL_FUSED 1
 
 /* Trigonometry of the 10x10 Jacobi solve and of the field angles.
  * REFERENCE uses the hardware approximations the reference uses
@@ -155,9 +165,8 @@ gm_status gm_configure(gm_ctx *ctx, const gm_config *cfg);
  * whose budget leaves room for fewer than 16384 pixels of state run one fused
  * persistent kernel.  Both execute the same LM arithmetic; compiled
  * as different kernels they round differently at the float level, so their
- * trajectories agree to rounding.  The environment variable
- * GMILOS_INVERT_KERNEL=fused selects the fused kernel for every call (for
- * comparisons). */
+ * trajectories agree to rounding.  gm_config.kernel = GM_KERNEL_FUSED
+ * selects the fused kernel for every call (for comparisons). */
 gm_status gm_invert(gm_ctx *ctx, const float *iquv, int64_t npix, int nl,
                     float *model, float *chi2, int *iters, float *fitted,
                     uint32_t *status, void *stream);
@@ -170,20 +179,26 @@ gm_status gm_invert_ex(gm_ctx *ctx, const float *iquv, int64_t npix, int nl,
                        uint32_t *status, void *stream);
 
 /* Inversion for callers that cannot allocate device memory (the fused kernel,
- * its results those of gm_invert with GMILOS_INVERT_KERNEL=fused).  No
- * counterpart in the reference.  Some callers cannot call cudaMalloc while they run: code
- * inside a CUDA-graph capture or a real-time pipeline that must not block on
- * the allocator, or a host framework that owns every device byte itself.
- * This entry point allocates nothing: it takes the configuration directly
- * (no gm_ctx) and only device pointers (inputs [P][4][nl], outputs as in
- * gm_invert; fitted, chi2, iters, status may be NULL).  Its scratch -- the
- * work-stealing counters and the global stray-light profile -- lives in one
- * file-scope device array of GM_NOALLOC_SCRATCH_BYTES that every GPU loading
- * the library keeps until the process exits; requests needing more are
- * rejected with GM_ERR_INVALID.  The first call on a device looks up that
- * array's address and loads the kernel; make it before any stream capture.
- * All calls share the array: calls that overlap on the GPU race, so serialise
- * them (one stream, or events).  Errors are reported by status only:
+ * its results those of gm_invert with gm_config.kernel = GM_KERNEL_FUSED).  No
+ * counterpart in the reference.  Some callers cannot call cudaMalloc while
+ * they run: a real-time pipeline (a telescope's on-line reduction loop, say)
+ * that must not stall on the allocator, which can synchronise the device and
+ * take milliseconds, or a host framework that owns every device byte through
+ * its own pool and whose accounting would break if the library allocated
+ * behind its back.  This entry point allocates nothing: it takes the
+ * configuration directly (no gm_ctx) and only device pointers (inputs
+ * [P][4][nl], outputs as in gm_invert; fitted, chi2, iters, status may be
+ * NULL; a per-pixel stray map must be device memory, a single stray profile
+ * may be host or device memory and is copied on `stream` by every call).
+ * Its scratch -- the work-stealing counters and the single stray-light
+ * profile -- lives in one file-scope device array of GM_NOALLOC_SCRATCH_BYTES
+ * that every GPU loading the library keeps until the process exits; requests
+ * needing more are rejected with GM_ERR_INVALID.  The first call on a device
+ * (with that device current) looks up that array's address and loads the
+ * inversion kernels; later calls do neither.  Every call clears the counters
+ * it needs before its launch.  All calls share the array and it keeps the
+ * last call's contents: calls that overlap on the GPU race, so serialise them
+ * (one stream, or events).  Errors are reported by status only:
  * GM_ERR_INVALID (bad configuration, host pointer, or scratch over the
  * maximum), GM_ERR_UNSUPPORTED (per-pixel wavelength grids), GM_ERR_CUDA. */
 #define GM_NOALLOC_SCRATCH_BYTES 4096

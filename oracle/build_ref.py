@@ -43,7 +43,10 @@ what the sources above contain, so a changed reference fails loudly.  Then:
       oracle/ref_shim/gmref_gpu.cu.
 
 Usage: python oracle/build_ref.py [--reference DIR] [--cpu-only]
-Requires the reference's sources; outputs only the two .so files.
+The reference checkout is --reference, else the GM_REFERENCE_DIR environment
+variable, else a directory named `reference` beside this repository's
+directory when one exists (locate_reference); without it nothing is built.
+Outputs only the two .so files.
 """
 from __future__ import annotations
 
@@ -58,7 +61,6 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 SHIM = os.path.join(HERE, "ref_shim")
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_REFERENCE = "/root/reference"
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
@@ -75,6 +77,18 @@ EXPECTED = {
     "mil_sinrf.cu": dict(launch=2, conv=1, sig=4, index=2, sync=3),
     "me_der.cu": dict(launch=2, conv=2, sig=4, index=2, sync=4),
 }
+
+
+def locate_reference(explicit=None):
+    """The reference checkout: `explicit`, else $GM_REFERENCE_DIR, else a
+    directory named `reference` beside this repository; None when none of
+    them holds the reference's sources."""
+    repo = os.path.dirname(HERE)
+    for cand in (explicit, os.environ.get("GM_REFERENCE_DIR"),
+                 os.path.join(os.path.dirname(repo), "reference")):
+        if cand and os.path.isfile(os.path.join(cand, "milosUtils.cu")):
+            return cand
+    return None
 
 
 def _match_paren(text: str, open_pos: int) -> int:
@@ -290,15 +304,16 @@ def build_gpu(reference: str) -> str:
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("--reference", default=os.environ.get("GM_REFERENCE_DIR", DEFAULT_REFERENCE))
+    ap.add_argument("--reference", default=None)
     ap.add_argument("--cpu-only", action="store_true")
     a = ap.parse_args(argv)
-    if not os.path.isfile(os.path.join(a.reference, "milosUtils.cu")):
-        print(f"reference sources not found under {a.reference}; nothing built")
+    reference = locate_reference(a.reference)
+    if reference is None:
+        print("reference sources not found (--reference, GM_REFERENCE_DIR or ../reference); nothing built")
         return 0
-    print(build_cpu(a.reference))
+    print(build_cpu(reference))
     if not a.cpu_only:
-        print(build_gpu(a.reference))
+        print(build_gpu(reference))
     return 0
 
 

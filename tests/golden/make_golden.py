@@ -1,8 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the reference tree.
 
-Run here, where the reference checkout exists (its path is the first argument,
-default /root/reference); the fixtures it writes are committed so that the
-tests never read the reference at run time.
+Run where the reference checkout exists (its path is the first argument, else
+GM_REFERENCE_DIR, else a `reference` directory beside this repository); the
+fixtures it writes are committed so that the tests never read the reference
+at run time.
 
 kat_synthesis.npz -- the reference's only shipped known-answer vector
 (data/synthesis_gpu.per, produced by `gmilos run/synthesis.mtrol`) together
@@ -62,4 +63,9 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle"))
+    from build_ref import locate_reference
+    where = locate_reference(sys.argv[1] if len(sys.argv) > 1 else None)
+    if where is None:
+        sys.exit("reference checkout not found: pass its path or set GM_REFERENCE_DIR")
+    main(where)

@@ -94,3 +94,10 @@ def rf_rel(a, b):
 def angle_diff(a, b, period=180.0):
     d = np.abs(np.asarray(a) - np.asarray(b)) % period
     return np.minimum(d, period - d)
+
+
+def fits_agree(ma, mb):
+    """Per pixel: two fitted models [P][11] agree to |dB| < 1 G, |d gamma| and
+    |d phi| < 0.1 deg (phi modulo 180) and |d vlos| < 5 m/s."""
+    return ((np.abs(ma[:, 1] - mb[:, 1]) < 1.0) & (angle_diff(ma[:, 5], mb[:, 5], 360) < 0.1)
+            & (angle_diff(ma[:, 6], mb[:, 6]) < 0.1) & (np.abs(ma[:, 2] - mb[:, 2]) < 0.005))

@@ -76,3 +76,18 @@ def test_mismatched_roi_is_an_error():
     bad = (rng.normal(size=(4, 4, 29)).astype(np.float32), g)
     with pytest.raises(ValueError):
         batch.invert_rois(FakeEngine(), [roi(rng, 4, g), bad], lambda lam: None)
+
+
+def test_grids_grouped_by_tolerance_not_rounding():
+    """Grids that differ by far less than the tolerance share a group even
+    where rounding to a fixed number of decimals would split them; grids
+    that differ by more, or in length, do not."""
+    base = 6173.3356 + np.linspace(-0.35, 0.665, 30)
+    base[3] = 6173.0000000004999999   # rounds to ...000 at 9 decimals
+    near = base.copy()
+    near[3] = 6173.0000000005000001   # rounds to ...001 at 9 decimals
+    far = base + 5e-9
+    short = base[:29]
+    idx = batch.group_grids([base, near, far, short, base.copy()])
+    assert idx[0] == idx[1] == idx[4]
+    assert len({idx[0], idx[2], idx[3]}) == 3

@@ -47,7 +47,7 @@ def configs(nl=30, psf=False, stray=False, fix=H.FREE9, **kw):
                                                                        if k in ("miter", "ilambda", "logclambda", "weight", "classical_init")})
     sl = H.stray_profile(ocfg) if stray else None
     gkw = {k: v for k, v in kw.items() if k in ("miter", "ilambda", "logclambda", "weight", "init_mode",
-                                                 "numerics")}
+                                                 "numerics", "kernel")}
     gcfg = G.make_config(lam, l0, zg, psf=p, fix=fix, init=H.GUESS, slight=sl, **gkw)
     return ocfg, gcfg, sl
 
@@ -182,7 +182,7 @@ def test_inversion_matches_reference(engine, psf, stray):
 
 
 @pytest.mark.parametrize("nl", [30, 45])
-def test_wave_and_fused_kernels_agree(engine, monkeypatch, nl):
+def test_wave_and_fused_kernels_agree(engine, nl):
     """The wave-synchronous kernels (the default) and the fused persistent
     kernel run the same LM arithmetic, compiled in different kernels: after
     one trial the models agree to float rounding, and full inversions match
@@ -195,12 +195,12 @@ def test_wave_and_fused_kernels_agree(engine, monkeypatch, nl):
     obs = H.observations(ocfg, t, rng, slight=sl)
     mr, cr, _, _, _ = O.lm_batch_f(ocfg, obs, slight=sl, nthreads=0)
     res = {}
-    for mode in ("waves", "fused"):
-        monkeypatch.setenv("GMILOS_INVERT_KERNEL", mode)
+    for mode, kernel in (("waves", G.KERNEL_AUTO), ("fused", G.KERNEL_FUSED)):
+        gcfg.kernel = kernel
         engine.configure(gcfg)
         full = engine.invert(obs)
         launches = engine.stats()["kernel_launches"]
-        _, g1, _ = configs(nl=nl, psf=True, stray=True, fix=fix, numerics=1, miter=1)
+        _, g1, _ = configs(nl=nl, psf=True, stray=True, fix=fix, numerics=1, miter=1, kernel=kernel)
         engine.configure(g1)
         res[mode] = (full, launches, engine.invert(obs)["model64"])
     (w, lw, w1), (f, lf, f1) = res["waves"], res["fused"]
@@ -329,17 +329,16 @@ def test_pipelined_host_inversion_equals_one_launch(engine):
     assert st["iterations"] == int(host["iters"].sum())
 
 
-def test_classical_prepass_equals_in_kernel_estimates(engine, monkeypatch):
+def test_classical_prepass_equals_in_kernel_estimates(engine):
     """gm_invert forms the classical start models in a pre-pass kernel;
     gm_invert_noalloc forms them inside the fused inversion kernel with the
     same device code: with gm_invert on the fused kernel too, the inversions
     agree bit for bit."""
     import ctypes as C
     torch = pytest.importorskip("torch")
-    monkeypatch.setenv("GMILOS_INVERT_KERNEL", "fused")
     rng = np.random.default_rng(720)
     fix = (1,) * 9 + (0, 1)
-    ocfg, gcfg, sl = configs(psf=True, stray=True, fix=fix)
+    ocfg, gcfg, sl = configs(psf=True, stray=True, fix=fix, kernel=G.KERNEL_FUSED)
     obs = H.observations(ocfg, H.truth_models(4096, rng, alpha_range=(0.7, 1.0)), rng, slight=sl)
     engine.configure(gcfg)
     a = engine.invert(obs)

@@ -6,14 +6,17 @@ reference's lm_mils with its own launch geometry, streams and device heap,
 child launches run in-thread).  The engine runs through its C ABI.
 
   - One LM iteration (miter = 1, classical-estimate start): the engine in
-    ACCURATE numerics against the host build; model p99 <= 1e-4 relative,
-    chi2 <= 1e-4 relative, identical accept/reject.
+    ACCURATE numerics against the host build, and in REFERENCE numerics
+    (the reference's __sincosf / __fdividef) against the sm_100a build;
+    model p99 <= 1e-4 relative, chi2 <= 1e-4 relative, the same
+    accept/reject decisions.
   - Full inversions of a cube with PSF and stray light: the engine in
-    REFERENCE numerics (the reference's __sincosf / __fdividef) against the
-    sm_100a build on identical inputs: median chi2 within 1 %, parameters
-    agreeing (|dB| < 1 G, angles < 0.1 deg, vlos < 5 m/s) on >= 75 % of
-    pixels, the engine's chi2 worse (by > 1e-3) on no more pixels than the
-    reference's is worse (+1 %), and truth recovery no worse.
+    REFERENCE numerics against the sm_100a build on identical inputs: median
+    chi2 within 1 %, parameters agreeing (|dB| < 1 G, angles < 0.1 deg,
+    vlos < 5 m/s) on at least the share (-2 %) on which the reference's own
+    host build agrees with its sm_100a build, the engine's chi2 worse (by
+    > 1e-3) on no more pixels than the reference's is worse (+1 %), and
+    truth recovery no worse.
 Skipped when the libraries are not built.
 """
 import numpy as np
@@ -72,37 +75,76 @@ def test_one_iteration_matches_reference_host_build(engine, psf, stray):
     assert np.percentile(crel, 99) < 1e-4
 
 
-@pytest.mark.skipif(not ref.available(gpu=True), reason="libgmref_gpu.so not built")
+@pytest.mark.skipif(not (ref.available(gpu=True) and ref.available()),
+                    reason="libgmref_gpu.so / libgmref_cpu.so not built")
 def test_inversions_match_reference_gpu_build(engine):
+    """Full inversions (PSF, stray light, 9 ME + alpha, <= 50 iterations).
+    Two FP32 implementations of the same LM trajectory part ways wherever
+    rounding flips one accept/reject decision, so the bar for the engine is
+    the reference's own: the engine agrees with the reference's sm_100a build
+    on at least as many pixels (-2 %) as the reference's host build does with
+    that same sm_100a build, on the same pixels; where fits part, neither
+    side is systematically better."""
     ocfg, s, gcfg, sl = setups(True, True, numerics=G.NUMERICS_REFERENCE)
     # 16 384 pixels: the shares of pixels where either side ends worse are
     # ~10 % each, so their difference has a standard deviation of ~0.34 %
     # and the 1 % margin below is ~3 sigma (on 4096 pixels single seeds
-    # swing by +-1.2 % either way)
+    # swing by +-1.2 % either way); the agreement shares have a standard
+    # deviation of ~0.35 %, so the 2 % margin is over 4 sigma
     t, obs = cube(ocfg, sl, 16384, 22)
     engine.configure(gcfg)
     out = engine.invert(obs)
     mr, cr, ir, _, rep = ref.invert_gpu(s, obs, slight=sl, nstreams=16)
     assert rep["malloc_failures"] == 0
+    mh, ch, ih, _ = ref.invert_cpu(s, obs, slight=sl)
     mg, cg = out["model64"], out["chi2"]
-    agree = ((np.abs(mg[:, 1] - mr[:, 1]) < 1.0) & (H.angle_diff(mg[:, 5], mr[:, 5], 360) < 0.1)
-             & (H.angle_diff(mg[:, 6], mr[:, 6]) < 0.1) & (np.abs(mg[:, 2] - mr[:, 2]) < 0.005))
+    agree = H.fits_agree(mg, mr)
+    agree_ref = H.fits_agree(mh, mr)
     worse_g = ~agree & (cg > cr * (1 + 1e-3) + 1e-6)
     worse_r = ~agree & (cr > cg * (1 + 1e-3) + 1e-6)
+    worse_h = ~agree_ref & (ch > cr * (1 + 1e-3) + 1e-6)
+    worse_hr = ~agree_ref & (cr > ch * (1 + 1e-3) + 1e-6)
     rec_g = (np.abs(mg[:, 1] - t[:, 1]) < 50).mean()
     rec_r = (np.abs(mr[:, 1] - t[:, 1]) < 50).mean()
-    print("vs reference sm_100a build: agree %.4f, engine chi2 worse %.4f, reference chi2 worse %.4f, "
-          "median chi2 %.4f / %.4f, iters %.1f / %.1f, |dB-truth|<50G %.4f / %.4f"
-          % (agree.mean(), worse_g.mean(), worse_r.mean(), np.median(cg), np.median(cr),
-             out["iters"].mean(), ir.mean(), rec_g, rec_r))
+    print("vs reference sm_100a build: engine agrees %.4f (chi2 worse %.4f, reference's worse %.4f); "
+          "reference host build agrees %.4f (chi2 worse %.4f, GPU build's worse %.4f); "
+          "median chi2 %.4f / %.4f / %.4f, iters %.1f / %.1f / %.1f, |dB-truth|<50G %.4f / %.4f"
+          % (agree.mean(), worse_g.mean(), worse_r.mean(), agree_ref.mean(), worse_h.mean(),
+             worse_hr.mean(), np.median(cg), np.median(cr), np.median(ch), out["iters"].mean(),
+             ir.mean(), ih.mean(), rec_g, rec_r))
     assert np.median(cg) == pytest.approx(np.median(cr), rel=0.01)
-    # Two FP32 implementations of the same LM trajectory part ways wherever
-    # rounding flips an accept/reject decision (the reference's host and GPU
-    # builds agree on ~84 % of these pixels); where they part, neither side
-    # is systematically better.
-    assert agree.mean() >= 0.75
+    assert agree.mean() >= agree_ref.mean() - 0.02
     assert worse_g.mean() <= worse_r.mean() + 0.01
     assert rec_g >= rec_r - 0.01
+
+
+@pytest.mark.skipif(not ref.available(gpu=True), reason="libgmref_gpu.so not built")
+@pytest.mark.parametrize("psf,stray", [(False, False), (True, True)])
+def test_one_iteration_reference_numerics_vs_reference_gpu_build(engine, psf, stray):
+    """One LM iteration (miter = 1, classical-estimate start) in REFERENCE
+    numerics -- the reference's __sincosf / __fdividef in the solve and the
+    angles -- against the reference's own sm_100a build: the same
+    accept/reject decision and trial models within 1e-4 (p99)."""
+    fix = FIX if stray else H.FREE9
+    ocfg, s, gcfg, sl = setups(psf, stray, miter=1, numerics=G.NUMERICS_REFERENCE, fix=fix)
+    t, obs = cube(ocfg, sl, 4096, 24)
+    engine.configure(gcfg)
+    out = engine.invert(obs)
+    mr, cr, ir, _, rep = ref.invert_gpu(s, obs, slight=sl, nstreams=16)
+    assert rep["malloc_failures"] == 0
+    rel = np.abs(out["model64"] - mr) / np.maximum(np.abs(mr), 1e-3)
+    crel = np.abs(out["chi2"] - cr) / cr
+    # the output is the last accepted model: a different accept/reject
+    # decision shows as a whole step's difference, far above 1e-3
+    same = (rel[:, :9].max(axis=1) < 1e-3).mean()
+    print("one iteration, REFERENCE numerics vs reference sm_100a build: same decision %.4f, model rel "
+          "p50 %.2e p99 %.2e max %.2e, chi2 rel p99 %.2e"
+          % (same, np.percentile(rel[:, :9], 50), np.percentile(rel[:, :9], 99), rel[:, :9].max(),
+             np.percentile(crel, 99)))
+    assert (out["iters"] == ir).all()
+    assert same >= 0.999
+    assert np.percentile(rel[:, :9], 99) < 1e-4
+    assert np.percentile(crel, 99) < 1e-4
 
 
 @pytest.mark.skipif(not ref.available(), reason="libgmref_cpu.so not built")

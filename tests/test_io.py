@@ -10,7 +10,9 @@ import pytest
 
 import gmilos_b200.io as gio
 
-REF = os.environ.get("GM_REFERENCE_DIR", "/root/reference")
+from build_ref import locate_reference
+
+REF = locate_reference() or ""
 
 FIELDS = ["Number of cycles          (*)", "Observed profiles          (*)", "Stray light file             ",
           "PSF file                     ", "Wavelength grid file      (s)", "Atomic parameters file       ",
