@@ -390,6 +390,11 @@ def run_engine(args):
             result["reference_gpu"] = {"unavailable": "oracle/_ref/libgmref_gpu.so not built"}
     if rank == 0 and world == 1 and args.config1:
         result["config1"] = config1_block(eng, args, torch)
+    if rank == 0 and world == 1 and args.mlp_train_pixels > 0:
+        try:
+            result["learned_init"] = learned_block(eng, args, torch)
+        except Exception as exc:  # the block must not take the bench line down
+            result["learned_init"] = {"unavailable": str(exc)[:300]}
     if rank == 0:
         print(json.dumps(result), flush=True)
     eng.close()
@@ -515,6 +520,107 @@ def config1_block(eng, args, torch, reps=10):
         res["speedup_e2e_vs_reference_cpu"] = res["engine"]["e2e"] / cpu_value
         res["fit_vs_reference"] = _fit_comparison(out["model64"].cpu().numpy(), out["chi2"].cpu().numpy(),
                                                   out["iters"].cpu().numpy(), mr, cr, ir)
+    return res
+
+
+def _timed_inversions(eng, obs_d, torch, reps):
+    """Device time per inversion (CUDA events over `reps` calls after one
+    untimed call) and the last call's outputs."""
+    stream = torch.cuda.current_stream()
+    out = eng.invert(obs_d, stream=stream.cuda_stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for _ in range(reps):
+        eng.invert(obs_d, out=out, stream=stream.cuda_stream)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    return ev[0].elapsed_time(ev[1]) / reps, out
+
+
+def learned_block(eng, args, torch, reps=3):
+    """The learned initial guess (MLP 120 -> 256 -> 256 -> 9, GELU, BF16
+    weights, FP32 accumulation): trained by the engine's own tensor-core
+    kernels on pixels its ME synthesis generates (the 30-sample grid, the
+    PSF of the headline cube, truth from the same ranges, noise 1e-3 Ic),
+    then used as the start model of a cube it has not seen, against the
+    plain GPU form (classical start, the reference's stop rule) on the same
+    cube: pixels/s, iterations, chi2 and the error against the truth."""
+    import gmilos_b200 as G
+    lam, off = grid()
+    x, y = psf_table()
+    psf = G.psf_from_table(x, y, off, GRID[1])
+    zee = G.zeeman_from_levels(2, 1, 1.0, 2, 2, 0.0, 1.0)
+    mk = lambda **kw: G.make_config(lam, LAMBDA0, zee, psf=psf, fix=FIX9, init=GUESS, miter=MAXITER, **kw)
+    eng.configure(mk())
+    dev = torch.device("cuda")
+
+    def cube(n, seed):
+        rng = np.random.default_rng(seed)
+        t = truth_models(n, rng)
+        t[:, 10] = 1.0
+        td = torch.tensor(t, dtype=torch.float64, device=dev)
+        o = eng.synthesize(td)
+        g = torch.Generator(device=dev)
+        g.manual_seed(seed)
+        o += NOISE * torch.randn(o.shape, generator=g, device=dev, dtype=torch.float32)
+        torch.cuda.synchronize()
+        return t, td, o.contiguous()
+
+    n_train = args.mlp_train_pixels
+    _, t_train, o_train = cube(n_train, args.seed + 400)
+    net = G.mlp_new(len(lam), args.seed)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = eng.mlp_train(net, o_train, t_train, epochs=args.mlp_epochs, batch=16384, lr=2e-3, seed=args.seed)
+    train_s = time.perf_counter() - t0
+    del o_train, t_train
+    # algorithmic FLOPs per training sample: forward 2 (120*256 + 256*256 + 256*9),
+    # backward twice that (activation and weight gradients)
+    f_fwd = 2 * (120 * 256 + 256 * 256 + 256 * 9)
+    P = args.mlp_eval_pixels
+    truth, _, obs = cube(P, args.seed + 500)
+    # inference alone (includes uploading and packing the network)
+    eng.configure(mk())
+    eng.mlp_predict(net, obs)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record()
+    for _ in range(reps):
+        starts = eng.mlp_predict(net, obs)
+    ev[1].record()
+    torch.cuda.synchronize()
+    infer_ms = ev[0].elapsed_time(ev[1]) / reps
+    res = {"workload": "train %d px (%d epochs, batch 16384); evaluate on %d px x 4 x 30 lambda, PSF, noise 1e-3 Ic, "
+                       "9 free, <= 50 iterations" % (n_train, args.mlp_epochs, P),
+           "training": {"seconds": train_s, "loss_per_epoch": [float(v) for v in losses],
+                        "samples_per_s": n_train * args.mlp_epochs / train_s,
+                        "tflops_algorithmic": 3 * f_fwd * n_train * args.mlp_epochs / train_s / 1e12},
+           "inference": {"ms": infer_ms, "pixels_per_s": P / (infer_ms / 1e3),
+                         "tflops_algorithmic": f_fwd * P / (infer_ms / 1e3) / 1e12}}
+    variants = {"plain": mk(), "plain_early_stop": mk(stop_dchi2=1e-4),
+                "learned": mk(init_mode=G.INIT_LEARNED, mlp=net),
+                "learned_early_stop": mk(init_mode=G.INIT_LEARNED, mlp=net, stop_dchi2=1e-4)}
+    for name, cfg in variants.items():
+        eng.configure(cfg)
+        ms, out = _timed_inversions(eng, obs, torch, reps)
+        m = out["model64"].cpu().numpy()
+        chi = out["chi2"].cpu().numpy()
+        st = out["status"].cpu().numpy()
+        res[name] = {"pixels_per_s": P / (ms / 1e3), "ms": ms,
+                     "mean_iterations": float(out["iters"].float().mean()),
+                     "median_chi2": float(np.median(chi)),
+                     "learned_start_share": float(((st & G.PIX_LEARNED_INIT) != 0).mean()),
+                     "median_abs_error": {"B_G": float(np.median(np.abs(m[:, 1] - truth[:, 1]))),
+                                          "vlos_kms": float(np.median(np.abs(m[:, 2] - truth[:, 2]))),
+                                          "gamma_deg": float(np.median(np.abs(m[:, 5] - truth[:, 5]))),
+                                          "phi_deg": float(np.median(np.minimum(np.abs(m[:, 6] - truth[:, 6]) % 180,
+                                                                                180 - np.abs(m[:, 6] - truth[:, 6]) % 180)))}}
+    res["speedup_learned_early_stop_vs_plain"] = res["learned_early_stop"]["pixels_per_s"] / res["plain"]["pixels_per_s"]
+    # the network's own start models against the truth
+    s = starts.cpu().numpy()
+    res["start_models_median_abs_error"] = {"B_G": float(np.median(np.abs(s[:, 1] - truth[:, 1]))),
+                                            "vlos_kms": float(np.median(np.abs(s[:, 2] - truth[:, 2])))}
     return res
 
 
@@ -690,6 +796,10 @@ def main():
     ap.add_argument("--serve-side-max", type=int, default=2048)
     ap.add_argument("--no-config1", dest="config1", action="store_false",
                     help="skip the 64x64 no-PSF case (engine and the reference's CPU routines)")
+    ap.add_argument("--mlp-train-pixels", type=int, default=1 << 22,
+                    help="training pixels of the learned initial guess (0: skip that block)")
+    ap.add_argument("--mlp-epochs", type=int, default=8)
+    ap.add_argument("--mlp-eval-pixels", type=int, default=1 << 20)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

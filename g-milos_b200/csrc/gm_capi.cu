@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include "gm_kernels.cuh"
+#include "gm_mlp.cuh"
 #include "gmilos.h"
 
 namespace {
@@ -109,6 +110,11 @@ struct gm_ctx {
   std::thread worker;
   bool stopping = false;
   std::mutex call_mu;                 // serialises the synchronous entry points
+  // learned initial guess (GM_INIT_LEARNED): the configured network on the
+  // device, and the error word its kernels set when a wait gives up
+  gm::mlp::DevNet net;
+  bool learned = false;
+  int* mlp_err = nullptr;
 };
 
 namespace {
@@ -206,7 +212,10 @@ gm_status build_devcfg(gm_ctx* ctx, const gm_config& c, gm::DevCfg* d) {
   d->slight_per_pixel = c.slight_per_pixel ? 1 : 0;
   d->lambda_per_pixel = c.lambda_per_pixel ? 1 : 0;
   d->lam_map = nullptr;   // bound per call
-  d->init_mode = c.init_mode == GM_INIT_CLASSICAL ? 0 : 1;
+  if (c.init_mode < GM_INIT_CLASSICAL || c.init_mode > GM_INIT_LEARNED)
+    return fail(ctx, GM_ERR_INVALID, "unknown init_mode");
+  // the learned guess competes with the classical start: both need the pre-pass
+  d->init_mode = (c.init_mode == GM_INIT_CLASSICAL || c.init_mode == GM_INIT_LEARNED) ? 0 : 1;
   d->miter = c.miter;
   d->logclambda = c.logclambda;
   d->quirks = c.reference_quirks;
@@ -324,6 +333,8 @@ gm_status gm_create(int device, size_t hbm_budget, gm_ctx** out) {
   cudaEventCreate(&ctx->ev1);
   if (cudaMalloc(&ctx->work, sizeof(gm::WorkCounters)) != cudaSuccess) return GM_ERR_NOMEM;
   if (cudaMalloc(&ctx->work2, sizeof(gm::WorkCounters)) != cudaSuccess) return GM_ERR_NOMEM;
+  if (cudaMalloc(&ctx->mlp_err, sizeof(int) * 4) != cudaSuccess) return GM_ERR_NOMEM;
+  cudaMemset(ctx->mlp_err, 0, sizeof(int) * 4);
   if (cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking) != cudaSuccess) return GM_ERR_CUDA;
   cudaEventCreateWithFlags(&ctx->evx0, cudaEventDisableTiming);
   cudaEventCreateWithFlags(&ctx->evx1, cudaEventDisableTiming);
@@ -348,6 +359,8 @@ gm_status gm_destroy(gm_ctx* ctx) {
   if (ctx->aux) cudaStreamSynchronize(ctx->aux);
   if (ctx->work) cudaFree(ctx->work);
   if (ctx->work2) cudaFree(ctx->work2);
+  gm::mlp::devnet_destroy(&ctx->net);
+  if (ctx->mlp_err) cudaFree(ctx->mlp_err);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   if (ctx->evx0) cudaEventDestroy(ctx->evx0);
@@ -380,7 +393,24 @@ gm_status gm_configure(gm_ctx* ctx, const gm_config* cfg) {
     if (e != cudaSuccess) return cuda_fail(ctx, e, "stray-light upload");
     d.slight = (const float*)ctx->slight.p;
   }
+  if (cfg->init_mode == GM_INIT_LEARNED) {
+    const gm_mlp* net = cfg->mlp;
+    if (!net) return fail(ctx, GM_ERR_INVALID, "GM_INIT_LEARNED needs gm_config.mlp");
+    if (net->abi_version != GM_ABI_VERSION) return fail(ctx, GM_ERR_INVALID, "gm_mlp.abi_version mismatch");
+    if (net->nl != cfg->nl || 4 * cfg->nl > GM_MLP_IN)
+      return fail(ctx, GM_ERR_INVALID, "the network was made for another grid (its nl differs, or nl > 32)");
+    if (cfg->lambda_per_pixel)
+      return fail(ctx, GM_ERR_UNSUPPORTED, "the learned guess reads one grid, not per-pixel grids");
+    cudaError_t e = gm::mlp::devnet_create(&ctx->net, net, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "learned initial guess upload");
+    ctx->learned = true;
+  } else {
+    gm::mlp::devnet_destroy(&ctx->net);
+    ctx->learned = false;
+  }
   ctx->cfg = *cfg;
+  ctx->cfg.mlp = nullptr;                                  // the network now lives on the device
   if (!cfg->slight_per_pixel) ctx->cfg.slight = nullptr;   // the global profile now lives on the device
   ctx->dev = d;
   ctx->configured = true;
@@ -436,9 +466,32 @@ static gm_status wave_buffers(gm_ctx* ctx, const char* name, const gm::DevCfg& d
 // starts after the caller's prior work and the caller's stream waits for it
 // at the end, so the call stays ordered on the caller's stream.  outs[0..n)
 // are the per-pixel outputs (per-pixel size = bytes / npix).
+// Start models of a learned-guess inversion (after the classical pre-pass
+// wrote `models` and `status`): the network's guesses into `scratch`, then
+// per pixel the one with the lower chi2.
+static cudaError_t learned_starts(gm_ctx* ctx, const gm::DevCfg& d, const float* iquv, int64_t n, double* models,
+                                  double* scratch, uint32_t* status, cudaStream_t s) {
+  int fix[GM_NPAR];
+  for (int i = 0; i < GM_NPAR; ++i) fix[i] = d.fix[i];
+  cudaError_t e = gm::mlp::predict(ctx->net, iquv, n, d.nl, ctx->cfg.init_model, fix, scratch, ctx->mlp_err, s);
+  if (e == cudaSuccess) e = gm::launch_select_init(d, iquv, n, models, scratch, status, s);
+  return e;
+}
+
+// After a synchronised call that ran the learned guess: did one of its
+// kernels give up waiting?
+static gm_status learned_check(gm_ctx* ctx) {
+  int code = 0;
+  if (cudaMemcpy(&code, ctx->mlp_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess || code != 0) {
+    cudaMemset(ctx->mlp_err, 0, sizeof(int));
+    return fail(ctx, GM_ERR_CUDA, "a learned-guess kernel gave up waiting for its tensor-core work");
+  }
+  return GM_OK;
+}
+
 static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::InvertArgs& ia,
                                const float* iquv, const Arg& a_in, const Arg* const* outs, int nouts,
-                               int64_t npix, int nl, bool prepass, size_t need, cudaStream_t s) {
+                               int64_t npix, int nl, bool prepass, double* learned, size_t need, cudaStream_t s) {
   const size_t row = 4 * (size_t)nl;
   // two chunks or more, of at least four times kPipeChunk when there are
   // more than two: the wave kernels prefer long launches
@@ -476,6 +529,9 @@ static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::Inver
     if (prepass) {
       e = gm::launch_classical(dc, c.iquv, n, const_cast<double*>(c.init_models),
                                const_cast<uint32_t*>(c.init_status), true, q);
+      if (e == cudaSuccess && learned)
+        e = learned_starts(ctx, dc, c.iquv, n, const_cast<double*>(c.init_models), learned + a * 11,
+                           const_cast<uint32_t*>(c.init_status), q);
       if (e != cudaSuccess) break;
       dc.init_mode = 1;
     }
@@ -483,10 +539,10 @@ static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::Inver
     if (waves) {
       int nk = 0;
       e = gm::launch_invert_waves(dc, c, wb[k & 1], q, &nk);
-      launches += nk + (prepass ? 1 : 0);
+      launches += nk + (prepass ? 1 : 0) + (learned ? 2 : 0);
     } else {
       e = gm::launch_invert(dc, c, (int)grid, q);
-      launches += 1 + (prepass ? 1 : 0);
+      launches += 1 + (prepass ? 1 : 0) + (learned ? 2 : 0);
     }
     ctx->stats.grid_blocks = (int)grid;
     ctx->stats.block_threads = geo.threads;
@@ -535,9 +591,10 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   // classical estimates of the start models in a pre-pass kernel, so that
   // their code stays out of the inversion kernel's instruction stream
   const bool prepass = dcfg.init_mode == 0 && !init_models;
+  const bool learned = prepass && ctx->learned && !so;
   size_t need = cube + (fitted ? cube : 0) + (size_t)npix * (11 * 12 + 16) +
                 (dcfg.lambda_per_pixel ? sizeof(double) * (size_t)nl * npix : 0) +
-                (prepass ? (size_t)npix * (11 * 8 + 4) : 0);
+                (prepass ? (size_t)npix * (11 * 8 + 4) : 0) + (learned ? (size_t)npix * 11 * 8 : 0);
   if (need > ctx->budget) return fail(ctx, GM_ERR_NOMEM, "request exceeds the context's HBM budget");
   Arg a_in, a_init, a_sl, a_lam, a_model, a_m64, a_chi, a_it, a_acc, a_fit, a_st;
   gm_status st;
@@ -603,15 +660,30 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
     ia.init_models = (const double*)mp;
     ia.init_status = (const uint32_t*)sp;
   }
+  double* lguess = nullptr;
+  if (learned) {
+    void* lp = nullptr;
+    if ((st = ensure_buf(ctx, "linit", sizeof(double) * 11 * npix, &lp)) != GM_OK) return st;
+    lguess = (double*)lp;
+    cudaMemsetAsync(ctx->mlp_err, 0, sizeof(int), s);
+  }
   const Arg* outs[] = {&a_model, &a_m64, &a_chi, &a_it, &a_acc, &a_fit, &a_st,
                        &a_sd, &a_strial, &a_sc0, &a_sc1};
-  if (pipeline) return invert_chunks(ctx, d, ia, iquv, a_in, outs, 7, npix, nl, prepass, need, s);
+  if (pipeline) {
+    st = invert_chunks(ctx, d, ia, iquv, a_in, outs, 7, npix, nl, prepass, lguess, need, s);
+    return (st == GM_OK && learned) ? learned_check(ctx) : st;
+  }
   cudaError_t e = cudaMemsetAsync(ctx->work, 0, sizeof(gm::WorkCounters), s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "work counter reset");
   if (prepass) {
     e = gm::launch_classical(d, ia.iquv, npix, const_cast<double*>(ia.init_models),
                              const_cast<uint32_t*>(ia.init_status), true, s);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "classical-estimates pre-pass");
+    if (learned) {
+      e = learned_starts(ctx, d, ia.iquv, npix, const_cast<double*>(ia.init_models), lguess,
+                         const_cast<uint32_t*>(ia.init_status), s);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "learned initial guess");
+    }
     d.init_mode = 1;
   }
   gm::InvertGeometry geo;
@@ -628,7 +700,7 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   ctx->stats.grid_blocks = (int)grid;
   ctx->stats.block_threads = geo.threads;
   ctx->stats.warps_per_block = geo.threads / 32;
-  ctx->stats.kernel_launches = launches + (prepass ? 1 : 0);
+  ctx->stats.kernel_launches = launches + (prepass ? 1 : 0) + (learned ? 2 : 0);
   ctx->stats.pixels = npix;
   bool any_host = false;
   for (const Arg* o : outs) {
@@ -648,6 +720,7 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
     cudaMemcpy(&wc, ctx->work, sizeof(wc), cudaMemcpyDeviceToHost);
     ctx->stats.iterations = (int64_t)wc.iterations;
     ctx->stats.accepted = (int64_t)wc.accepted;
+    if (learned) return learned_check(ctx);
   }
   return GM_OK;
 }
@@ -945,6 +1018,8 @@ gm_status gm_submit(gm_ctx* ctx, const gm_request* req, gm_ticket* ticket) {
     return fail(ctx, GM_ERR_UNSUPPORTED, "serving takes one stray-light profile, not a per-pixel map");
   if (ctx->dev.lambda_per_pixel)
     return fail(ctx, GM_ERR_UNSUPPORTED, "serving takes one wavelength grid, not per-pixel grids");
+  if (ctx->learned)
+    return fail(ctx, GM_ERR_UNSUPPORTED, "serving starts from the classical estimates, not the learned guess");
   auto r = std::make_shared<Request>();
   r->req = *req;
   r->dev = ctx->dev;
@@ -1186,6 +1261,123 @@ void serve_loop(gm_ctx* ctx) {
 
 }  // namespace
 
+// ---------------------------------------------------------------- learned initial guess
+extern "C" {
+
+gm_status gm_mlp_init(gm_mlp* net, int nl, uint64_t seed) {
+  if (!net || nl < 1 || 4 * nl > GM_MLP_IN) return GM_ERR_INVALID;
+  gm::mlp::init_net(net, nl, seed);
+  return GM_OK;
+}
+
+void gm_mlp_train_defaults(gm_mlp_train_opts* o) {
+  if (!o) return;
+  o->epochs = 8;
+  o->batch = 16384;
+  o->lr = 2e-3f;
+  o->weight_decay = 0.f;
+  o->seed = 1;
+}
+
+}  // extern "C"
+
+// Training and gradients: the data staged onto the device when they are in
+// host memory, then the training driver on the context's stream.
+static gm_status mlp_train_impl(gm_ctx* ctx, gm_mlp* net, const float* iquv, const double* truth, int64_t n,
+                                const gm_mlp_train_opts* o, float* loss, gm_mlp* grads, bool grads_only) {
+  if (!ctx || !net || !iquv || !truth || n <= 0) return ctx ? fail(ctx, GM_ERR_INVALID, "bad argument") : GM_ERR_INVALID;
+  if (net->abi_version != GM_ABI_VERSION) return fail(ctx, GM_ERR_INVALID, "gm_mlp.abi_version mismatch");
+  if (net->nl < 1 || 4 * net->nl > GM_MLP_IN) return fail(ctx, GM_ERR_INVALID, "the network's nl must be 1..32");
+  std::lock_guard<std::mutex> lk(ctx->call_mu);
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const int nl = net->nl;
+  Arg a_in, a_t;
+  gm_status st;
+  if ((st = stage_in(ctx, "mlp_iquv", iquv, sizeof(float) * 4 * (size_t)nl * n, &a_in, s)) != GM_OK) return st;
+  if ((st = stage_in(ctx, "mlp_truth", truth, sizeof(double) * 11 * (size_t)n, &a_t, s)) != GM_OK) return st;
+  gm_mlp_train_opts def;
+  gm_mlp_train_defaults(&def);
+  if (!o) o = &def;
+  gm::mlp::TrainArgs ta{};
+  ta.iquv = (const float*)a_in.dev;
+  ta.truth = (const double*)a_t.dev;
+  ta.n = n;
+  ta.nl = nl;
+  ta.epochs = o->epochs;
+  ta.batch = o->batch;
+  ta.lr = o->lr;
+  ta.weight_decay = o->weight_decay;
+  ta.seed = o->seed;
+  ta.grads_only = grads_only;
+  cudaMemsetAsync(ctx->mlp_err, 0, sizeof(int), s);
+  const char* why = nullptr;
+  cudaError_t e = gm::mlp::train(net, ta, loss, grads, ctx->mlp_err, s, &why);
+  if (e == cudaErrorInvalidValue && why) return fail(ctx, GM_ERR_INVALID, why);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, why ? why : "training");
+  return GM_OK;
+}
+
+extern "C" {
+
+gm_status gm_mlp_train(gm_ctx* ctx, gm_mlp* net, const float* iquv, const double* truth, int64_t n,
+                       const gm_mlp_train_opts* opts, float* loss_per_epoch) {
+  return mlp_train_impl(ctx, net, iquv, truth, n, opts, loss_per_epoch, nullptr, false);
+}
+
+gm_status gm_mlp_gradients(gm_ctx* ctx, const gm_mlp* net, const float* iquv, const double* truth, int64_t n,
+                           gm_mlp* grads, float* loss) {
+  if (!grads) return ctx ? fail(ctx, GM_ERR_INVALID, "grads is NULL") : GM_ERR_INVALID;
+  gm_mlp copy = net ? *net : gm_mlp{};
+  if (n % gm::mlp::kTile) return ctx ? fail(ctx, GM_ERR_INVALID, "n must be a multiple of 128") : GM_ERR_INVALID;
+  gm_mlp_train_opts o;
+  gm_mlp_train_defaults(&o);
+  o.batch = (int)n;
+  o.epochs = 1;
+  float l = 0.f;
+  gm_status st = mlp_train_impl(ctx, net ? &copy : nullptr, iquv, truth, n, &o, &l, grads, true);
+  if (st == GM_OK && loss) *loss = l;
+  return st;
+}
+
+gm_status gm_mlp_predict(gm_ctx* ctx, const gm_mlp* net, const float* iquv, int64_t n, double* models,
+                         void* stream) {
+  if (!ctx) return GM_ERR_INVALID;
+  if (!net || !iquv || !models || n < 0) return fail(ctx, GM_ERR_INVALID, "bad argument");
+  if (!ctx->configured) return fail(ctx, GM_ERR_NOT_CONFIGURED, "gm_configure first");
+  if (net->abi_version != GM_ABI_VERSION) return fail(ctx, GM_ERR_INVALID, "gm_mlp.abi_version mismatch");
+  if (net->nl != ctx->dev.nl || 4 * net->nl > GM_MLP_IN)
+    return fail(ctx, GM_ERR_INVALID, "the network was made for another grid");
+  if (n == 0) return GM_OK;
+  std::lock_guard<std::mutex> lk(ctx->call_mu);
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  const int nl = net->nl;
+  Arg a_in, a_out;
+  gm_status st;
+  if ((st = stage_in(ctx, "iquv", iquv, sizeof(float) * 4 * (size_t)nl * n, &a_in, s)) != GM_OK) return st;
+  if ((st = stage_out(ctx, "pmodels", models, sizeof(double) * 11 * (size_t)n, &a_out)) != GM_OK) return st;
+  gm::mlp::DevNet d;
+  cudaError_t e = gm::mlp::devnet_create(&d, net, s);
+  int fix[GM_NPAR];
+  for (int i = 0; i < GM_NPAR; ++i) fix[i] = ctx->dev.fix[i];
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->mlp_err, 0, sizeof(int), s);
+  if (e == cudaSuccess)
+    e = gm::mlp::predict(d, (const float*)a_in.dev, n, nl, ctx->cfg.init_model, fix, (double*)a_out.dev,
+                         ctx->mlp_err, s);
+  if (e == cudaSuccess && (st = copy_back(ctx, a_out, s)) != GM_OK) {
+    gm::mlp::devnet_destroy(&d);
+    return st;
+  }
+  // the network's device copy is released with the call
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  gm::mlp::devnet_destroy(&d);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "learned initial guess");
+  return learned_check(ctx);
+}
+
+}  // extern "C"
+
 // ---------------------------------------------------------------- no-alloc inversion
 // Scratch of gm_invert_noalloc: the work-stealing counters at offset 0 and the
 // global stray-light profile [4][nl] at offset 256.  A file-scope device array
@@ -1241,7 +1433,7 @@ extern "C" gm_status gm_invert_noalloc(const gm_config* cfg, const float* iquv, 
   gm_status st = build_devcfg(nullptr, *cfg, &d);
   if (st != GM_OK) return st;
   if (nl != d.nl) return GM_ERR_INVALID;
-  if (d.lambda_per_pixel) return GM_ERR_UNSUPPORTED;
+  if (d.lambda_per_pixel || cfg->init_mode == GM_INIT_LEARNED) return GM_ERR_UNSUPPORTED;
   const bool global_slight = d.use_slight && !d.slight_per_pixel;
   const size_t need = kNoallocSlightOffset + (global_slight ? sizeof(float) * 4 * (size_t)nl : 0);
   if (need > GM_NOALLOC_SCRATCH_BYTES) return GM_ERR_INVALID;

@@ -701,6 +701,98 @@ cudaError_t launch_classical(const DevCfg& cfg, const float* iquv, int64_t npix,
   return cudaGetLastError();
 }
 
+// Start models of a learned-guess inversion, one warp per pixel: the
+// classical start (models, from the pre-pass) and the learned guess
+// (learned) are each synthesised with the inversion's forward model (PSF,
+// stray light) and the one with the lower chi2 is kept in models; a learned
+// win sets GM_PIX_LEARNED_INIT in status.  Ties and non-finite chi2 keep the
+// classical start, the reference's own (milosUtils.cu:616-628).
+template <int LPL, int V>
+__global__ void __launch_bounds__(warps_per_block<LPL>() * 32)
+select_init_kernel(const DevCfg c, const float* __restrict__ iquv, int64_t npix, double* models,
+                   const double* __restrict__ learned, uint32_t* status) {
+  const int WPB = warps_per_block<LPL>();
+  const int lane = threadIdx.x & 31;
+  load_taps<LPL>(c);
+  WarpSmem<LPL, V>& sm = warp_smem<LPL, V>();
+  init_rows<LPL, V>(c, sm, lane);
+  const int nl = c.nl;
+  float dlv[LPL];
+  double dld[LPL];
+  bool valid[LPL];
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+    valid[k] = l < nl;
+    dlv[k] = valid[k] ? c.dl[l] : 0.f;
+    dld[k] = 0.0;
+  }
+  float slg[LPL][4];
+  if (c.use_slight && !c.slight_per_pixel) load_pixel<LPL>(c.slight, nl, lane, slg);
+  else {
+#pragma unroll
+    for (int k = 0; k < LPL; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
+  }
+  const int64_t wid = (int64_t)blockIdx.x * WPB + (threadIdx.x >> 5);
+  const int64_t nw = (int64_t)gridDim.x * WPB;
+  for (int64_t pix = wid; pix < npix; pix += nw) {
+    const size_t off = (size_t)pix * 4 * nl;
+    float ob[LPL][4];
+    load_pixel<LPL>(iquv + off, nl, lane, ob);
+    if (c.use_slight && c.slight_per_pixel) load_pixel<LPL>(c.slight + off, nl, lane, slg);
+    float chi[2];
+#pragma unroll 1
+    for (int k = 0; k < 2; ++k) {
+      if (lane < 11) sm.m[lane] = (k == 0 ? models : learned)[pix * 11 + lane];
+      __syncwarp();
+      Lane<LPL, V> ln;
+      Angles an;
+      float syn[LPL][4], pure[LPL][4];
+      synth_lane<LPL, V>(c, sm.m, dlv, lane, ln, an, syn, pure, slg, sm);
+      chi[k] = chisq<LPL>(c, syn, ob, valid);
+      __syncwarp();
+    }
+    if (isfinite(chi[1]) && (!isfinite(chi[0]) || chi[1] < chi[0])) {
+      if (lane < 11) models[pix * 11 + lane] = learned[pix * 11 + lane];
+      if (lane == 0) status[pix] |= GM_PIX_LEARNED_INIT;
+    }
+    __syncwarp();
+  }
+}
+
+template <int LPL, int V>
+cudaError_t launch_select_t(const DevCfg& cfg, const float* iquv, int64_t npix, double* models,
+                            const double* learned, uint32_t* status, cudaStream_t s) {
+  const size_t bytes = tap_bytes<LPL>() + sizeof(WarpSmem<LPL, V>) * warps_per_block<LPL>();
+  cudaError_t e = cudaFuncSetAttribute(select_init_kernel<LPL, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)bytes);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t need = (npix + warps_per_block<LPL>() - 1) / warps_per_block<LPL>();
+  const int grid = (int)(need < (int64_t)sms * 16 ? (need < 1 ? 1 : need) : (int64_t)sms * 16);
+  select_init_kernel<LPL, V><<<grid, warps_per_block<LPL>() * 32, bytes, s>>>(cfg, iquv, npix, models, learned,
+                                                                             status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_select_init(const DevCfg& cfg, const float* iquv, int64_t npix, double* models,
+                               const double* learned, uint32_t* status, cudaStream_t s) {
+  if (npix <= 0) return cudaSuccess;
+  const int v = kernel_variant(cfg, false);
+  if (cfg.nl <= 32) {
+    if (v == 0) return launch_select_t<1, 0>(cfg, iquv, npix, models, learned, status, s);
+    if (v == 1) return launch_select_t<1, 1>(cfg, iquv, npix, models, learned, status, s);
+    return launch_select_t<1, 2>(cfg, iquv, npix, models, learned, status, s);
+  }
+  if (v == 0) return launch_select_t<2, 0>(cfg, iquv, npix, models, learned, status, s);
+  if (v == 1) return launch_select_t<2, 1>(cfg, iquv, npix, models, learned, status, s);
+  return launch_select_t<2, 2>(cfg, iquv, npix, models, learned, status, s);
+}
+
 // Pure ME profiles (no PSF, no stray light) on an arbitrary offset grid, one
 // thread per (pixel, sample): used to synthesise observations on fine grids.
 __global__ void synth_grid_kernel(const DevCfg c, const double* __restrict__ models, int64_t npix,

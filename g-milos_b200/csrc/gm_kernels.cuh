@@ -136,6 +136,11 @@ cudaError_t launch_classical(const DevCfg& cfg, const float* iquv, int64_t npix,
                              uint32_t* status, bool for_init, cudaStream_t s);
 cudaError_t launch_synth_grid(const DevCfg& cfg, const double* models, int64_t npix,
                               const double* offsets, int ngrid, float* out, cudaStream_t s);
+// learned-guess inversions: per pixel the start model with the lower chi2 of
+// models (classical, in/out) and learned; GM_PIX_LEARNED_INIT in status when
+// the learned one is kept
+cudaError_t launch_select_init(const DevCfg& cfg, const float* iquv, int64_t npix, double* models,
+                               const double* learned, uint32_t* status, cudaStream_t s);
 // kernel variant for a configuration (0: 10 terms, 1: 10 terms with
 // macroturbulence, 2: 11 terms); per_pixel_init: start models given per pixel
 int kernel_variant(const DevCfg& cfg, bool per_pixel_init);

@@ -29,7 +29,9 @@ PIX_CHI2_EXIT = 0x08
 PIX_NONFINITE = 0x10
 PIX_BAD_INPUT = 0x20
 
-INIT_CLASSICAL, INIT_GIVEN, INIT_PER_PIXEL = 0, 1, 2
+INIT_CLASSICAL, INIT_GIVEN, INIT_PER_PIXEL, INIT_LEARNED = 0, 1, 2, 3
+PIX_LEARNED_INIT = 0x40
+MLP_IN, MLP_HIDDEN, MLP_OUT, MLP_OUT_PAD = 128, 256, 9, 16
 NUMERICS_REFERENCE, NUMERICS_ACCURATE = 0, 1
 KERNEL_AUTO, KERNEL_FUSED = 0, 1
 
@@ -38,7 +40,8 @@ EXPORTS = ("gm_create", "gm_destroy", "gm_last_error", "gm_status_string", "gm_c
            "gm_configure", "gm_invert", "gm_invert_ex", "gm_synthesize", "gm_synthesize_f64",
            "gm_synthesize_grid", "gm_lm_step", "gm_submit", "gm_poll", "gm_cancel", "gm_zeeman_from_levels",
            "gm_psf_gaussian", "gm_psf_from_table", "gm_get_stats", "gm_measure_peaks", "gm_measure_sfu_peak",
-           "gm_invert_noalloc", "gm_classical", "gm_serving_options", "gm_wave_state_bytes")
+           "gm_invert_noalloc", "gm_classical", "gm_serving_options", "gm_wave_state_bytes",
+           "gm_mlp_init", "gm_mlp_train_defaults", "gm_mlp_train", "gm_mlp_gradients", "gm_mlp_predict")
 
 
 class GmError(RuntimeError):
@@ -54,6 +57,30 @@ class Zeeman(C.Structure):
                 ("gl", C.c_float), ("gu", C.c_float), ("geff", C.c_float), ("fo", C.c_float)]
 
 
+class Mlp(C.Structure):
+    """gm_mlp: the learned initial guess (FP32 parameters, standardisation)."""
+    _fields_ = [("abi_version", C.c_int), ("nl", C.c_int), ("steps", C.c_int64),
+                ("in_mean", C.c_float * MLP_IN), ("in_scale", C.c_float * MLP_IN),
+                ("out_mean", C.c_float * MLP_OUT_PAD), ("out_scale", C.c_float * MLP_OUT_PAD),
+                ("w1", (C.c_float * MLP_IN) * MLP_HIDDEN), ("b1", C.c_float * MLP_HIDDEN),
+                ("w2", (C.c_float * MLP_HIDDEN) * MLP_HIDDEN), ("b2", C.c_float * MLP_HIDDEN),
+                ("w3", (C.c_float * MLP_HIDDEN) * MLP_OUT), ("b3", C.c_float * MLP_OUT_PAD)]
+
+    def arrays(self):
+        """numpy views (no copies) of the parameters and standardisation."""
+        a = lambda name, shape: np.ctypeslib.as_array(getattr(self, name)).reshape(shape)
+        return {"in_mean": a("in_mean", (MLP_IN,)), "in_scale": a("in_scale", (MLP_IN,)),
+                "out_mean": a("out_mean", (MLP_OUT_PAD,)), "out_scale": a("out_scale", (MLP_OUT_PAD,)),
+                "w1": a("w1", (MLP_HIDDEN, MLP_IN)), "b1": a("b1", (MLP_HIDDEN,)),
+                "w2": a("w2", (MLP_HIDDEN, MLP_HIDDEN)), "b2": a("b2", (MLP_HIDDEN,)),
+                "w3": a("w3", (MLP_OUT, MLP_HIDDEN)), "b3": a("b3", (MLP_OUT_PAD,))}
+
+
+class TrainOpts(C.Structure):
+    _fields_ = [("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_float), ("weight_decay", C.c_float),
+                ("seed", C.c_uint64)]
+
+
 class Config(C.Structure):
     _fields_ = [("abi_version", C.c_int), ("nl", C.c_int), ("lambda0", C.c_double),
                 ("lambda_", C.c_double * MAX_NL), ("zeeman", Zeeman), ("use_psf", C.c_int),
@@ -64,7 +91,8 @@ class Config(C.Structure):
                 ("use_slight", C.c_int), ("slight_per_pixel", C.c_int),
                 ("slight", C.POINTER(C.c_float)), ("reference_quirks", C.c_int),
                 ("numerics", C.c_int), ("lambda_per_pixel", C.c_int),
-                ("lambda_map", C.POINTER(C.c_double)), ("kernel", C.c_int)]
+                ("lambda_map", C.POINTER(C.c_double)), ("kernel", C.c_int),
+                ("mlp", C.POINTER(Mlp))]
 
 
 class Request(C.Structure):
@@ -120,6 +148,12 @@ def lib():
         L.gm_invert_noalloc.argtypes = [C.POINTER(Config), vp, i64, C.c_int, vp, vp, vp, vp, vp, vp]
         L.gm_wave_state_bytes.argtypes = [C.c_int, C.c_int, i64]
         L.gm_wave_state_bytes.restype = C.c_size_t
+        L.gm_mlp_init.argtypes = [C.POINTER(Mlp), C.c_int, C.c_uint64]
+        L.gm_mlp_train_defaults.argtypes = [C.POINTER(TrainOpts)]
+        L.gm_mlp_train_defaults.restype = None
+        L.gm_mlp_train.argtypes = [vp, C.POINTER(Mlp), vp, vp, i64, C.POINTER(TrainOpts), vp]
+        L.gm_mlp_gradients.argtypes = [vp, C.POINTER(Mlp), vp, vp, i64, C.POINTER(Mlp), C.POINTER(C.c_float)]
+        L.gm_mlp_predict.argtypes = [vp, C.POINTER(Mlp), vp, i64, vp, vp]
         _lib = L
     return _lib
 
@@ -181,6 +215,13 @@ def psf_gaussian(fwhm_mA, lam):
     return out
 
 
+def mlp_new(nl, seed=0):
+    """A fresh learned-guess network for grids of nl samples (gm_mlp_init)."""
+    net = Mlp()
+    _check(lib().gm_mlp_init(C.byref(net), int(nl), int(seed)))
+    return net
+
+
 def wave_state_bytes(nl, miter, pixels):
     """Device bytes of wave-kernel LM state for a chunk of `pixels` pixels
     (gm_wave_state_bytes): what an HBM budget must leave room for."""
@@ -200,13 +241,13 @@ def make_config(lam, lambda0, zeeman, psf=None, mu=1.0, weight=(1, 1, 1, 1), noi
                 fix=(1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0), init=None, init_mode=INIT_CLASSICAL,
                 miter=50, ilambda=0.1, toplim=1e-12, logclambda=0, stop_dchi2=0.0,
                 slight=None, slight_per_pixel=False, reference_quirks=1, numerics=0,
-                lambda_map=None, kernel=KERNEL_AUTO):
+                lambda_map=None, kernel=KERNEL_AUTO, mlp=None):
     """Engine configuration (gm_config).  lambda_map: optional per-pixel
     wavelength grids [P][nl] (absolute, A; numpy or a CUDA tensor of float64),
     read at each call like a per-pixel stray map; `lam` then only sizes the
     grid and the PSF stays `psf`.  kernel: KERNEL_AUTO (wave-synchronous
     kernels where they cover the call) or KERNEL_FUSED (the fused kernel for
-    every call)."""
+    every call).  mlp: a trained Mlp for init_mode INIT_LEARNED."""
     c = Config()
     lib().gm_config_defaults(C.byref(c))
     lam = np.asarray(lam, dtype=np.float64)
@@ -239,6 +280,9 @@ def make_config(lam, lambda0, zeeman, psf=None, mu=1.0, weight=(1, 1, 1, 1), noi
     c.reference_quirks = reference_quirks
     c.numerics = numerics
     c.kernel = kernel
+    c._mlp_ref = mlp
+    if mlp is not None:
+        c.mlp = C.pointer(mlp)
     c._slight_ref = None
     c._lambda_ref = None
     if lambda_map is not None:
@@ -449,6 +493,39 @@ class Engine:
         a = C.c_double()
         _check(lib().gm_measure_sfu_peak(self._ctx, C.byref(a)), self._ctx)
         return a.value
+
+    # ------------------------------------------------------- learned guess
+    def mlp_train(self, net, iquv, truth, epochs=8, batch=16384, lr=2e-3, weight_decay=0.0, seed=1):
+        """Train `net` (an Mlp, in place) on profiles iquv [n][4][nl] and the
+        models that made them, truth [n][11] (numpy or CUDA tensors).
+        Returns the mean loss of each epoch."""
+        o = TrainOpts()
+        lib().gm_mlp_train_defaults(C.byref(o))
+        o.epochs, o.batch, o.lr, o.weight_decay, o.seed = int(epochs), int(batch), float(lr), float(weight_decay), \
+            int(seed)
+        loss = np.zeros(max(1, int(epochs)), dtype=np.float32)
+        _check(lib().gm_mlp_train(self._ctx, C.byref(net), _ptr(iquv), _ptr(truth), int(iquv.shape[0]),
+                                  C.byref(o), _ptr(loss)), self._ctx)
+        return loss
+
+    def mlp_gradients(self, net, iquv, truth):
+        """(loss, gradients as an Mlp) of one batch (n a multiple of 128)."""
+        g = Mlp()
+        loss = C.c_float()
+        _check(lib().gm_mlp_gradients(self._ctx, C.byref(net), _ptr(iquv), _ptr(truth), int(iquv.shape[0]),
+                                      C.byref(g), C.byref(loss)), self._ctx)
+        return loss.value, g
+
+    def mlp_predict(self, net, iquv):
+        """Start models [n][11] (float64) the network predicts for iquv."""
+        n = int(iquv.shape[0])
+        if hasattr(iquv, "data_ptr"):
+            import torch
+            out = torch.empty((n, NPAR), dtype=torch.float64, device=iquv.device)
+        else:
+            out = np.empty((n, NPAR), dtype=np.float64)
+        _check(lib().gm_mlp_predict(self._ctx, C.byref(net), _ptr(iquv), n, _ptr(out), None), self._ctx)
+        return out
 
     def stats(self):
         s = Stats()

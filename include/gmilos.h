@@ -65,13 +65,47 @@ typedef enum {
 #define GM_PIX_CHI2_EXIT     0x08u  /* stopped by the relative-chi2 or chi2 < 1e-4 rule */
 #define GM_PIX_NONFINITE     0x10u  /* final chi2 not finite */
 #define GM_PIX_BAD_INPUT     0x20u  /* no valid continuum sample in Stokes I */
+#define GM_PIX_LEARNED_INIT  0x40u  /* the start model came from the learned initial guess
+                                       (its chi2 beat the classical start's) */
 
 typedef enum {
     GM_INIT_CLASSICAL = 0,    /* reference: guess model + classical estimates of B, vlos,
                                  gamma, phi (milosUtils.cu:616-628) */
     GM_INIT_GIVEN = 1,        /* guess model as given, no estimates */
-    GM_INIT_PER_PIXEL = 2     /* caller supplies init_models [P][11] to gm_invert_ex */
+    GM_INIT_PER_PIXEL = 2,    /* caller supplies init_models [P][11] to gm_invert_ex */
+    GM_INIT_LEARNED = 3       /* per pixel the better (lower chi2) of the classical start
+                                 and the learned initial guess gm_config.mlp; no
+                                 counterpart in the reference */
 } gm_init_mode;
+
+/* Learned initial guess: a multilayer perceptron 4 nl -> 256 -> 256 -> 9
+ * (GELU), nl <= 32 (120 inputs on the 30-sample grid), that maps a pixel's
+ * Stokes profiles to a start model.  Inputs are the profiles [4][nl] in the
+ * cube's order, standardised per feature (x' = (x - in_mean) * in_scale,
+ * zero past 4 nl).  The 9 outputs, standardised the same way (y = y' *
+ * out_scale + out_mean), are eta0, vlos [km/s], Doppler width [A], damping,
+ * S0, S1, and the field as B cos gamma, B sin gamma cos 2 phi,
+ * B sin gamma sin 2 phi [G] (continuous across the 180-degree azimuth
+ * ambiguity).  The parameters are kept in FP32 here; the engine's kernels
+ * compute with BF16 copies of the weights and FP32 accumulation on the
+ * tensor cores.  No counterpart in the reference. */
+#define GM_MLP_IN 128
+#define GM_MLP_HIDDEN 256
+#define GM_MLP_OUT 9
+#define GM_MLP_OUT_PAD 16
+typedef struct {
+    int abi_version;                              /* GM_ABI_VERSION */
+    int nl;                                       /* samples per Stokes parameter read */
+    int64_t steps;                                /* optimiser steps taken */
+    float in_mean[GM_MLP_IN], in_scale[GM_MLP_IN];
+    float out_mean[GM_MLP_OUT_PAD], out_scale[GM_MLP_OUT_PAD];
+    float w1[GM_MLP_HIDDEN][GM_MLP_IN];           /* [out][in], inputs past 4 nl unused */
+    float b1[GM_MLP_HIDDEN];
+    float w2[GM_MLP_HIDDEN][GM_MLP_HIDDEN];
+    float b2[GM_MLP_HIDDEN];
+    float w3[GM_MLP_OUT][GM_MLP_HIDDEN];
+    float b3[GM_MLP_OUT_PAD];
+} gm_mlp;
 
 /* Zeeman pattern of the line (Cuantic, defines.h:108-123) */
 typedef struct {
@@ -123,6 +157,8 @@ typedef struct {
                                      fused kernel; GM_KERNEL_FUSED: the fused
                                      persistent kernel for every call (the kernel
                                      of gm_invert_noalloc) */
+    const gm_mlp *mlp;            /* network of GM_INIT_LEARNED (host memory, copied
+                                     at gm_configure; its nl must be the grid's) */
 } gm_config;
 
 /* Inversion kernels (gm_config.kernel).  Both execute the same LM arithmetic;
@@ -313,6 +349,48 @@ gm_status gm_measure_sfu_peak(gm_ctx *ctx, double *gops);
  * worth, else the fused kernel runs).  0 for nl outside 1..GM_MAX_NL or a
  * negative count.  No counterpart in the reference; needs no device. */
 size_t gm_wave_state_bytes(int nl, int miter, int64_t pixels);
+
+/* ---------------- learned initial guess (no reference counterpart) -------- */
+/* A fresh network for grids of nl samples (nl <= 32): identity
+ * standardisation, weights drawn from `seed` (uniform, variance 2 / fan-in),
+ * zero biases.  Host only, needs no device. */
+gm_status gm_mlp_init(gm_mlp *net, int nl, uint64_t seed);
+
+typedef struct {
+    int epochs;                   /* passes over the training set (default 8) */
+    int batch;                    /* pixels per optimiser step, a multiple of 128
+                                     (default 16384) */
+    float lr;                     /* peak Adam learning rate, cosine decay to 0
+                                     (default 2e-3) */
+    float weight_decay;           /* decoupled (AdamW) decay (default 0) */
+    uint64_t seed;                /* shuffling */
+} gm_mlp_train_opts;
+void gm_mlp_train_defaults(gm_mlp_train_opts *o);
+
+/* Train `net` in place on n pixels: Stokes profiles iquv [n][4][nl] and the
+ * models that made them, truth [n][11] (Init_Model layout); host or device
+ * memory.  Every forward and backward pass runs on the device in the
+ * engine's own tensor-core kernels (BF16 operands, FP32 accumulation, Adam on
+ * FP32 parameters).  An untrained net (steps == 0) first takes its
+ * standardisation from the data.  loss_per_epoch (optional, [epochs]): mean
+ * squared error of the standardised outputs over each epoch.  n must be at
+ * least one batch. */
+gm_status gm_mlp_train(gm_ctx *ctx, gm_mlp *net, const float *iquv, const double *truth,
+                       int64_t n, const gm_mlp_train_opts *opts, float *loss_per_epoch);
+
+/* Loss and gradients of one batch (n a multiple of 128) without an update,
+ * in `grads` (same layout as the network; its weight and bias arrays are
+ * written).  For checks of the training kernels. */
+gm_status gm_mlp_gradients(gm_ctx *ctx, const gm_mlp *net, const float *iquv, const double *truth,
+                           int64_t n, gm_mlp *grads, float *loss);
+
+/* Start models [n][11] (Init_Model layout) predicted by `net` for the
+ * profiles iquv [n][4][nl]: the 9 outputs mapped back to the model
+ * parameters within the reference's ranges (milosUtils.cu:160-238); v_mac
+ * and the filling factor from the configured guess model.  The context must
+ * be configured on a grid of net->nl samples. */
+gm_status gm_mlp_predict(gm_ctx *ctx, const gm_mlp *net, const float *iquv, int64_t n,
+                         double *models, void *stream);
 
 #ifdef __cplusplus
 }

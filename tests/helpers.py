@@ -101,3 +101,25 @@ def fits_agree(ma, mb):
     |d phi| < 0.1 deg (phi modulo 180) and |d vlos| < 5 m/s."""
     return ((np.abs(ma[:, 1] - mb[:, 1]) < 1.0) & (angle_diff(ma[:, 5], mb[:, 5], 360) < 0.1)
             & (angle_diff(ma[:, 6], mb[:, 6]) < 0.1) & (np.abs(ma[:, 2] - mb[:, 2]) < 0.005))
+
+
+def random_net(seed, nl=30, realistic=True):
+    """A learned-guess network with random weights and biases, standardised
+    (when realistic) to the truth-model distribution so that its outputs land
+    inside the parameter ranges."""
+    import gmilos_b200 as G
+    import mlp_oracle as M
+    net = G.mlp_new(nl, seed)
+    a = net.arrays()
+    rng = np.random.default_rng(seed)
+    a["b1"][:] = rng.normal(0, 0.1, a["b1"].shape)
+    a["b2"][:] = rng.normal(0, 0.1, a["b2"].shape)
+    a["w3"][:] *= 10.0
+    a["b3"][:M.OUT] = rng.normal(0, 0.1, M.OUT)
+    if realistic:
+        t = M.targets(truth_models(4096, rng))
+        a["out_mean"][:M.OUT] = t.mean(axis=0)
+        a["out_scale"][:M.OUT] = t.std(axis=0)
+        a["in_mean"][:4 * nl] = rng.normal(0, 0.1, 4 * nl)
+        a["in_scale"][:4 * nl] = rng.uniform(5, 20, 4 * nl)
+    return net
