@@ -390,6 +390,11 @@ def run_engine(args):
             result["reference_gpu"] = {"unavailable": "oracle/_ref/libgmref_gpu.so not built"}
     if rank == 0 and world == 1 and args.config1:
         result["config1"] = config1_block(eng, args, torch)
+    if rank == 0 and world == 1 and args.ragged_rois > 0:
+        try:
+            result["ragged"] = ragged_block(eng, args, torch)
+        except Exception as exc:  # the block must not take the bench line down
+            result["ragged"] = {"unavailable": str(exc)[:300]}
     if rank == 0 and world == 1 and args.mlp_train_pixels > 0:
         try:
             result["learned_init"] = learned_block(eng, args, torch)
@@ -402,22 +407,26 @@ def run_engine(args):
         dist.destroy_process_group()
 
 
-def serving_latency(eng, obs_h, args):
+def serving_latency(eng, obs_h, args, rate=None, n=None):
     """Serving under load: a Poisson stream of inversion requests, frames of
     side uniform in [side_min, side_max] px x 4 x 30 lambda with PSF and
     stray light, half of them with S0 and S1 fixed (7 ME + alpha free instead
     of 9 + alpha), host buffers in and out (pinned), through the engine's
     continuous-batching entry points (gm_submit / gm_poll).  Latency is
     submit -> results in host memory, taken by the engine.  Frames are cut
-    from the bench cube, tiled when a frame is larger than the cube."""
+    from the bench cube, tiled when a frame is larger than the cube.  Beside
+    the latency percentiles: per frame-size class, and the stretch (latency
+    over the frame's inversion time at the engine's unloaded rate), which
+    takes the frame size out."""
     import torch
-    rng = np.random.default_rng(args.seed + 77)
-    n = args.serve_requests
+    rate = args.serve_rate if rate is None else rate
+    n = args.serve_requests if n is None else n
+    rng = np.random.default_rng(args.seed + 77 + int(rate * 100))
     sides = rng.integers(args.serve_side_min, args.serve_side_max + 1, n)
     npix = (sides.astype(np.int64) ** 2)
     fix7 = (1, 1, 1, 1, 1, 1, 1, 0, 0, 0, 1)
     mixes = [FIX if k % 2 == 0 else fix7 for k in range(n)]
-    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
     P = obs_h.shape[0]
     reps = int(np.ceil(npix.max() / P))
     pool = obs_h if reps <= 1 else torch.cat([obs_h] * reps).pin_memory()
@@ -443,15 +452,62 @@ def serving_latency(eng, obs_h, args):
     t_end = t0 + max(arrivals[k] + lat[k] / 1e3 for k in range(n))
     lat = np.array(lat)
     span = t_end - t0
+    alone_ms = npix / args.serve_unloaded_rate * 1e3
+    stretch = lat / alone_ms
+    edges = np.linspace(args.serve_side_min, args.serve_side_max + 1, 5)
+    classes = []
+    for a, b in zip(edges[:-1], edges[1:]):
+        m = (sides >= a) & (sides < b)
+        if m.sum():
+            classes.append({"sides": [int(a), int(b) - 1], "requests": int(m.sum()),
+                            "p50_ms": float(np.percentile(lat[m], 50)), "p99_ms": float(np.percentile(lat[m], 99))})
     return {"what": "Poisson stream of %d requests at %.2f req/s, frames %d^2-%d^2 px x 4 x 30 lambda, "
                     "PSF + stray light, half with S0/S1 fixed; host buffers; continuous batching "
-                    "(%d lanes, %d-pixel chunks)" % (n, args.serve_rate, args.serve_side_min,
-                                                     args.serve_side_max, 4, 65536),
-            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                    "(%d lanes, %d-pixel chunks, %s policy, HBM budget %s)"
+                    % (n, rate, args.serve_side_min, args.serve_side_max, 4, 65536, args.serve_policy,
+                       "%d GB" % args.serve_budget_gb if args.serve_budget_gb else "whole device"),
+            "rate": rate, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50)),
             "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
             "mean_queue_ms": float(np.mean(queue)),
+            "stretch_p50": float(np.percentile(stretch, 50)), "stretch_p99": float(np.percentile(stretch, 99)),
+            "by_size": classes,
             "pixels_per_s": float(npix.sum() / span), "offered_pixels_per_s": float(npix.sum() / arrivals[-1]),
             "requests": n, "pixels": int(npix.sum())}
+
+
+SERVE_POLICIES = {"round_robin": 0, "fifo": 1, "shortest_first": 2}
+
+
+def run_serve_sweep(args):
+    """--serve-sweep: the serving stream at each of the given arrival rates,
+    on a context whose HBM budget is --serve-budget-gb, one JSON line."""
+    import torch
+    import gmilos_b200 as G
+    torch.cuda.set_device(0)
+    lam, off = grid()
+    x, y = psf_table()
+    psf = G.psf_from_table(x, y, off, GRID[1])
+    eng = G.Engine(0, hbm_budget=int(args.serve_budget_gb) << 30)
+    zee = G.zeeman_from_levels(2, 1, 1.0, 2, 2, 0.0, 1.0)
+    eng.configure(G.make_config(lam, LAMBDA0, zee, fix=FIX, init=GUESS))
+    fine, W = fine_operator(off)
+    sl_fine = eng.synthesize_grid(np.array([STRAY_MODEL]), np.ascontiguousarray(fine / 1000.0))
+    slight = (sl_fine @ W.T.astype(np.float32))[0].astype(np.float32)
+    eng.configure(G.make_config(lam, LAMBDA0, zee, psf=psf, fix=FIX, init=GUESS, miter=MAXITER, slight=slight))
+    eng.serving_policy(SERVE_POLICIES[args.serve_policy])
+    P = args.pixels
+    rng = np.random.default_rng(args.seed)
+    obs = make_cube_gpu(eng, truth_models(P, rng), off, slight, args.seed + 1000, torch)
+    obs_h = obs.cpu().pin_memory()
+    del obs
+    rates = [float(r) for r in args.serve_sweep.split(",")]
+    out = {"metric": "serving latency", "policy": args.serve_policy, "budget_gb": args.serve_budget_gb,
+           "unloaded_rate_pixels_per_s": args.serve_unloaded_rate, "sweep": []}
+    for r in rates:
+        out["sweep"].append(serving_latency(eng, obs_h, args, rate=r, n=args.serve_requests))
+    print(json.dumps(out), flush=True)
+    eng.close()
 
 
 FIX9 = (1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 0)         # the 9 ME parameters
@@ -521,6 +577,70 @@ def config1_block(eng, args, torch, reps=10):
         res["fit_vs_reference"] = _fit_comparison(out["model64"].cpu().numpy(), out["chi2"].cpu().numpy(),
                                                   out["iters"].cpu().numpy(), mr, cr, ir)
     return res
+
+
+def ragged_block(eng, args, torch):
+    """Ragged batch: 64 ROIs, side lengths uniform in 16-512 px, centred
+    35 mA grids of 12-60 samples (same line, truth ranges, noise 1e-3 Ic, no
+    PSF), early stop at an accepted chi2 gain below 1e-4, 9 free, <= 50
+    iterations.  The whole batch goes to gm_invert_rois: one persistent
+    launch sequence per samples-per-lane class, autotuned on the first call,
+    then timed direct and as a replayed CUDA graph; beside it the same ROIs
+    inverted one gm_invert call each on their own grid."""
+    import gmilos_b200 as G
+    rng = np.random.default_rng(args.seed + 3)
+    zee = G.zeeman_from_levels(2, 1, 1.0, 2, 2, 0.0, 1.0)
+    dev = torch.device("cuda")
+    lam30, _ = grid()
+    eng.configure(G.make_config(lam30, LAMBDA0, zee, fix=FIX9, init=GUESS, miter=MAXITER))
+    rois = []
+    for k in range(args.ragged_rois):
+        side = int(rng.integers(16, 513))
+        nl = int(rng.integers(12, 61))
+        off = 35.0 * (np.arange(nl) - nl // 2)
+        lam = LAMBDA0 + off / 1000.0
+        t = truth_models(side * side, rng)
+        t[:, 10] = 1.0
+        o = eng.synthesize_grid(torch.tensor(t, dtype=torch.float64, device=dev),
+                                torch.tensor(off / 1000.0, dtype=torch.float64, device=dev))
+        o += NOISE * torch.randn(o.shape, device=dev, dtype=torch.float32)
+        rois.append((o.contiguous(), lam, None))
+    torch.cuda.synchronize()
+    P = sum(int(a.shape[0]) for a, _, _ in rois)
+    eng.configure(G.make_config(lam30, LAMBDA0, zee, fix=FIX9, init=GUESS, miter=MAXITER, stop_dchi2=1e-4))
+    _, tuned = eng.invert_rois(rois, autotune=True)
+    _, direct = eng.invert_rois(rois, autotune=True)
+    _, cap = eng.invert_rois(rois, use_graph=True, autotune=True)
+    reps = [eng.invert_rois(rois, use_graph=True, autotune=True)[1] for _ in range(2)]
+    outs, _ = eng.invert_rois(rois, use_graph=True, autotune=True)
+    graph_ms = float(np.mean([r["device_ms"] for r in reps]))
+    # the same ROIs one call each on their own grid (device-resident, no graph)
+    stream = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    cfgs = [G.make_config(lam, LAMBDA0, zee, fix=FIX9, init=GUESS, miter=MAXITER, stop_dchi2=1e-4)
+            for _, lam, _ in rois]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    t0 = time.perf_counter()
+    for (a, _, _), c in zip(rois, cfgs):
+        eng.configure(c)
+        eng.invert(a, stream=stream.cuda_stream)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    per_roi_wall = time.perf_counter() - t0
+    per_roi_ms = ev[0].elapsed_time(ev[1])
+    iters = np.concatenate([o["iters"].cpu().numpy() for o in outs])
+    return {"workload": "%d ROIs, sides 16-512 px, centred 35 mA grids of 12-60 samples, %d px in all, no PSF, "
+                        "noise 1e-3 Ic, early stop dchi2 < 1e-4" % (len(rois), P),
+            "pixels": P, "grids": tuned["grids"], "mean_iterations": float(iters.mean()),
+            "lane_occupancy": direct["lane_occupancy"],
+            "tuned_blocks_per_sm": {"trial": tuned["cap_trial"], "accept": tuned["cap_accept"]},
+            "direct": {"pixels_per_s": P / (direct["device_ms"] / 1e3), "ms": direct["device_ms"],
+                       "launches": direct["launches"]},
+            "graph": {"pixels_per_s": P / (graph_ms / 1e3), "ms": graph_ms, "replayed": reps[-1]["graph_replayed"],
+                      "capture_call_ms": cap["device_ms"]},
+            "one_call_per_roi": {"pixels_per_s": P / (per_roi_ms / 1e3), "ms": per_roi_ms,
+                                 "wall_s": per_roi_wall}}
 
 
 def _timed_inversions(eng, obs_d, torch, reps):
@@ -789,19 +909,28 @@ def main():
     ap.add_argument("--ref-gpu-pixels", type=int, default=65536,
                     help="pixels of the cube run through the reference's sm_100a build (0: skip)")
     ap.add_argument("--ref-gpu-streams", type=int, default=16)
-    ap.add_argument("--serve-requests", type=int, default=20,
-                    help="requests of the serving-latency phase (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=40,
+                    help="requests of the serving-latency phase, per rate with --serve-sweep (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=1.0, help="mean arrivals per second")
     ap.add_argument("--serve-side-min", type=int, default=256)
     ap.add_argument("--serve-side-max", type=int, default=2048)
+    ap.add_argument("--serve-policy", default="round_robin", choices=sorted(SERVE_POLICIES))
+    ap.add_argument("--serve-budget-gb", type=int, default=150, help="HBM budget of the serving context")
+    ap.add_argument("--serve-unloaded-rate", type=float, default=3.1e6,
+                    help="pixels/s of an unloaded host-memory inversion (the stretch's denominator)")
+    ap.add_argument("--serve-sweep", default="",
+                    help="comma-separated arrival rates: run only the serving stream at each (one JSON line)")
     ap.add_argument("--no-config1", dest="config1", action="store_false",
                     help="skip the 64x64 no-PSF case (engine and the reference's CPU routines)")
     ap.add_argument("--mlp-train-pixels", type=int, default=1 << 22,
                     help="training pixels of the learned initial guess (0: skip that block)")
     ap.add_argument("--mlp-epochs", type=int, default=8)
+    ap.add_argument("--ragged-rois", type=int, default=64, help="ROIs of the ragged-batch block (0: skip it)")
     ap.add_argument("--mlp-eval-pixels", type=int, default=1 << 20)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.serve_sweep:
+        run_serve_sweep(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.impl == "reference_gpu":
         run_reference_gpu(args)

@@ -105,6 +105,7 @@ struct gm_ctx {
   int serve_streams = 4;
   int64_t serve_chunk = 65536;        // pixels per launch
   int serve_max_active = 16;
+  int serve_policy = GM_SERVE_ROUND_ROBIN;   // which admitted request a free lane takes
   size_t rr = 0;                      // round-robin cursor over active requests
   gm_ticket next_ticket = 1;
   std::thread worker;
@@ -115,6 +116,12 @@ struct gm_ctx {
   gm::mlp::DevNet net;
   bool learned = false;
   int* mlp_err = nullptr;
+  // ragged batches: the layout of the last batch, its captured device work
+  // and its resident-block limits per samples-per-lane class
+  std::string batch_key;
+  cudaGraphExec_t batch_exec = nullptr;
+  int batch_cap[2][2] = {{0, 0}, {0, 0}};
+  bool batch_tuned = false;
 };
 
 namespace {
@@ -361,6 +368,7 @@ gm_status gm_destroy(gm_ctx* ctx) {
   if (ctx->work2) cudaFree(ctx->work2);
   gm::mlp::devnet_destroy(&ctx->net);
   if (ctx->mlp_err) cudaFree(ctx->mlp_err);
+  if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   if (ctx->evx0) cudaEventDestroy(ctx->evx0);
@@ -1009,6 +1017,15 @@ gm_status gm_serving_options(gm_ctx* ctx, int streams, int64_t chunk_pixels, int
   return GM_OK;
 }
 
+gm_status gm_serving_policy(gm_ctx* ctx, int policy) {
+  if (!ctx) return GM_ERR_INVALID;
+  if (policy != GM_SERVE_ROUND_ROBIN && policy != GM_SERVE_FIFO && policy != GM_SERVE_SHORTEST_FIRST)
+    return fail(ctx, GM_ERR_INVALID, "unknown serving policy");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->serve_policy = policy;
+  return GM_OK;
+}
+
 gm_status gm_submit(gm_ctx* ctx, const gm_request* req, gm_ticket* ticket) {
   if (!ctx || !req || !ticket) return GM_ERR_INVALID;
   if (!ctx->configured) return fail(ctx, GM_ERR_NOT_CONFIGURED, "gm_configure first");
@@ -1216,18 +1233,29 @@ void serve_loop(gm_ctx* ctx) {
       if (--r->outstanding == 0 && (r->next >= r->req.npix || r->result != GM_OK))
         finish(ctx, r, r->result);
     }
-    // keep every lane busy with the next chunk, round robin over requests
+    // keep every lane busy with the next chunk of the request the policy
+    // picks: round robin over the admitted requests, the earliest submitted,
+    // or the one with the fewest pixels left
     for (ServeLane& L : ctx->lanes) {
       if (L.busy) continue;
       std::shared_ptr<Request> pick;
       {
         std::lock_guard<std::mutex> lk(ctx->mu);
         const size_t n = ctx->active.size();
-        for (size_t k = 0; k < n && !pick; ++k) {
-          auto& c = ctx->active[(ctx->rr + k) % n];
-          if (c->result == GM_OK && c->next < c->req.npix && !c->done) {
+        for (size_t k = 0; k < n; ++k) {
+          const size_t i = (ctx->rr + k) % n;
+          auto& c = ctx->active[i];
+          if (c->result != GM_OK || c->next >= c->req.npix || c->done) continue;
+          bool better = !pick;
+          if (pick && ctx->serve_policy == GM_SERVE_FIFO) better = c->t_submit < pick->t_submit;
+          if (pick && ctx->serve_policy == GM_SERVE_SHORTEST_FIRST)
+            better = c->req.npix - c->next < pick->req.npix - pick->next;
+          if (better) {
             pick = c;
-            ctx->rr = (ctx->rr + k + 1) % n;
+            if (ctx->serve_policy == GM_SERVE_ROUND_ROBIN) {
+              ctx->rr = (i + 1) % n;
+              break;
+            }
           }
         }
       }
@@ -1260,6 +1288,341 @@ void serve_loop(gm_ctx* ctx) {
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------- ragged batches
+namespace {
+
+// One samples-per-lane class of a ragged batch: its grids' configurations,
+// its ROIs in batch order, its pixels' grid indices and profile offsets, and
+// the device buffers of its launch.
+struct BatchClass {
+  std::vector<gm::DevCfg> cfgs;
+  std::vector<int> rois;              // indices into the batch
+  std::vector<int64_t> first;         // first pixel of each of its ROIs
+  std::vector<uint64_t> in_off;       // offset (floats) of each ROI's profiles
+  int64_t pixels = 0;
+  uint64_t floats = 0;                // profile floats of the class
+  // device
+  float* in = nullptr;
+  float* model = nullptr;
+  float* chi2 = nullptr;
+  int* iters = nullptr;
+  uint32_t* status = nullptr;
+  double* cinit = nullptr;
+  uint32_t* cstat = nullptr;
+  gm::DevCfg* dcfgs = nullptr;
+  uint16_t* grid = nullptr;
+  uint64_t* off = nullptr;
+  gm::WaveBuffers wb{};
+  int bt = 0, ba = 0;                 // resident blocks per SM (full)
+};
+
+// The configuration of one grid: the context's, with the grid's samples and
+// PSF taps (the host-side arithmetic of build_devcfg).
+gm::DevCfg grid_devcfg(const gm::DevCfg& base, const gm_roi& r, double lambda0) {
+  gm::DevCfg d = base;
+  d.nl = r.nl;
+  d.use_psf = r.psf ? 1 : 0;
+  for (int l = 0; l < gm::kMaxNl; ++l) {
+    const bool in = l < r.nl;
+    const double off = in ? r.lambda[l] - lambda0 : 0.0;
+    d.dl[l] = (float)off;
+    d.dld[l] = off;
+    d.lam[l] = in ? r.lambda[l] : 0.0;
+    d.psfd[l] = (in && r.psf) ? r.psf[l] : 0.0;
+  }
+  d.init_mode = 1;   // start models from the classical pre-pass
+  return d;
+}
+
+bool same_grid(const gm_roi& a, const gm_roi& b) {
+  if (a.nl != b.nl || (a.psf == nullptr) != (b.psf == nullptr)) return false;
+  if (std::memcmp(a.lambda, b.lambda, sizeof(double) * a.nl)) return false;
+  return !a.psf || !std::memcmp(a.psf, b.psf, sizeof(double) * a.nl);
+}
+
+// The device work of a batch (both classes, class 1 on the auxiliary stream
+// between a fork and a join), launched directly or captured.
+cudaError_t batch_device_work(gm_ctx* ctx, BatchClass* cls, const int (*cap)[2], cudaStream_t s, int* launches) {
+  cudaError_t e = cudaEventRecord(ctx->evx0, s);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->aux, ctx->evx0, 0);
+  for (int c = 0; c < 2 && e == cudaSuccess; ++c) {
+    BatchClass& k = cls[c];
+    if (!k.pixels) continue;
+    cudaStream_t q = c == 0 ? s : ctx->aux;
+    gm::WorkCounters* w = c == 0 ? ctx->work : ctx->work2;
+    gm::MultiGrid mg{k.dcfgs, k.grid, k.off};
+    e = cudaMemsetAsync(w, 0, sizeof(gm::WorkCounters), q);
+    if (e == cudaSuccess) e = gm::launch_classical_mg(k.cfgs[0], mg, k.in, k.pixels, k.cinit, k.cstat, q);
+    if (e != cudaSuccess) break;
+    gm::InvertArgs ia{};
+    ia.iquv = k.in;
+    ia.npix = k.pixels;
+    ia.init_models = k.cinit;
+    ia.init_status = k.cstat;
+    ia.model = k.model;
+    ia.chi2 = k.chi2;
+    ia.iters = k.iters;
+    ia.status = k.status;
+    ia.work = w;
+    int n = 0;
+    e = gm::launch_invert_waves_mg(k.cfgs[0], mg, ia, k.wb, cap[c][0], cap[c][1], q, &n);
+    *launches += n + 1;
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->evx1, ctx->aux);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ctx->evx1, 0);
+  return e;
+}
+
+}  // namespace
+
+extern "C" gm_status gm_invert_rois(gm_ctx* ctx, const gm_roi* rois, int nroi, const gm_batch_opts* opts,
+                                    gm_batch_stats* stats, void* stream) {
+  if (!ctx) return GM_ERR_INVALID;
+  if (!rois || nroi < 0) return fail(ctx, GM_ERR_INVALID, "bad argument");
+  if (!ctx->configured) return fail(ctx, GM_ERR_NOT_CONFIGURED, "gm_configure first");
+  const gm::DevCfg& base = ctx->dev;
+  if (base.use_slight || base.lambda_per_pixel || ctx->learned || ctx->cfg.init_mode != GM_INIT_CLASSICAL)
+    return fail(ctx, GM_ERR_UNSUPPORTED,
+                "ragged batches start from the classical estimates, without stray light or per-pixel grids");
+  for (int i = 0; i < nroi; ++i) {
+    const gm_roi& r = rois[i];
+    if (!r.iquv || !r.model || !r.lambda || r.npix < 0 || r.nl < 2 || r.nl > GM_MAX_NL)
+      return fail(ctx, GM_ERR_INVALID, "ROI " + std::to_string(i) + ": bad description");
+  }
+  gm_batch_opts def{};
+  if (!opts) opts = &def;
+  std::lock_guard<std::mutex> lk(ctx->call_mu);
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  if (ctx->scratch_pending) cudaStreamWaitEvent(s, ctx->ev_scratch, 0);
+  // grids, classes, the pixels' tables
+  BatchClass cls[2];
+  std::vector<const gm_roi*> gfirst[2];   // one ROI per grid of a class
+  std::string key;
+  for (int i = 0; i < nroi; ++i) {
+    const gm_roi& r = rois[i];
+    BatchClass& k = cls[r.nl <= 32 ? 0 : 1];
+    auto& gl = gfirst[r.nl <= 32 ? 0 : 1];
+    int g = 0;
+    while (g < (int)gl.size() && !same_grid(*gl[g], r)) ++g;
+    if (g == (int)gl.size()) {
+      if (g >= 65535) return fail(ctx, GM_ERR_INVALID, "too many distinct grids in one batch");
+      gl.push_back(&r);
+      k.cfgs.push_back(grid_devcfg(base, r, ctx->cfg.lambda0));
+    }
+    k.rois.push_back(i);
+    k.first.push_back(k.pixels);
+    k.in_off.push_back(k.floats);
+    k.pixels += r.npix;
+    k.floats += 4 * (uint64_t)r.nl * r.npix;
+    key += std::to_string(r.npix) + ":" + std::to_string(r.nl) + ":" + std::to_string(g) + ";";
+  }
+  for (int c = 0; c < 2; ++c) key += "|" + std::to_string(cls[c].cfgs.size());
+  gm_batch_stats st{};
+  int64_t total = cls[0].pixels + cls[1].pixels;
+  st.pixels = total;
+  st.grids = (int)(cls[0].cfgs.size() + cls[1].cfgs.size());
+  if (total == 0) {
+    if (stats) *stats = st;
+    return GM_OK;
+  }
+  // device buffers within the budget: inputs, outputs, start models, tables
+  size_t need = 0;
+  for (int c = 0; c < 2; ++c)
+    need += sizeof(float) * cls[c].floats +
+            (size_t)cls[c].pixels * (11 * 4 + 4 + 4 + 4 + 11 * 8 + 4 + 2 + 8) + sizeof(gm::DevCfg) * cls[c].cfgs.size();
+  gm_status stt;
+  for (int c = 0; c < 2; ++c) {
+    BatchClass& k = cls[c];
+    if (!k.pixels) continue;
+    const std::string p = c ? "rg1_" : "rg0_";
+    void* q = nullptr;
+    const int64_t P = k.pixels;
+    if ((stt = ensure_buf(ctx, p + "in", sizeof(float) * k.floats, &q)) != GM_OK) return stt;
+    k.in = (float*)q;
+    if ((stt = ensure_buf(ctx, p + "model", sizeof(float) * 11 * P, &q)) != GM_OK) return stt;
+    k.model = (float*)q;
+    if ((stt = ensure_buf(ctx, p + "chi2", sizeof(float) * P, &q)) != GM_OK) return stt;
+    k.chi2 = (float*)q;
+    if ((stt = ensure_buf(ctx, p + "iters", sizeof(int) * P, &q)) != GM_OK) return stt;
+    k.iters = (int*)q;
+    if ((stt = ensure_buf(ctx, p + "status", sizeof(uint32_t) * P, &q)) != GM_OK) return stt;
+    k.status = (uint32_t*)q;
+    if ((stt = ensure_buf(ctx, p + "cinit", sizeof(double) * 11 * P, &q)) != GM_OK) return stt;
+    k.cinit = (double*)q;
+    if ((stt = ensure_buf(ctx, p + "cstat", sizeof(uint32_t) * P, &q)) != GM_OK) return stt;
+    k.cstat = (uint32_t*)q;
+    if ((stt = ensure_buf(ctx, p + "cfgs", sizeof(gm::DevCfg) * k.cfgs.size(), &q)) != GM_OK) return stt;
+    k.dcfgs = (gm::DevCfg*)q;
+    if ((stt = ensure_buf(ctx, p + "grid", sizeof(uint16_t) * P, &q)) != GM_OK) return stt;
+    k.grid = (uint16_t*)q;
+    if ((stt = ensure_buf(ctx, p + "off", sizeof(uint64_t) * P, &q)) != GM_OK) return stt;
+    k.off = (uint64_t*)q;
+    gm::waves_mg_occupancy(k.cfgs[0], &k.bt, &k.ba);
+    if (k.bt < 1 || k.ba < 1) return fail(ctx, GM_ERR_CUDA, "ragged-batch kernels cannot be resident");
+  }
+  for (int c = 0; c < 2; ++c) {
+    BatchClass& k = cls[c];
+    if (!k.pixels) continue;
+    const int64_t chunk = wave_chunk_for(ctx, k.cfgs[0], need, k.pixels, 2);
+    if (!chunk) return fail(ctx, GM_ERR_NOMEM, "the batch's wave state does not fit the HBM budget");
+    if ((stt = wave_buffers(ctx, c ? "rg1_waves" : "rg0_waves", k.cfgs[0], chunk, &k.wb)) != GM_OK) return stt;
+    key += "|" + std::to_string(chunk) + "@" + std::to_string((uintptr_t)k.wb.w.state) + "/" +
+           std::to_string((uintptr_t)k.in);
+  }
+  // uploads: the profiles, the grids' configurations, the per-pixel tables
+  cudaError_t e = cudaSuccess;
+  for (int c = 0; c < 2 && e == cudaSuccess; ++c) {
+    BatchClass& k = cls[c];
+    if (!k.pixels) continue;
+    std::vector<uint16_t> grid((size_t)k.pixels);
+    std::vector<uint64_t> off((size_t)k.pixels);
+    for (size_t j = 0; j < k.rois.size(); ++j) {
+      const gm_roi& r = rois[k.rois[j]];
+      int g = 0;
+      const auto& gl = gfirst[c];
+      while (!same_grid(*gl[g], r)) ++g;
+      const uint64_t row = 4 * (uint64_t)r.nl;
+      for (int64_t p = 0; p < r.npix; ++p) {
+        grid[(size_t)(k.first[j] + p)] = (uint16_t)g;
+        off[(size_t)(k.first[j] + p)] = k.in_off[j] + (uint64_t)p * row;
+      }
+      if (e == cudaSuccess && r.npix)
+        e = cudaMemcpyAsync(k.in + k.in_off[j], r.iquv, sizeof(float) * row * r.npix, cudaMemcpyDefault, s);
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(k.dcfgs, k.cfgs.data(), sizeof(gm::DevCfg) * k.cfgs.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(k.grid, grid.data(), sizeof(uint16_t) * grid.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(k.off, off.data(), sizeof(uint64_t) * off.size(), cudaMemcpyHostToDevice, s);
+  }
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "ragged-batch upload");
+  // layout change: forget the captured work and the tuning
+  if (key != ctx->batch_key) {
+    if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
+    ctx->batch_exec = nullptr;
+    ctx->batch_key = key;
+    ctx->batch_tuned = false;
+    for (int c = 0; c < 2; ++c) {
+      ctx->batch_cap[c][0] = cls[c].bt;
+      ctx->batch_cap[c][1] = cls[c].ba;
+    }
+  }
+  int launches = 0;
+  float ms = 0.f;
+  if (opts->autotune && !ctx->batch_tuned) {
+    // candidates: full, trial kernel at 3/4, accept kernel at 3/4, both at 1/2
+    const int frac[4][2] = {{4, 4}, {3, 4}, {4, 3}, {2, 2}};
+    float best = -1.f;
+    int bestc = 0;
+    for (int t = 0; t < 4; ++t) {
+      int cap[2][2];
+      for (int c = 0; c < 2; ++c) {
+        cap[c][0] = std::max(1, cls[c].bt * frac[t][0] / 4);
+        cap[c][1] = std::max(1, cls[c].ba * frac[t][1] / 4);
+      }
+      launches = 0;
+      e = cudaEventRecord(ctx->ev0, s);
+      if (e == cudaSuccess) e = batch_device_work(ctx, cls, cap, s, &launches);
+      if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, s);
+      if (e == cudaSuccess) e = cudaEventSynchronize(ctx->ev1);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "ragged-batch tuning");
+      cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+      if (best < 0 || ms < best) {
+        best = ms;
+        bestc = t;
+      }
+    }
+    for (int c = 0; c < 2; ++c) {
+      ctx->batch_cap[c][0] = std::max(1, cls[c].bt * frac[bestc][0] / 4);
+      ctx->batch_cap[c][1] = std::max(1, cls[c].ba * frac[bestc][1] / 4);
+    }
+    ctx->batch_tuned = true;
+    if (ctx->batch_exec) cudaGraphExecDestroy(ctx->batch_exec);
+    ctx->batch_exec = nullptr;
+  }
+  launches = 0;
+  if (opts->use_graph) {
+    if (!ctx->batch_exec) {
+      cudaGraph_t g = nullptr;
+      e = cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed);
+      if (e == cudaSuccess) {
+        const cudaError_t we = batch_device_work(ctx, cls, ctx->batch_cap, s, &launches);
+        e = cudaStreamEndCapture(s, &g);
+        if (we != cudaSuccess) e = we;
+      }
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->batch_exec, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        ctx->batch_exec = nullptr;
+        return cuda_fail(ctx, e, "ragged-batch graph capture");
+      }
+    } else {
+      st.graph_replayed = 1;
+      for (int c = 0; c < 2; ++c)
+        if (cls[c].pixels) {
+          const int waves = 1 + (cls[c].cfgs[0].miter > 1 ? cls[c].cfgs[0].miter : 1);
+          const int64_t ch = cls[c].wb.chunk;
+          launches += (int)((cls[c].pixels + ch - 1) / ch) * (2 * waves - 1) + 1;
+        }
+    }
+    e = cudaEventRecord(ctx->ev0, s);
+    if (e == cudaSuccess) e = cudaGraphLaunch(ctx->batch_exec, s);
+  } else {
+    e = cudaEventRecord(ctx->ev0, s);
+    if (e == cudaSuccess) e = batch_device_work(ctx, cls, ctx->batch_cap, s, &launches);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "ragged-batch launch");
+  // outputs back into the callers' buffers
+  for (int c = 0; c < 2 && e == cudaSuccess; ++c) {
+    BatchClass& k = cls[c];
+    for (size_t j = 0; j < k.rois.size() && e == cudaSuccess; ++j) {
+      const gm_roi& r = rois[k.rois[j]];
+      if (!r.npix) continue;
+      const int64_t f = k.first[j];
+      e = cudaMemcpyAsync(r.model, k.model + f * 11, sizeof(float) * 11 * r.npix, cudaMemcpyDefault, s);
+      if (e == cudaSuccess && r.chi2)
+        e = cudaMemcpyAsync(r.chi2, k.chi2 + f, sizeof(float) * r.npix, cudaMemcpyDefault, s);
+      if (e == cudaSuccess && r.iters)
+        e = cudaMemcpyAsync(r.iters, k.iters + f, sizeof(int) * r.npix, cudaMemcpyDefault, s);
+      if (e == cudaSuccess && r.status)
+        e = cudaMemcpyAsync(r.status, k.status + f, sizeof(uint32_t) * r.npix, cudaMemcpyDefault, s);
+    }
+  }
+  cudaEventRecord(ctx->ev_scratch, s);
+  ctx->scratch_pending = true;
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "ragged batch");
+  cudaEventElapsedTime(&st.device_ms, ctx->ev0, ctx->ev1);
+  // lane occupancy: samples over lane slots, weighted by each pixel's trials
+  double samples = 0, slots = 0;
+  for (int c = 0; c < 2; ++c) {
+    BatchClass& k = cls[c];
+    if (!k.pixels) continue;
+    std::vector<int> it((size_t)k.pixels);
+    if (cudaMemcpy(it.data(), k.iters, sizeof(int) * it.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return fail(ctx, GM_ERR_CUDA, "ragged-batch statistics");
+    for (size_t j = 0; j < k.rois.size(); ++j) {
+      const gm_roi& r = rois[k.rois[j]];
+      double trials = 0;
+      for (int64_t p = 0; p < r.npix; ++p) trials += it[(size_t)(k.first[j] + p)] + 1;
+      samples += trials * r.nl;
+      slots += trials * 32.0 * (c + 1);
+    }
+  }
+  st.lane_occupancy = slots > 0 ? samples / slots : 0.0;
+  st.launches = launches;
+  st.cap_trial = ctx->batch_cap[cls[0].pixels ? 0 : 1][0];
+  st.cap_accept = ctx->batch_cap[cls[0].pixels ? 0 : 1][1];
+  ctx->stats.pixels = total;
+  ctx->stats.kernel_launches = launches;
+  ctx->stats.kernel_ms = st.device_ms;
+  if (stats) *stats = st;
+  return GM_OK;
+}
 
 // ---------------------------------------------------------------- learned initial guess
 extern "C" {

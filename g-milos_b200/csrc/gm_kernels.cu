@@ -324,10 +324,10 @@ __device__ __forceinline__ void stage_get(const float* __restrict__ q, Lane<LPL,
 }
 
 // Outputs of a pixel that stopped (as invert_kernel writes them).
-template <int LPL>
+template <int LPL, bool MG>
 __device__ __forceinline__ void finish_pixel(const InvertArgs& a, const double* m, float ochisqr, int iter,
                                              int acc, uint32_t st, const float (&syn)[LPL][4],
-                                             uint64_t pix, int nl, int lane) {
+                                             uint64_t pix, int nl, int lane, const MultiGrid& mg) {
   if (lane < 11) {
     if (a.model) a.model[pix * 11 + lane] = (float)m[lane];
     if (a.model_f64) a.model_f64[pix * 11 + lane] = m[lane];
@@ -339,7 +339,7 @@ __device__ __forceinline__ void finish_pixel(const InvertArgs& a, const double* 
     if (a.status) a.status[pix] = st;
   }
   if (a.fitted) {
-    const size_t off = (size_t)pix * 4 * nl;
+    const size_t off = MG ? (size_t)mg.off[pix] : (size_t)pix * 4 * nl;
 #pragma unroll
     for (int k = 0; k < LPL; ++k) {
       const int l = lane + 32 * k;
@@ -350,22 +350,20 @@ __device__ __forceinline__ void finish_pixel(const InvertArgs& a, const double* 
   }
 }
 
-// One trial of every pixel in the wave's active list (wave 0: the start
-// models, every pixel of the chunk).  The body is invert_kernel's loop
-// body from the solve to the damping schedule (milosUtils.cu:630-700).
-template <int LPL, int V>
-__global__ void __launch_bounds__(warps_per_block<LPL>() * 32, trial_min_blocks<LPL, V>())
-trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
-  constexpr int NS = Variant<V>::SOLVES, NT = Variant<V>::NT, NA = NT * (NT + 1) / 2;
-  const int lane = threadIdx.x & 31;
-  load_taps<LPL>(c);
-  WarpSmem<LPL, V>& sm = trial_smem<LPL, V>();
-  for (int i = lane; i < 8 * row_pitch<LPL>(); i += 32) (&sm.rows[0][0])[i] = 0.f;
-  __syncwarp();
-  const int nl = c.nl;
-  float dlv[LPL];
-  double dld[LPL];
-  bool valid[LPL];
+// The configuration a pixel runs on: the launch's own or, in a ragged
+// batch, its grid's (device memory).
+template <bool MG>
+__device__ __forceinline__ const DevCfg& pixel_cfg(const DevCfg& c0, const DevCfg* cp) {
+  if constexpr (MG) return *cp;
+  else return c0;
+}
+
+// Per-lane constants of a grid: samples held, offsets from the line centre,
+// the single stray-light profile (zero without one).
+template <int LPL>
+__device__ __forceinline__ void grid_lanes(const DevCfg& c, int lane, int& nl, float (&dlv)[LPL],
+                                           double (&dld)[LPL], bool (&valid)[LPL], float (&slg)[LPL][4]) {
+  nl = c.nl;
 #pragma unroll
   for (int k = 0; k < LPL; ++k) {
     const int l = lane + 32 * k;
@@ -373,7 +371,6 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
     dlv[k] = valid[k] ? c.dl[l] : 0.f;
     dld[k] = valid[k] ? c.dld[l] : 0.0;
   }
-  float slg[LPL][4];
   if (c.use_slight && !c.slight_per_pixel) load_pixel<LPL>(c.slight, nl, lane, slg);
   else {
 #pragma unroll
@@ -381,6 +378,46 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
 #pragma unroll
       for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
   }
+}
+
+// Blocks of the wave kernels: warps_per_block warps, or one warp in a ragged
+// batch (its PSF taps, shared by a block's warps, follow the warp's grid).
+template <int LPL, bool MG>
+constexpr int wave_warps() { return MG ? 1 : warps_per_block<LPL>(); }
+
+// One trial of every pixel in the wave's active list (wave 0: the start
+// models, every pixel of the chunk).  The body is invert_kernel's loop
+// body from the solve to the damping schedule (milosUtils.cu:630-700).
+template <int LPL, int V, bool MG>
+__global__ void __launch_bounds__(wave_warps<LPL, MG>() * 32,
+                                  trial_min_blocks<LPL, V>() * warps_per_block<LPL>() / wave_warps<LPL, MG>())
+trial_kernel(const DevCfg c0, const InvertArgs a, const WaveArgs w, int wave, const MultiGrid mg) {
+  constexpr int NS = Variant<V>::SOLVES, NT = Variant<V>::NT, NA = NT * (NT + 1) / 2;
+  const int lane = threadIdx.x & 31;
+  if constexpr (!MG) load_taps<LPL>(c0);
+  WarpSmem<LPL, V>& sm = trial_smem<LPL, V>();
+  for (int i = lane; i < 8 * row_pitch<LPL>(); i += 32) (&sm.rows[0][0])[i] = 0.f;
+  __syncwarp();
+  int nl = c0.nl;
+  float dlv[LPL];
+  double dld[LPL];
+  bool valid[LPL];
+#pragma unroll
+  for (int k = 0; k < LPL; ++k) {
+    const int l = lane + 32 * k;
+    valid[k] = l < nl;
+    dlv[k] = valid[k] ? c0.dl[l] : 0.f;
+    dld[k] = valid[k] ? c0.dld[l] : 0.0;
+  }
+  float slg[LPL][4];
+  if (c0.use_slight && !c0.slight_per_pixel) load_pixel<LPL>(c0.slight, nl, lane, slg);
+  else {
+#pragma unroll
+    for (int k = 0; k < LPL; ++k)
+#pragma unroll
+      for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
+  }
+  int cur = -1;   // grid whose constants are loaded (ragged batches)
   const SolvePlan plan = make_solve_plan<NS>(lane);
   Solve11Plan plan11;
   if constexpr (NT == 11) plan11 = make_solve11_plan(lane);
@@ -394,8 +431,19 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
     j = __shfl_sync(kFull, j, 0);
     if (j >= n) break;
     const uint32_t pix = wave == 0 ? j : in[j];
+    const DevCfg* cp = nullptr;
+    if constexpr (MG) {
+      const int gi = mg.grid[pix];
+      cp = mg.cfgs + gi;
+      if (gi != cur) {
+        cur = gi;
+        load_taps<LPL>(*cp);
+        grid_lanes<LPL>(*cp, lane, nl, dlv, dld, valid, slg);
+      }
+    }
+    const DevCfg& c = pixel_cfg<MG>(c0, cp);
     PixLM& P = w.state[pix];
-    const size_t off = (size_t)pix * 4 * nl;
+    const size_t off = MG ? (size_t)mg.off[pix] : (size_t)pix * 4 * nl;
     float ob[LPL][4];
     load_pixel<LPL>(a.iquv + off, nl, lane, ob);
     if (c.use_slight && c.slight_per_pixel) load_pixel<LPL>(c.slight + off, nl, lane, slg);
@@ -486,7 +534,7 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
     if (wave > 0 && (iter >= c.miter || stop)) {
       if (!stop) st |= GM_PIX_MAXITER;
       if (!isfinite(ochisqr)) st |= GM_PIX_NONFINITE;
-      finish_pixel<LPL>(a, sm.m, ochisqr, iter, acc, st, syn, pix, nl, lane);
+      finish_pixel<LPL, MG>(a, sm.m, ochisqr, iter, acc, st, syn, pix, nl, lane, mg);
       my_iter += iter;
       my_acc += acc;
     } else {
@@ -526,14 +574,17 @@ trial_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
 
 // Response functions and normal equations of every pixel whose trial of
 // this wave was accepted (the accept branch of invert_kernel's loop).
-template <int LPL, int V>
-__global__ void __launch_bounds__(warps_per_block<LPL>() * 32, accept_min_blocks<LPL, V>())
-accept_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
+template <int LPL, int V, bool MG>
+__global__ void __launch_bounds__(wave_warps<LPL, MG>() * 32,
+                                  accept_min_blocks<LPL, V>() * warps_per_block<LPL>() / wave_warps<LPL, MG>())
+accept_kernel(const DevCfg c0, const InvertArgs a, const WaveArgs w, int wave, const MultiGrid mg) {
   const int lane = threadIdx.x & 31;
-  load_taps<LPL>(c);
   WarpSmem<LPL, V>& sm = warp_smem<LPL, V>();
-  init_rows<LPL, V>(c, sm, lane);
-  const int nl = c.nl;
+  if constexpr (!MG) {
+    load_taps<LPL>(c0);
+    init_rows<LPL, V>(c0, sm, lane);
+  }
+  int nl = c0.nl;
   float dlv[LPL];
   double dld[LPL];
   bool valid[LPL];
@@ -544,23 +595,36 @@ accept_kernel(const DevCfg c, const InvertArgs a, const WaveArgs w, int wave) {
     dld[k] = 0.0;
   }
   float slg[LPL][4];
-  if (c.use_slight && !c.slight_per_pixel) load_pixel<LPL>(c.slight, nl, lane, slg);
+  if (c0.use_slight && !c0.slight_per_pixel) load_pixel<LPL>(c0.slight, nl, lane, slg);
   else {
 #pragma unroll
     for (int k = 0; k < LPL; ++k)
 #pragma unroll
       for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
   }
+  int cur = -1;   // grid whose constants are loaded (ragged batches)
   const uint32_t n = w.cnt[wave].n_acc;
-  const bool alpha_mixed = wave > 0 && c.quirks;
+  const bool alpha_mixed = wave > 0 && c0.quirks;
   while (true) {
     uint32_t j = 0;
     if (lane == 0) j = atomicAdd(&w.cnt[wave].cur_acc, 1u);
     j = __shfl_sync(kFull, j, 0);
     if (j >= n) break;
     const uint32_t pix = w.accl[j];
+    const DevCfg* cp = nullptr;
+    if constexpr (MG) {
+      const int gi = mg.grid[pix];
+      cp = mg.cfgs + gi;
+      if (gi != cur) {
+        cur = gi;
+        load_taps<LPL>(*cp);
+        init_rows<LPL, V>(*cp, sm, lane);
+        grid_lanes<LPL>(*cp, lane, nl, dlv, dld, valid, slg);
+      }
+    }
+    const DevCfg& c = pixel_cfg<MG>(c0, cp);
     PixLM& P = w.state[pix];
-    const size_t off = (size_t)pix * 4 * nl;
+    const size_t off = MG ? (size_t)mg.off[pix] : (size_t)pix * 4 * nl;
     float ob[LPL][4];
     load_pixel<LPL>(a.iquv + off, nl, lane, ob);
     if (c.use_slight && c.slight_per_pixel) load_pixel<LPL>(c.slight + off, nl, lane, slg);
@@ -655,25 +719,37 @@ synth_kernel(const DevCfg c, const SynthArgs a) {
 // exactly as the inversion kernel forms them in place (milosUtils.cu:616-628),
 // with their status bits in `status` -- a pre-pass that keeps this code out
 // of the inversion kernel's instruction stream.
-template <int LPL, bool FOR_INIT>
-__global__ void __launch_bounds__(128) classical_kernel(const DevCfg c, const float* __restrict__ iquv,
+template <int LPL, bool FOR_INIT, bool MG>
+__global__ void __launch_bounds__(128) classical_kernel(const DevCfg c0, const float* __restrict__ iquv,
                                                         int64_t npix, double* __restrict__ models,
-                                                        uint32_t* __restrict__ status) {
+                                                        uint32_t* __restrict__ status, const MultiGrid mg) {
   __shared__ double ms[4][11];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int nl = c.nl;
+  int nl = c0.nl;
   double dld[LPL];
   bool valid[LPL];
 #pragma unroll
   for (int k = 0; k < LPL; ++k) {
     const int l = lane + 32 * k;
     valid[k] = l < nl;
-    dld[k] = valid[k] ? c.dld[l] : 0.0;
+    dld[k] = valid[k] ? c0.dld[l] : 0.0;
   }
   const int64_t nw = (int64_t)gridDim.x * 4;
   for (int64_t pix = (int64_t)blockIdx.x * 4 + w; pix < npix; pix += nw) {
+    const DevCfg* cp = nullptr;
+    if constexpr (MG) {
+      cp = mg.cfgs + mg.grid[pix];
+      nl = cp->nl;
+#pragma unroll
+      for (int k = 0; k < LPL; ++k) {
+        const int l = lane + 32 * k;
+        valid[k] = l < nl;
+        dld[k] = valid[k] ? cp->dld[l] : 0.0;
+      }
+    }
+    const DevCfg& c = pixel_cfg<MG>(c0, cp);
     float ob[LPL][4], dlv[LPL];
-    load_pixel<LPL>(iquv + (size_t)pix * 4 * nl, nl, lane, ob);
+    load_pixel<LPL>(iquv + (MG ? (size_t)mg.off[pix] : (size_t)pix * 4 * nl), nl, lane, ob);
     pixel_grid<LPL>(c, (unsigned long long)pix, lane, dlv, dld);
     if (lane < 11) ms[w][lane] = c.init[lane];
     __syncwarp();
@@ -685,19 +761,33 @@ __global__ void __launch_bounds__(128) classical_kernel(const DevCfg c, const fl
   }
 }
 
-cudaError_t launch_classical(const DevCfg& cfg, const float* iquv, int64_t npix, double* models,
-                             uint32_t* status, bool for_init, cudaStream_t s) {
+static int classical_blocks(int64_t npix) {
   int64_t blocks = (npix + 3) / 4;
   if (blocks > 148 * 32) blocks = 148 * 32;
-  if (blocks < 1) blocks = 1;
+  return blocks < 1 ? 1 : (int)blocks;
+}
+
+cudaError_t launch_classical(const DevCfg& cfg, const float* iquv, int64_t npix, double* models,
+                             uint32_t* status, bool for_init, cudaStream_t s) {
+  const int blocks = classical_blocks(npix);
   const bool l1 = cfg.nl <= 32;
+  const MultiGrid none{};
   if (for_init) {
-    if (l1) classical_kernel<1, true><<<(int)blocks, 128, 0, s>>>(cfg, iquv, npix, models, status);
-    else classical_kernel<2, true><<<(int)blocks, 128, 0, s>>>(cfg, iquv, npix, models, status);
+    if (l1) classical_kernel<1, true, false><<<blocks, 128, 0, s>>>(cfg, iquv, npix, models, status, none);
+    else classical_kernel<2, true, false><<<blocks, 128, 0, s>>>(cfg, iquv, npix, models, status, none);
   } else {
-    if (l1) classical_kernel<1, false><<<(int)blocks, 128, 0, s>>>(cfg, iquv, npix, models, status);
-    else classical_kernel<2, false><<<(int)blocks, 128, 0, s>>>(cfg, iquv, npix, models, status);
+    if (l1) classical_kernel<1, false, false><<<blocks, 128, 0, s>>>(cfg, iquv, npix, models, status, none);
+    else classical_kernel<2, false, false><<<blocks, 128, 0, s>>>(cfg, iquv, npix, models, status, none);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_classical_mg(const DevCfg& cfg, const MultiGrid& mg, const float* iquv, int64_t npix,
+                                double* models, uint32_t* status, cudaStream_t s) {
+  if (npix <= 0) return cudaSuccess;
+  const int blocks = classical_blocks(npix);
+  if (cfg.nl <= 32) classical_kernel<1, true, true><<<blocks, 128, 0, s>>>(cfg, iquv, npix, models, status, mg);
+  else classical_kernel<2, true, true><<<blocks, 128, 0, s>>>(cfg, iquv, npix, models, status, mg);
   return cudaGetLastError();
 }
 
@@ -987,24 +1077,59 @@ bool waves_cover(const DevCfg& cfg, const InvertArgs& a) {
   return cfg.init_mode != 0 && !a.step_delta && !a.step_trial && !a.step_chi2_start && !a.step_chi2_trial;
 }
 
+// Shared memory of the wave kernels: the block's taps and its warps' blocks
+// (the trial kernel packs its warps at trial_warp_bytes).
+template <int LPL, int V, bool MG>
+constexpr size_t wave_trial_smem() { return tap_bytes<LPL>() + trial_warp_bytes<LPL, V>() * wave_warps<LPL, MG>(); }
+template <int LPL, int V, bool MG>
+constexpr size_t wave_accept_smem() { return tap_bytes<LPL>() + sizeof(WarpSmem<LPL, V>) * wave_warps<LPL, MG>(); }
+
+// Attributes of both wave kernels and their resident blocks per SM.
+template <int LPL, int V, bool MG>
+cudaError_t wave_occupancy(int* bt, int* ba) {
+  const size_t tsmem = wave_trial_smem<LPL, V, MG>(), smem = wave_accept_smem<LPL, V, MG>();
+  cudaError_t e =
+      cudaFuncSetAttribute(trial_kernel<LPL, V, MG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(accept_kernel<LPL, V, MG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int threads = wave_warps<LPL, MG>() * 32;
+  *bt = *ba = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(bt, trial_kernel<LPL, V, MG>, threads, tsmem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(ba, accept_kernel<LPL, V, MG>, threads, smem);
+  return (*bt < 1 || *ba < 1) ? cudaErrorInvalidConfiguration : cudaSuccess;
+}
+
+// The waves of one chunk: a pre-zeroed counter block, then per wave the
+// trial kernel over the pixels still iterating and the accept kernel over
+// those accepted.
+template <int LPL, int V, bool MG>
+cudaError_t run_waves(const DevCfg& dc, const InvertArgs& c, const WaveBuffers& b, const MultiGrid& mg, int gt,
+                      int ga, cudaStream_t s, int* count) {
+  const int waves = 1 + (dc.miter > 1 ? dc.miter : 1);
+  const int threads = wave_warps<LPL, MG>() * 32;
+  cudaError_t e = cudaMemsetAsync(b.w.cnt, 0, sizeof(WaveCounters) * (size_t)waves, s);
+  if (e != cudaSuccess) return e;
+  for (int wv = 0; wv < waves; ++wv) {
+    trial_kernel<LPL, V, MG><<<gt, threads, wave_trial_smem<LPL, V, MG>(), s>>>(dc, c, b.w, wv, mg);
+    ++*count;
+    // the last wave's pixels all stop: nothing to accept
+    if (wv + 1 < waves) {
+      accept_kernel<LPL, V, MG><<<ga, threads, wave_accept_smem<LPL, V, MG>(), s>>>(dc, c, b.w, wv, mg);
+      ++*count;
+    }
+  }
+  return cudaGetLastError();
+}
+
 template <int LPL, int V>
 cudaError_t launch_waves_t(const DevCfg& cfg, const InvertArgs& a, const WaveBuffers& b, cudaStream_t s,
                            int* launches) {
-  const size_t smem = smem_bytes<LPL, V>();
-  const size_t tsmem = tap_bytes<LPL>() + trial_warp_bytes<LPL, V>() * warps_per_block<LPL>();
-  cudaError_t e =
-      cudaFuncSetAttribute(trial_kernel<LPL, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(accept_kernel<LPL, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  const int threads = warps_per_block<LPL>() * 32;
   int dev = 0, sms = 0, bt = 0, ba = 0;
+  cudaError_t e = wave_occupancy<LPL, V, false>(&bt, &ba);
+  if (e != cudaSuccess) return e;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, trial_kernel<LPL, V>, threads, tsmem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ba, accept_kernel<LPL, V>, threads, smem);
-  if (bt < 1 || ba < 1) return cudaErrorInvalidConfiguration;
-  const int waves = 1 + (cfg.miter > 1 ? cfg.miter : 1);
   int count = 0;
   for (int64_t first = 0; first < a.npix; first += b.chunk) {
     const int64_t n = a.npix - first < b.chunk ? a.npix - first : b.chunk;
@@ -1013,22 +1138,70 @@ cudaError_t launch_waves_t(const DevCfg& cfg, const InvertArgs& a, const WaveBuf
     const int64_t need = (n + warps_per_block<LPL>() - 1) / warps_per_block<LPL>();
     const int gt = (int)(need < (int64_t)bt * sms ? need : (int64_t)bt * sms);
     const int ga = (int)(need < (int64_t)ba * sms ? need : (int64_t)ba * sms);
-    e = cudaMemsetAsync(b.w.cnt, 0, sizeof(WaveCounters) * (size_t)waves, s);
-    if (e != cudaSuccess) return e;
-    for (int wv = 0; wv < waves; ++wv) {
-      trial_kernel<LPL, V><<<gt, threads, tsmem, s>>>(dc, c, b.w, wv);
-      ++count;
-      // the last wave's pixels all stop: nothing to accept
-      if (wv + 1 < waves) {
-        accept_kernel<LPL, V><<<ga, threads, smem, s>>>(dc, c, b.w, wv);
-        ++count;
-      }
-    }
-    e = cudaGetLastError();
+    e = run_waves<LPL, V, false>(dc, c, b, MultiGrid{}, gt, ga, s, &count);
     if (e != cudaSuccess) return e;
   }
   if (launches) *launches = count;
   return cudaSuccess;
+}
+
+// Ragged batches: chunks of the batch's pixel list; profiles and fitted
+// profiles are addressed through mg.off, so only the per-pixel outputs,
+// start models and tables move with the chunk.
+template <int LPL, int V>
+cudaError_t launch_waves_mg_t(const DevCfg& cfg, const MultiGrid& mg, const InvertArgs& a, const WaveBuffers& b,
+                              int cap_t, int cap_a, cudaStream_t s, int* launches) {
+  int dev = 0, sms = 0, bt = 0, ba = 0;
+  cudaError_t e = wave_occupancy<LPL, V, true>(&bt, &ba);
+  if (e != cudaSuccess) return e;
+  if (cap_t > 0 && cap_t < bt) bt = cap_t;
+  if (cap_a > 0 && cap_a < ba) ba = cap_a;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int count = 0;
+  for (int64_t first = 0; first < a.npix; first += b.chunk) {
+    const int64_t n = a.npix - first < b.chunk ? a.npix - first : b.chunk;
+    InvertArgs c = offset_args(a, first, n, cfg.nl, cfg.nterms);
+    c.iquv = a.iquv;
+    c.fitted = a.fitted;
+    MultiGrid m = mg;
+    m.grid = mg.grid + first;
+    m.off = mg.off + first;
+    const int gt = (int)(n < (int64_t)bt * sms ? n : (int64_t)bt * sms);
+    const int ga = (int)(n < (int64_t)ba * sms ? n : (int64_t)ba * sms);
+    e = run_waves<LPL, V, true>(cfg, c, b, m, gt, ga, s, &count);
+    if (e != cudaSuccess) return e;
+  }
+  if (launches) *launches = count;
+  return cudaSuccess;
+}
+
+cudaError_t launch_invert_waves_mg(const DevCfg& cfg, const MultiGrid& mg, const InvertArgs& a,
+                                   const WaveBuffers& b, int cap_t, int cap_a, cudaStream_t s, int* launches) {
+  if (!waves_cover(cfg, a) || !a.init_status || b.chunk < 1 || b.chunk > 0x7fffffff || cfg.lambda_per_pixel ||
+      (cfg.use_slight && cfg.slight_per_pixel))
+    return cudaErrorInvalidValue;
+  const int v = kernel_variant(cfg, false);
+  if (cfg.nl <= 32) {
+    if (v == 0) return launch_waves_mg_t<1, 0>(cfg, mg, a, b, cap_t, cap_a, s, launches);
+    if (v == 1) return launch_waves_mg_t<1, 1>(cfg, mg, a, b, cap_t, cap_a, s, launches);
+    return launch_waves_mg_t<1, 2>(cfg, mg, a, b, cap_t, cap_a, s, launches);
+  }
+  if (v == 0) return launch_waves_mg_t<2, 0>(cfg, mg, a, b, cap_t, cap_a, s, launches);
+  if (v == 1) return launch_waves_mg_t<2, 1>(cfg, mg, a, b, cap_t, cap_a, s, launches);
+  return launch_waves_mg_t<2, 2>(cfg, mg, a, b, cap_t, cap_a, s, launches);
+}
+
+void waves_mg_occupancy(const DevCfg& cfg, int* bt, int* ba) {
+  const int v = kernel_variant(cfg, false);
+  cudaError_t e;
+  if (cfg.nl <= 32)
+    e = v == 0 ? wave_occupancy<1, 0, true>(bt, ba) : v == 1 ? wave_occupancy<1, 1, true>(bt, ba)
+                                                             : wave_occupancy<1, 2, true>(bt, ba);
+  else
+    e = v == 0 ? wave_occupancy<2, 0, true>(bt, ba) : v == 1 ? wave_occupancy<2, 1, true>(bt, ba)
+                                                             : wave_occupancy<2, 2, true>(bt, ba);
+  if (e != cudaSuccess) *bt = *ba = 0;
 }
 
 cudaError_t launch_invert_waves(const DevCfg& cfg, const InvertArgs& a, const WaveBuffers& b, cudaStream_t s,

@@ -115,6 +115,17 @@ inline DevCfg offset_cfg(const DevCfg& d, int64_t first) {
   return dc;
 }
 
+// Ragged batches: pixels of many wavelength grids in one launch.  Pixel p
+// runs on configuration cfgs[grid[p]] (its grid, PSF taps and stray profile;
+// everything else shared) and its profiles start at iquv + off[p] (floats),
+// its fitted profiles (when asked for) at fitted + off[p].  A launch holds
+// grids of one samples-per-lane class (all <= 32 or all 33..64 samples).
+struct MultiGrid {
+  const DevCfg* cfgs;          // device [grids]
+  const uint16_t* grid;        // [P] configuration index per pixel
+  const uint64_t* off;         // [P] offset of the pixel's [4][nl] block
+};
+
 struct SynthArgs {
   const float* models_f32;    // [P][11] (one of the two)
   const double* models_f64;
@@ -129,6 +140,18 @@ cudaError_t launch_invert(const DevCfg& cfg, const InvertArgs& a, int grid, cuda
 // stream s (waves_cover must hold); *launches receives the kernel count.
 cudaError_t launch_invert_waves(const DevCfg& cfg, const InvertArgs& a, const WaveBuffers& b, cudaStream_t s,
                                 int* launches);
+// The same for a ragged batch (one warp per block, the grid's constants
+// reloaded when a warp moves to a pixel of another grid): cfg is any of the
+// batch's configurations (they share everything but the grid, taps and stray
+// profile); a.init_models / a.init_status come from launch_classical_mg.
+// cap: resident blocks per SM of the trial / accept kernels (0: as many as fit).
+cudaError_t launch_invert_waves_mg(const DevCfg& cfg, const MultiGrid& mg, const InvertArgs& a,
+                                   const WaveBuffers& b, int cap_trial, int cap_accept, cudaStream_t s,
+                                   int* launches);
+cudaError_t launch_classical_mg(const DevCfg& cfg, const MultiGrid& mg, const float* iquv, int64_t npix,
+                                double* models, uint32_t* status, cudaStream_t s);
+// resident blocks per SM of the ragged-batch wave kernels (the autotuner's range)
+void waves_mg_occupancy(const DevCfg& cfg, int* trial_blocks, int* accept_blocks);
 cudaError_t launch_synth(const DevCfg& cfg, const SynthArgs& a, cudaStream_t s);
 // classical estimates: for_init false -> the classical-estimates mode
 // (S0 = B_los); true -> start models of an inversion plus status bits

@@ -34,6 +34,7 @@ PIX_LEARNED_INIT = 0x40
 MLP_IN, MLP_HIDDEN, MLP_OUT, MLP_OUT_PAD = 128, 256, 9, 16
 NUMERICS_REFERENCE, NUMERICS_ACCURATE = 0, 1
 KERNEL_AUTO, KERNEL_FUSED = 0, 1
+SERVE_ROUND_ROBIN, SERVE_FIFO, SERVE_SHORTEST_FIRST = 0, 1, 2
 
 # Symbols include/gmilos.h declares (checked by the tests against the .so).
 EXPORTS = ("gm_create", "gm_destroy", "gm_last_error", "gm_status_string", "gm_config_defaults",
@@ -41,7 +42,8 @@ EXPORTS = ("gm_create", "gm_destroy", "gm_last_error", "gm_status_string", "gm_c
            "gm_synthesize_grid", "gm_lm_step", "gm_submit", "gm_poll", "gm_cancel", "gm_zeeman_from_levels",
            "gm_psf_gaussian", "gm_psf_from_table", "gm_get_stats", "gm_measure_peaks", "gm_measure_sfu_peak",
            "gm_invert_noalloc", "gm_classical", "gm_serving_options", "gm_wave_state_bytes",
-           "gm_mlp_init", "gm_mlp_train_defaults", "gm_mlp_train", "gm_mlp_gradients", "gm_mlp_predict")
+           "gm_mlp_init", "gm_mlp_train_defaults", "gm_mlp_train", "gm_mlp_gradients", "gm_mlp_predict",
+           "gm_invert_rois", "gm_serving_policy")
 
 
 class GmError(RuntimeError):
@@ -102,6 +104,22 @@ class Request(C.Structure):
                 ("latency_ms", C.POINTER(C.c_double)), ("queue_ms", C.POINTER(C.c_double))]
 
 
+class Roi(C.Structure):
+    _fields_ = [("iquv", C.c_void_p), ("npix", C.c_int64), ("nl", C.c_int), ("lambda_", C.c_void_p),
+                ("psf", C.c_void_p), ("model", C.c_void_p), ("chi2", C.c_void_p), ("iters", C.c_void_p),
+                ("status", C.c_void_p)]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("use_graph", C.c_int), ("autotune", C.c_int)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("pixels", C.c_int64), ("grids", C.c_int), ("launches", C.c_int), ("graph_replayed", C.c_int),
+                ("cap_trial", C.c_int), ("cap_accept", C.c_int), ("device_ms", C.c_float),
+                ("lane_occupancy", C.c_double)]
+
+
 class Stats(C.Structure):
     _fields_ = [("pixels", C.c_int64), ("iterations", C.c_int64), ("accepted", C.c_int64),
                 ("kernel_ms", C.c_float), ("grid_blocks", C.c_int), ("block_threads", C.c_int),
@@ -136,6 +154,7 @@ def lib():
         L.gm_synthesize_grid.argtypes = [vp, vp, i64, vp, C.c_int, vp, vp]
         L.gm_classical.argtypes = [vp, vp, i64, C.c_int, vp, vp]
         L.gm_serving_options.argtypes = [vp, C.c_int, i64, C.c_int]
+        L.gm_serving_policy.argtypes = [vp, C.c_int]
         L.gm_submit.argtypes = [vp, C.POINTER(Request), C.POINTER(C.c_uint64)]
         L.gm_poll.argtypes = [vp, C.c_uint64, C.c_int]
         L.gm_cancel.argtypes = [vp, C.c_uint64]
@@ -154,6 +173,7 @@ def lib():
         L.gm_mlp_train.argtypes = [vp, C.POINTER(Mlp), vp, vp, i64, C.POINTER(TrainOpts), vp]
         L.gm_mlp_gradients.argtypes = [vp, C.POINTER(Mlp), vp, vp, i64, C.POINTER(Mlp), C.POINTER(C.c_float)]
         L.gm_mlp_predict.argtypes = [vp, C.POINTER(Mlp), vp, i64, vp, vp]
+        L.gm_invert_rois.argtypes = [vp, C.POINTER(Roi), C.c_int, C.POINTER(BatchOpts), C.POINTER(BatchStats), vp]
         _lib = L
     return _lib
 
@@ -443,6 +463,10 @@ class Engine:
         _check(lib().gm_serving_options(self._ctx, int(streams), int(chunk_pixels), int(max_active)),
                self._ctx)
 
+    def serving_policy(self, policy):
+        """SERVE_ROUND_ROBIN, SERVE_FIFO or SERVE_SHORTEST_FIRST (gm_serving_policy)."""
+        _check(lib().gm_serving_policy(self._ctx, int(policy)), self._ctx)
+
     def submit(self, iquv, model, chi2=None, iters=None, status=None, fix=None):
         """Queue an inversion (continuous batching).  The engine reads and
         writes the arrays until poll() returns for the ticket; this object
@@ -493,6 +517,34 @@ class Engine:
         a = C.c_double()
         _check(lib().gm_measure_sfu_peak(self._ctx, C.byref(a)), self._ctx)
         return a.value
+
+    # ------------------------------------------------------- ragged batches
+    def invert_rois(self, rois, use_graph=False, autotune=False, stream=None):
+        """Invert a ragged batch in one call (gm_invert_rois).  rois: list of
+        (iquv [P][4][nl], lambda [nl] absolute wavelengths, psf [nl] or None);
+        iquv numpy (host) or CUDA tensors (device).  Returns one output dict
+        per ROI (model [P][11], chi2, iters, status, in the ROI's memory
+        space) and the batch statistics."""
+        keep = []
+        arr = (Roi * max(1, len(rois)))()
+        outs = []
+        for i, (iquv, lam, psf) in enumerate(rois):
+            P, nl = int(iquv.shape[0]), int(iquv.shape[2])
+            lam = np.ascontiguousarray(lam, dtype=np.float64)
+            ps = None if psf is None else np.ascontiguousarray(psf, dtype=np.float64)
+            o = self._alloc_outputs(iquv, P, nl, False)
+            keep += [lam, ps, iquv]
+            r = arr[i]
+            r.iquv, r.npix, r.nl = _ptr(iquv), P, nl
+            r.lambda_ = lam.ctypes.data
+            r.psf = None if ps is None else ps.ctypes.data
+            r.model, r.chi2, r.iters, r.status = _ptr(o["model"]), _ptr(o["chi2"]), _ptr(o["iters"]), _ptr(o["status"])
+            outs.append({k: o[k] for k in ("model", "chi2", "iters", "status")})
+        opts = BatchOpts(int(bool(use_graph)), int(bool(autotune)))
+        st = BatchStats()
+        _check(lib().gm_invert_rois(self._ctx, arr, len(rois), C.byref(opts), C.byref(st),
+                                    C.c_void_p(stream) if stream else None), self._ctx)
+        return outs, {k: getattr(st, k) for k, _ in BatchStats._fields_}
 
     # ------------------------------------------------------- learned guess
     def mlp_train(self, net, iquv, truth, epochs=8, batch=16384, lr=2e-3, weight_decay=0.0, seed=1):

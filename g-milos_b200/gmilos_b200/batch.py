@@ -1,14 +1,14 @@
 """Ragged batches: regions of interest of any size and wavelength grid.
 
-Pixels are independent, so a batch of ROIs inverts as one engine call per
-distinct wavelength grid over the concatenated pixels of the ROIs on that
-grid: the kernels' work-stealing cursors take pixels of all of them alike,
-so ROI sizes do not matter.  The reference inverts one cube per
-run (gmilos.cu:1008-1249); this is the host-side loop a caller of it would
-write, done once.
+invert_rois hands a whole batch to the engine's gm_invert_rois: one
+persistent wave-synchronous launch sequence per samples-per-lane class (the
+grids of <= 32 samples and those of 33..64 run concurrently), in which
+every pixel carries its grid and a warp reloads the grid's constants when it
+moves to another grid, optionally captured in a CUDA graph and with its
+launch shape tuned on the first batch of a layout.  The reference inverts
+one cube on one grid per run (gmilos.cu:1008-1249).
 """
 import numpy as np
-
 
 GRID_ATOL = 1e-9   # A: grids closer than this everywhere are the same grid
 
@@ -27,42 +27,23 @@ def group_grids(lams, atol=GRID_ATOL):
         else:
             firsts.append(lam)
             idx.append(len(firsts) - 1)
-    return idx
+    return idx, firsts
 
 
-def invert_rois(engine, rois, config_for_grid, fitted=False):
+def invert_rois(engine, rois, psf_for_grid=None, use_graph=False, autotune=False):
     """Invert a ragged batch.  rois: list of (iquv [P_i][4][nl_i] float32,
-    lambda [nl_i] absolute wavelengths); config_for_grid(lam) returns the
-    engine configuration (make_config) for one grid.  Returns one output
-    dict per ROI (engine.invert's keys) and a summary: engine calls
-    ("launches", one per grid), pixels and
-    the lane occupancy (wavelength samples over lane slots, 32 per lane row
-    of up to 32 samples, 64 above)."""
-    groups = {}
-    gidx = group_grids([lam for _, lam in rois])
+    lambda [nl_i] absolute wavelengths); psf_for_grid(lam) gives the PSF taps
+    of a grid (None: no PSF).  The engine must be configured (line, weights,
+    free parameters, stop rule; its grid is not used).  Grids that agree to
+    GRID_ATOL share one configuration.  Returns one output dict per ROI
+    (model, chi2, iters, status) and the batch statistics (pixels, grids,
+    launches, lane_occupancy, device_ms, graph_replayed, tuned limits)."""
+    idx, firsts = group_grids([lam for _, lam in rois])
+    psfs = [None if psf_for_grid is None else psf_for_grid(f) for f in firsts]
+    batch = []
     for i, (iquv, lam) in enumerate(rois):
-        a = np.ascontiguousarray(iquv, dtype=np.float32)
+        a = iquv if hasattr(iquv, "data_ptr") else np.ascontiguousarray(iquv, dtype=np.float32)
         if a.ndim != 3 or a.shape[1] != 4 or a.shape[2] != len(lam):
             raise ValueError("ROI %d: iquv must be [P][4][nl] on its own grid" % i)
-        groups.setdefault(gidx[i], []).append((i, a, lam))
-    out = [None] * len(rois)
-    pixels = 0
-    slots = 0.0
-    samples = 0.0
-    for members in groups.values():
-        lam = members[0][2]
-        nl = len(lam)
-        cube = np.concatenate([a for _, a, _ in members], axis=0)
-        engine.configure(config_for_grid(lam))
-        res = engine.invert(cube, fitted=fitted)
-        start = 0
-        for i, a, _ in members:
-            n = len(a)
-            out[i] = {k: (None if v is None else v[start:start + n]) for k, v in res.items()}
-            start += n
-        pixels += len(cube)
-        samples += len(cube) * nl
-        slots += len(cube) * (32 if nl <= 32 else 64)
-    summary = {"launches": len(groups), "pixels": pixels,
-               "lane_occupancy": samples / slots if slots else 0.0}
-    return out, summary
+        batch.append((a, firsts[idx[i]], psfs[idx[i]]))
+    return engine.invert_rois(batch, use_graph=use_graph, autotune=autotune)

@@ -272,6 +272,54 @@ gm_status gm_synthesize_f64(gm_ctx *ctx, const double *models, int64_t npix, flo
 gm_status gm_synthesize_grid(gm_ctx *ctx, const double *models, int64_t npix,
                              const double *offsets_A, int ngrid, float *iquv, void *stream);
 
+/* ---------------- ragged batches ------------------------------------------ */
+/* A batch of regions of interest, each with its own size and wavelength
+ * grid, inverted by one persistent wave-synchronous launch sequence per
+ * samples-per-lane class (grids of <= 32 samples, grids of 33..64; the two
+ * run concurrently): every pixel carries its grid's index and its profiles'
+ * offset, and a warp reloads the grid's constants (offsets, PSF taps) when
+ * it moves to a pixel of another grid, so ROIs of any size and grid share
+ * the work-stealing waves and pixels that converge early leave them.  The
+ * context's configuration supplies everything but the grids and PSF taps
+ * (classical start models; no stray light, no learned guess, no per-pixel
+ * grids).  The reference inverts one cube on one grid per run
+ * (gmilos.cu:1008-1249); no counterpart. */
+typedef struct {
+    const float *iquv;            /* [P][4][nl] host or device */
+    int64_t npix;
+    int nl;                       /* 2..GM_MAX_NL */
+    const double *lambda;         /* [nl] absolute wavelengths [A] (host) */
+    const double *psf;            /* [nl] taps centred at nl/2 (host), or NULL: no PSF */
+    float *model;                 /* [P][11] */
+    float *chi2;                  /* [P] (optional) */
+    int *iters;                   /* [P] (optional) */
+    uint32_t *status;             /* [P] (optional) */
+} gm_roi;
+
+typedef struct {
+    int use_graph;                /* capture the device work of a batch in a CUDA
+                                     graph and replay it for later batches of the
+                                     same layout (sizes, grids) */
+    int autotune;                 /* on the first batch of a layout, time the
+                                     resident-block limits of the two wave kernels
+                                     (full, 3/4, 1/2) and keep the fastest */
+} gm_batch_opts;
+
+typedef struct {
+    int64_t pixels;
+    int grids;                    /* distinct wavelength grids (with their taps) */
+    int launches;                 /* engine kernels launched (inside the graph too) */
+    int graph_replayed;           /* 1: the device work was a replayed graph */
+    int cap_trial, cap_accept;    /* resident blocks per SM used (tuned or full) */
+    float device_ms;              /* device time of the batch's kernels */
+    double lane_occupancy;        /* wavelength samples over lane slots, weighted by
+                                     each pixel's trials (sum nl (it + 1) over
+                                     sum 32 LPL (it + 1)) */
+} gm_batch_stats;
+
+gm_status gm_invert_rois(gm_ctx *ctx, const gm_roi *rois, int nroi, const gm_batch_opts *opts,
+                         gm_batch_stats *stats, void *stream);
+
 /* ---------------- serving (continuous batching) --------------------------- */
 /* Requests (frames or ROIs of any size) are admitted in arrival order as
  * slots and device memory free up: at most max_active at a time, their
@@ -304,6 +352,17 @@ typedef struct {
 /* before the first gm_submit: lanes (1..32, default 4), pixels per chunk
  * (default 65536), admitted requests at a time (default 16) */
 gm_status gm_serving_options(gm_ctx *ctx, int streams, int64_t chunk_pixels, int max_active);
+/* Which admitted request a free lane serves next (any time):
+ * GM_SERVE_ROUND_ROBIN (default) -- the admitted requests in turn, so each
+ *   progresses at the same rate and a request's latency grows with its size;
+ * GM_SERVE_FIFO -- the earliest submitted first, so requests finish in
+ *   arrival order and under load every request waits about as long;
+ * GM_SERVE_SHORTEST_FIRST -- the fewest pixels left first (the lowest mean
+ *   latency; large requests wait behind small ones). */
+#define GM_SERVE_ROUND_ROBIN 0
+#define GM_SERVE_FIFO 1
+#define GM_SERVE_SHORTEST_FIRST 2
+gm_status gm_serving_policy(gm_ctx *ctx, int policy);
 gm_status gm_submit(gm_ctx *ctx, const gm_request *req, gm_ticket *ticket);
 /* wait for a request (timeout_us < 0: no limit); consumes the ticket */
 gm_status gm_poll(gm_ctx *ctx, gm_ticket ticket, int timeout_us);

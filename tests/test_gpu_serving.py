@@ -150,3 +150,32 @@ def test_concurrent_submitters():
             x.join(timeout=120)
     for k in range(6):
         np.testing.assert_array_equal(results[k], alone(data[k], FIX9A)["model"])
+
+
+@pytest.mark.parametrize("policy", [G.SERVE_FIFO, G.SERVE_SHORTEST_FIRST])
+def test_every_policy_gives_the_lone_results(policy):
+    """The serving policies decide only which request's chunk a free lane
+    takes next: results stay those of each request inverted alone, and the
+    shortest-first policy finishes a small request submitted after a large
+    one first."""
+    sizes = [60000, 500, 3000]
+    data = [cube(n, 200 + k) for k, n in enumerate(sizes)]
+    _, gcfg, _ = config()
+    with G.Engine(0) as e:
+        e.configure(gcfg)
+        e.serving_options(streams=2, chunk_pixels=4096, max_active=4)
+        e.serving_policy(policy)
+        outs = [(np.empty((n, 11), np.float32), np.empty(n, np.float32)) for n in sizes]
+        tickets = [e.submit(d, o[0], chi2=o[1]) for d, o in zip(data, outs)]
+        lat = []
+        for t in tickets:
+            assert e.poll(t) == 0
+            lat.append(e.last_latency_ms)
+        with pytest.raises(G.GmError):
+            e.serving_policy(7)
+    for d, (model, chi2) in zip(data, outs):
+        ref = alone(d, FIX9A)
+        np.testing.assert_array_equal(model, ref["model"])
+        np.testing.assert_array_equal(chi2, ref["chi2"])
+    if policy == G.SERVE_SHORTEST_FIRST:
+        assert lat[1] < lat[0]
