@@ -39,13 +39,17 @@ NOISE = 1e-3
 GUESS = (40.0, 1000.0, 0.2, 0.03, 0.05, 150.0, 110.0, 0.35, 0.5, 0.0, 1.0)   # run/guess.mod
 FIX = (1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 1)          # 9 ME parameters + alpha
 STRAY_MODEL = (10.0, 0.0, 0.0, 0.03, 0.1, 0.0, 0.0, 0.3, 0.7, 0.0, 1.0)
+# --vmac-free: the reference's 11-term path (v_mac and alpha both free), v_mac starting at 0.5 km/s
+FIX11 = (1,) * 11
+GUESS_VMAC = GUESS[:9] + (0.5, 1.0)
 MAXITER = 50
 
 # DRAM bytes (read + write) per pixel of one inversion (classical pre-pass
 # and every trial / accept wave), measured with ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum summed over the launches) on a 65 536-pixel inversion
-# of this workload; traffic grows with the pixel count.
-DRAM_BYTES_PER_PIXEL = 222113.0
+# dram__bytes_write.sum summed over the 102 launches of an inversion) on
+# 65 536-pixel inversions of this workload with the current kernels;
+# traffic grows with the pixel count.
+DRAM_BYTES_PER_PIXEL = 223300.0
 
 # Algorithmic FLOPs per pixel (per-wavelength costs counted from the formulas)
 C_VOIGT, C_RTE, C_DVOIGT, C_DRTE = 100, 85, 23, 870
@@ -230,7 +234,8 @@ def run_engine(args):
     fine, W = fine_operator(off)
     sl_fine = eng.synthesize_grid(np.array([STRAY_MODEL]), np.ascontiguousarray(fine / 1000.0))
     slight = (sl_fine @ W.T.astype(np.float32))[0].astype(np.float32)
-    cfg = G.make_config(lam, LAMBDA0, zee, psf=psf, fix=FIX, init=GUESS, miter=MAXITER, slight=slight)
+    fix, guess = (FIX11, GUESS_VMAC) if args.vmac_free else (FIX, GUESS)
+    cfg = G.make_config(lam, LAMBDA0, zee, psf=psf, fix=fix, init=guess, miter=MAXITER, slight=slight)
     eng.configure(cfg)
 
     rng = np.random.default_rng(args.seed + rank)
@@ -309,7 +314,7 @@ def run_engine(args):
     d2h = (model_h.numel() + chi_h.numel() + it_h.numel()) * 4
 
     # roofline of the inversion kernel: algorithmic FLOPs / launch duration
-    ftr, facc, finit = flops_model(nl, nl, n_free=sum(FIX), s0_free=FIX[7], psf=True, stray=True)
+    ftr, facc, finit = flops_model(nl, nl, n_free=sum(fix), s0_free=fix[7], psf=True, stray=True)
     flops_launch = P * finit + iters_sum * ftr + acc_sum * facc
     launch_avg = float(np.mean(launch_ms))
     achieved = flops_launch / (launch_avg / 1e3) / 1e12
@@ -330,7 +335,8 @@ def run_engine(args):
         "config": {"workload": "full cube %dx%d px x 4 Stokes x 30 lambda, Fe I 6173 A, PSF FWHM 100 mA "
                                "(1 mA table), stray light alpha 0.7-1.0, noise 1e-3 Ic" % (int(np.sqrt(P)), int(np.sqrt(P))) if int(np.sqrt(P)) ** 2 == P
                                else "%d px x 4 x 30 lambda, PSF, stray light" % P,
-                   "pixels_per_gpu": P, "nlambda": nl, "free_parameters": int(sum(FIX)), "max_iterations": MAXITER,
+                   "pixels_per_gpu": P, "nlambda": nl, "free_parameters": int(sum(fix)), "max_iterations": MAXITER,
+                   "terms": 11 if args.vmac_free else 10,
                    "mean_iterations": iters_sum / P, "mean_accepted": acc_sum / P,
                    "l2_policy": "inputs 480 MB per GPU > 126 MB L2, no flush", "parallelism": "replicas (weak scaling, no collective)"},
         "e2e": {"value": e2e_value, "unit": "pixels/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -920,6 +926,8 @@ def main():
                     help="pixels/s of an unloaded host-memory inversion (the stretch's denominator)")
     ap.add_argument("--serve-sweep", default="",
                     help="comma-separated arrival rates: run only the serving stream at each (one JSON line)")
+    ap.add_argument("--vmac-free", action="store_true",
+                    help="free v_mac too (the reference's 11-term path, lm_mils_11), v_mac starting at 0.5 km/s")
     ap.add_argument("--no-config1", dest="config1", action="store_false",
                     help="skip the 64x64 no-PSF case (engine and the reference's CPU routines)")
     ap.add_argument("--mlp-train-pixels", type=int, default=1 << 22,

@@ -136,7 +136,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
           solved = !reuse;
           if (lane == 0) apply_delta_check<10>(c, sm.m, sm.vec[reuse ? 1 : 0][0], sm.t);
         } else {
-          solve11<LPL, V>(sm, plan11, flambda, lane);
+          if (!solve11_elim<LPL, V>(sm, flambda, lane)) solve11<LPL, V>(sm, plan11, flambda, lane);
           if (lane == 0) apply_delta_check<11>(c, sm.m, sm.dd, sm.t);
         }
         __syncwarp();
@@ -482,7 +482,7 @@ trial_kernel(const DevCfg c0, const InvertArgs a, const WaveArgs w, int wave, co
       }
       __syncwarp();
       if constexpr (NT == 11) {
-        solve11<LPL, V>(sm, plan11, flambda, lane);
+        if (!solve11_elim<LPL, V>(sm, flambda, lane)) solve11<LPL, V>(sm, plan11, flambda, lane);
         if (lane == 0) apply_delta_check<11>(c, sm.m, sm.dd, sm.t);
       } else {
         if (!reuse) {

@@ -96,22 +96,36 @@ def test_graph_replay_and_tuning_change_nothing(engine, rois):
                 np.testing.assert_array_equal(p[k], g[k], err_msg=k)
 
 
-def test_batch_against_plain_inversions(engine, rois):
+@pytest.mark.parametrize("numerics", [G.NUMERICS_REFERENCE, G.NUMERICS_ACCURATE])
+def test_batch_against_plain_inversions(engine, rois, numerics):
     """The ragged-batch kernels and the one-grid wave kernels run the same
-    LM arithmetic; compiled as other kernels they may round differently."""
-    engine.configure(base_config())
+    LM arithmetic.  At <= 32 samples they compile to the same results bit
+    for bit; at 33..64 samples they round differently, and in REFERENCE
+    numerics (hardware trigonometry in the solve) the trajectories then part
+    on some pixels as between any two builds: neither side is worse more
+    often, and in ACCURATE numerics the fits agree on nearly every pixel."""
+    engine.configure(base_config(numerics=numerics))
     got, _ = batch.invert_rois(engine, rois, psf_for)
-    agree, tot = 0, 0
+    worse_b, worse_p, agree, tot = 0, 0, 0, 0
     for (a, lam), g in zip(rois[1:6], got[1:6]):
-        engine.configure(G.make_config(lam, L0, ZG, psf=psf_for(lam), init=H.GUESS, stop_dchi2=STOP))
+        engine.configure(G.make_config(lam, L0, ZG, psf=psf_for(lam), init=H.GUESS, stop_dchi2=STOP,
+                                       numerics=numerics))
         ref = engine.invert(a)
-        ok = H.fits_agree(np.asarray(g["model"], dtype=np.float64), ref["model64"]) | (g["chi2"] <= ref["chi2"])
-        agree += int(ok.sum())
+        same = H.fits_agree(np.asarray(g["model"], dtype=np.float64), ref["model64"])
+        wb = ~same & (g["chi2"] > ref["chi2"] * (1 + 1e-3) + 1e-6)
+        wp = ~same & (ref["chi2"] > g["chi2"] * (1 + 1e-3) + 1e-6)
+        agree += int(same.sum())
+        worse_b += int(wb.sum())
+        worse_p += int(wp.sum())
         tot += len(a)
-        same = (g["iters"] == ref["iters"]).mean()
-        print("nl %d: agree or chi2 no worse %.4f, same trial count %.4f, bit-identical models %.4f"
-              % (len(lam), ok.mean(), same, (g["model"] == ref["model"]).all(axis=1).mean()))
-    assert agree / tot >= 0.97
+        bitwise = (g["model"] == ref["model"]).all(axis=1).mean()
+        print("numerics %d, nl %d: agree %.4f, batch worse %.4f, plain worse %.4f, bit-identical models %.4f"
+              % (numerics, len(lam), same.mean(), wb.mean(), wp.mean(), bitwise))
+        if len(lam) <= 32:
+            assert bitwise == 1.0
+    assert worse_b / tot <= worse_p / tot + 0.02
+    if numerics == G.NUMERICS_ACCURATE:
+        assert agree / tot >= 0.97
 
 
 def test_batch_against_the_oracle(engine, rois):
