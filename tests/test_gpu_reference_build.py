@@ -123,10 +123,13 @@ def test_inversions_match_reference_gpu_build(engine):
 def test_one_iteration_reference_numerics_vs_reference_gpu_build(engine, psf, stray):
     """One LM iteration (miter = 1, classical-estimate start) in REFERENCE
     numerics -- the reference's __sincosf / __fdividef in the solve and the
-    angles -- against the reference's own sm_100a build.  The engine forms
-    the normal equations in FP64 on the tensor cores where the reference
-    sums them in FP32 (lib.cu:65-118); the 18-step Jacobi with the hardware
-    trigonometry amplifies those last-bit differences of alpha into step
+    angles -- against the reference's own sm_100a build.  The two builds
+    round the synthesis, the response functions and the normal equations
+    differently (FMA contraction chosen by two compilations; the engine's
+    normal equations in FP64 on the tensor cores where the reference sums
+    them in FP32, lib.cu:65-118 -- on the CPU restatement that difference
+    alone moves one step by p99 1.5e-5), and the 18-step Jacobi with the
+    hardware trigonometry amplifies last-bit differences of alpha into step
     differences (measured: model p99 5e-5 to 1e-4, chi2 p99 1.4e-4 to
     1.9e-4, 99.4-99.7 % of pixels within 1e-3, the largest difference 5 % of
     a parameter -- a step-size difference, far below a whole step, so no
