@@ -482,7 +482,7 @@ def serving_latency(eng, obs_h, args, rate=None, n=None):
             "requests": n, "pixels": int(npix.sum())}
 
 
-SERVE_POLICIES = {"round_robin": 0, "fifo": 1, "shortest_first": 2}
+SERVE_POLICIES = {"round_robin": 0, "fifo": 1, "shortest_first": 2, "response_ratio": 3}
 
 
 def run_serve_sweep(args):
@@ -920,7 +920,7 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=1.0, help="mean arrivals per second")
     ap.add_argument("--serve-side-min", type=int, default=256)
     ap.add_argument("--serve-side-max", type=int, default=2048)
-    ap.add_argument("--serve-policy", default="round_robin", choices=sorted(SERVE_POLICIES))
+    ap.add_argument("--serve-policy", default="response_ratio", choices=sorted(SERVE_POLICIES))
     ap.add_argument("--serve-budget-gb", type=int, default=150, help="HBM budget of the serving context")
     ap.add_argument("--serve-unloaded-rate", type=float, default=3.1e6,
                     help="pixels/s of an unloaded host-memory inversion (the stretch's denominator)")

@@ -105,7 +105,7 @@ struct gm_ctx {
   int serve_streams = 4;
   int64_t serve_chunk = 65536;        // pixels per launch
   int serve_max_active = 16;
-  int serve_policy = GM_SERVE_ROUND_ROBIN;   // which admitted request a free lane takes
+  int serve_policy = GM_SERVE_RESPONSE_RATIO;   // which admitted request a free lane takes
   size_t rr = 0;                      // round-robin cursor over active requests
   gm_ticket next_ticket = 1;
   std::thread worker;
@@ -959,10 +959,10 @@ gm_status gm_measure_sfu_peak(gm_ctx* ctx, double* gops) {
 // within the context's HBM budget.  Admitted requests are cut into chunks
 // of serve_chunk pixels; a dispatcher thread keeps each of serve_streams
 // lanes (a stream with its own work counters) busy with the next chunk of
-// the admitted requests in round-robin order, so chunks of different
-// requests overlap on the device and a newly admitted request starts within
-// one chunk time.  Pixels are independent, so every result is the same
-// whatever the mix it ran in.
+// the admitted request the serving policy picks, so chunks of different
+// requests overlap on the device (with round robin a newly admitted request
+// starts within one chunk time).  Pixels are independent, so every result
+// is the same whatever the mix it ran in.
 namespace {
 
 size_t request_bytes(const gm_request& q) {
@@ -1019,7 +1019,8 @@ gm_status gm_serving_options(gm_ctx* ctx, int streams, int64_t chunk_pixels, int
 
 gm_status gm_serving_policy(gm_ctx* ctx, int policy) {
   if (!ctx) return GM_ERR_INVALID;
-  if (policy != GM_SERVE_ROUND_ROBIN && policy != GM_SERVE_FIFO && policy != GM_SERVE_SHORTEST_FIRST)
+  if (policy != GM_SERVE_ROUND_ROBIN && policy != GM_SERVE_FIFO && policy != GM_SERVE_SHORTEST_FIRST &&
+      policy != GM_SERVE_RESPONSE_RATIO)
     return fail(ctx, GM_ERR_INVALID, "unknown serving policy");
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->serve_policy = policy;
@@ -1235,12 +1236,16 @@ void serve_loop(gm_ctx* ctx) {
     }
     // keep every lane busy with the next chunk of the request the policy
     // picks: round robin over the admitted requests, the earliest submitted,
-    // or the one with the fewest pixels left
+    // the one with the fewest pixels left, or the one with the highest
+    // response ratio (time since submission over its pixels; compared
+    // cross-multiplied)
     for (ServeLane& L : ctx->lanes) {
       if (L.busy) continue;
       std::shared_ptr<Request> pick;
       {
         std::lock_guard<std::mutex> lk(ctx->mu);
+        const Clock::time_point now = Clock::now();
+        auto waited = [&](const Request& q) { return std::chrono::duration<double>(now - q.t_submit).count(); };
         const size_t n = ctx->active.size();
         for (size_t k = 0; k < n; ++k) {
           const size_t i = (ctx->rr + k) % n;
@@ -1250,6 +1255,8 @@ void serve_loop(gm_ctx* ctx) {
           if (pick && ctx->serve_policy == GM_SERVE_FIFO) better = c->t_submit < pick->t_submit;
           if (pick && ctx->serve_policy == GM_SERVE_SHORTEST_FIRST)
             better = c->req.npix - c->next < pick->req.npix - pick->next;
+          if (pick && ctx->serve_policy == GM_SERVE_RESPONSE_RATIO)
+            better = waited(*c) * (double)pick->req.npix > waited(*pick) * (double)c->req.npix;
           if (better) {
             pick = c;
             if (ctx->serve_policy == GM_SERVE_ROUND_ROBIN) {
@@ -1719,6 +1726,8 @@ gm_status gm_mlp_predict(gm_ctx* ctx, const gm_mlp* net, const float* iquv, int6
   Arg a_in, a_out;
   gm_status st;
   if ((st = stage_in(ctx, "iquv", iquv, sizeof(float) * 4 * (size_t)nl * n, &a_in, s)) != GM_OK) return st;
+  if (reinterpret_cast<uintptr_t>(a_in.dev) & 15u)
+    return fail(ctx, GM_ERR_INVALID, "device profiles must start on a 16-byte boundary");
   if ((st = stage_out(ctx, "pmodels", models, sizeof(double) * 11 * (size_t)n, &a_out)) != GM_OK) return st;
   gm::mlp::DevNet d;
   cudaError_t e = gm::mlp::devnet_create(&d, net, s);

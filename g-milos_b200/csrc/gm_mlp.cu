@@ -40,7 +40,12 @@ namespace gm {
 namespace mlp {
 namespace {
 
-constexpr int kThreads = 128;                 // 4 warps: one tensor-memory lane quarter each
+// Inference and training kernels: 8 warps, two per tensor-memory lane
+// quarter -- warp w reads rows 32 (w % 4) .. + 31 of the accumulator, and
+// the two warpgroups split each epilogue's columns (and the input features)
+// in halves.  The weight-gradient kernel: 4 warps, one row each.
+constexpr int kThreads = 256;
+constexpr int kWThreads = 128;
 constexpr uint64_t kWaitNs = 2000000000ull;   // a wait gives up after 2 s
 
 // error codes written to the kernel's error word
@@ -76,8 +81,8 @@ __device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
 // Wait for the phase of barrier b with the given parity.  Returns false when
 // it gave up: after kWaitNs (it then records `code` in *err and raises the
 // block's abort flag) or as soon as another thread has raised the flag.
-__device__ __noinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort, int* err, int code,
-                                       bool stop_on_abort = true) {
+__device__ __noinline__ bool mbar_wait_slow(uint64_t* b, uint32_t parity, volatile int* abort, int* err, int code,
+                                            bool stop_on_abort) {
   const uint64_t t0 = now_ns();
   while (!mbar_test(b, parity)) {
     if (stop_on_abort && *abort) return false;
@@ -88,6 +93,14 @@ __device__ __noinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile in
     }
   }
   return true;
+}
+// The phase is usually complete by the time a thread asks (a weight block
+// loaded during the previous products, the products during the epilogue):
+// one test inline, the bounded loop out of line.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort, int* err, int code,
+                                          bool stop_on_abort = true) {
+  if (mbar_test(b, parity)) return true;
+  return mbar_wait_slow(b, parity, abort, err, code, stop_on_abort);
 }
 
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -151,8 +164,10 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                : "memory");
 }
 // 32 consecutive columns of this thread's tensor-memory lane
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-  uint32_t r[32];
+// 32 columns of this warp's 32 lanes: the load is asynchronous; its
+// registers are valid after tmem_wait32 on the same array, whose asm takes
+// them as operands so that no read of them is placed before the wait.
+__device__ __forceinline__ void tmem_issue32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
       "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
@@ -162,7 +177,21 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
         "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
         "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait32(uint32_t (&r)[32]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                 "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                 "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]),
+                 "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]),
+                 "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+               :
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  tmem_issue32(taddr, r);
+  tmem_wait32(r);
 #pragma unroll
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
@@ -174,7 +203,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                 "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                 "+r"(r[15])
+               :
+               : "memory");
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
@@ -192,10 +226,22 @@ __device__ __forceinline__ void st_chunk(uint32_t atom, int r, int j, const uint
                : "memory");
 }
 
-// GELU with the error function, and its derivative
-__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel, 2016): z (1 + tanh u) / 2 with
+// u = sqrt(2 / pi) (z + 0.044715 z^3), written as z s, s = 1 / (1 + exp(-2 u))
+// -- one exponential and one reciprocal on the special-function unit -- and
+// its derivative s + z s (1 - s) d(2u)/dz.
+__device__ __forceinline__ float gelu_s(float z, float* du2) {
+  const float z2 = z * z;
+  const float u2 = 1.5957691216057308f * z * (1.f + 0.044715f * z2);
+  if (du2) *du2 = 1.5957691216057308f * (1.f + 0.134145f * z2);
+  // exp(80) keeps the denominator inside the fast reciprocal's range
+  return __fdividef(1.f, 1.f + __expf(fminf(-u2, 80.f)));
+}
+__device__ __forceinline__ float gelu(float z) { return z * gelu_s(z, nullptr); }
 __device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+  float du2;
+  const float s = gelu_s(z, &du2);
+  return s + z * s * (1.f - s) * du2;
 }
 
 
@@ -206,7 +252,9 @@ constexpr uint32_t kSW = 65536;        // weight ring: 2 stages x 64 KB
 constexpr uint32_t kStage = 65536;
 constexpr uint32_t kSD = 196608;       // output-gradient operand: 1 atom [128 x 64]
 constexpr uint32_t kSBar = 212992;     // barriers, tensor-memory address, abort flag
-constexpr size_t kSmemBytes = kSBar + 128 + 1024;
+constexpr uint32_t kSPar = kSBar + 128; // b1, b2, in_mean, in_scale (floats), read by every tile
+constexpr int kParFloats = 256 + 256 + 128 + 128;
+constexpr size_t kSmemBytes = kSPar + 4 * kParFloats + 1024;
 
 struct NetMaps {
   CUtensorMap m[5];                    // w1b, w2b, w3b, w2tb, w3tb
@@ -317,55 +365,95 @@ __device__ bool run_job(const Job& j, const Job* next, bool train, const NetMaps
 }
 
 // Load a tile's inputs (batch rows row0.., pixel idx[row] or the row itself)
-// standardised and rounded to BF16 into the activation atoms 0-1.
-__device__ __forceinline__ void load_x(const gm_mlp* __restrict__ P, const float* __restrict__ iquv,
+// standardised and rounded to BF16 into the activation atoms 0-1; this
+// thread's row r, features [64 half, 64 half + 64) (atom `half`).  Rows of
+// 4 nl floats start on 16-byte boundaries and the feature count is a
+// multiple of 4, so every 4-feature group is read whole or not at all.
+__device__ __forceinline__ void load_x(const float* spar, const float* __restrict__ iquv,
                                        const uint32_t* __restrict__ idx, int64_t row0, int64_t n, int nl,
-                                       uint32_t sA, int r) {
+                                       uint32_t sA, int r, int half) {
   const int64_t b = row0 + r;
   const int F = 4 * nl;
-  const float* src = nullptr;
-  if (b < n) src = iquv + (idx ? (int64_t)idx[b] : b) * F;
-#pragma unroll 1
-  for (int c = 0; c < 16; ++c) {
-    uint32_t w[4];
+  const float4* src = nullptr;
+  if (b < n) src = reinterpret_cast<const float4*>(iquv + (idx ? (int64_t)idx[b] : b) * F);
+  const float4* mean = reinterpret_cast<const float4*>(spar + 512);
+  const float4* scale = reinterpret_cast<const float4*>(spar + 640);
+#pragma unroll 2
+  for (int c = 8 * half; c < 8 * half + 8; ++c) {
+    float v[8];
 #pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      float v[2];
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int f = 8 * c + 2 * h + e;
-        v[e] = (src && f < F) ? (__ldg(src + f) - P->in_mean[f]) * P->in_scale[f] : 0.f;
+    for (int g = 0; g < 2; ++g) {
+      const int f4 = 2 * c + g;   // 4-feature group
+      float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (src && 4 * f4 < F) {
+        const float4 xi = __ldg(src + f4), mu = mean[f4], sc = scale[f4];
+        x = make_float4((xi.x - mu.x) * sc.x, (xi.y - mu.y) * sc.y, (xi.z - mu.z) * sc.z, (xi.w - mu.w) * sc.w);
       }
-      w[h] = pack_bf16(v[0], v[1]);
+      v[4 * g] = x.x;
+      v[4 * g + 1] = x.y;
+      v[4 * g + 2] = x.z;
+      v[4 * g + 3] = x.w;
     }
+    const uint32_t w[4] = {pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]),
+                           pack_bf16(v[6], v[7])};
     st_chunk(sA + (c >> 3) * 16384u, r, c & 7, w);
   }
 }
 
 // Epilogue of a hidden layer over the accumulator at tensor column zcol:
 // h = GELU(z + bias) into the activation atoms (K = feature); with zspill,
-// z + bias also to zspill[0..256) (this row).
-__device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, uint32_t zcol, const float* __restrict__ bias,
-                                                uint32_t sA, int r, float* zspill) {
-#pragma unroll 1
-  for (int q = 0; q < 8; ++q) {
-    float z[32];
-    tmem_ld32(tmem_row + zcol + 32 * q, z);
+// z + bias also to zspill[0..256) (this row).  This thread: row r, columns
+// [128 half, 128 half + 128) (atoms 2 half, 2 half + 1), 32 at a time, the
+// next 32 columns' tensor-memory load in flight while these are processed.
+// bias: 256 floats in shared memory.
+__device__ __forceinline__ void hidden_chunk(const uint32_t (&zr)[32], int q, const float* bias, uint32_t sA,
+                                             int r, float* zspill) {
+  float z[32];
+  const float4* b4 = reinterpret_cast<const float4*>(bias + 32 * q);
 #pragma unroll
-    for (int e = 0; e < 32; ++e) z[e] += __ldg(bias + 32 * q + e);
-    if (zspill) {
-      float4* dst = reinterpret_cast<float4*>(zspill + 32 * q);
-#pragma unroll
-      for (int u = 0; u < 8; ++u) dst[u] = make_float4(z[4 * u], z[4 * u + 1], z[4 * u + 2], z[4 * u + 3]);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      uint32_t w[4];
-#pragma unroll
-      for (int h = 0; h < 4; ++h) w[h] = pack_bf16(gelu(z[8 * u + 2 * h]), gelu(z[8 * u + 2 * h + 1]));
-      st_chunk(sA + (q >> 1) * 16384u, r, (q & 1) * 4 + u, w);
-    }
+  for (int u = 0; u < 8; ++u) {
+    const float4 bv = b4[u];
+    z[4 * u] = __uint_as_float(zr[4 * u]) + bv.x;
+    z[4 * u + 1] = __uint_as_float(zr[4 * u + 1]) + bv.y;
+    z[4 * u + 2] = __uint_as_float(zr[4 * u + 2]) + bv.z;
+    z[4 * u + 3] = __uint_as_float(zr[4 * u + 3]) + bv.w;
   }
+  if (zspill) {
+    float4* dst = reinterpret_cast<float4*>(zspill + 32 * q);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) dst[u] = make_float4(z[4 * u], z[4 * u + 1], z[4 * u + 2], z[4 * u + 3]);
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    uint32_t w[4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) w[h] = pack_bf16(gelu(z[8 * u + 2 * h]), gelu(z[8 * u + 2 * h + 1]));
+    st_chunk(sA + (q >> 1) * 16384u, r, (q & 1) * 4 + u, w);
+  }
+}
+
+__device__ __forceinline__ void hidden_epilogue(uint32_t tmem_row, uint32_t zcol, const float* bias, uint32_t sA,
+                                                int r, int half, float* zspill) {
+  const int q0 = 4 * half;
+  const uint32_t t0 = tmem_row + zcol + 32 * q0;
+  uint32_t za[32], zb[32];
+  tmem_issue32(t0, za);
+#pragma unroll
+  for (int j = 0; j < 4; j += 2) {
+    tmem_wait32(za);
+    tmem_issue32(t0 + 32 * (j + 1), zb);
+    hidden_chunk(za, q0 + j, bias, sA, r, zspill);
+    tmem_wait32(zb);
+    if (j + 2 < 4) tmem_issue32(t0 + 32 * (j + 2), za);
+    hidden_chunk(zb, q0 + j + 1, bias, sA, r, zspill);
+  }
+}
+
+// The parameters every tile reads (b1, b2, in_mean, in_scale) into the
+// shared-memory block at spar, once per launch.
+__device__ __forceinline__ void stage_params(const gm_mlp* __restrict__ P, float* spar) {
+  for (int i = threadIdx.x; i < kParFloats; i += blockDim.x)
+    spar[i] = i < 256 ? P->b1[i] : (i < 512 ? P->b2[i - 256] : (i < 640 ? P->in_mean[i - 512] : P->in_scale[i - 640]));
 }
 
 // Outputs (de-standardised) -> start model (Init_Model layout) within the
@@ -470,15 +558,18 @@ mlp_infer_kernel(const __grid_constant__ NetMaps nm, const InferArgs a) {
   const uint32_t base = (saddr(smem_raw) + 1023u) & ~1023u;
   Bars* B = reinterpret_cast<Bars*>(smem_raw + (base - saddr(smem_raw)) + kSBar);
   const int tid = threadIdx.x, warp = tid >> 5;
+  const int row = tid & (kTile - 1), half = tid >> 7;   // accumulator row, column half
+  float* spar = reinterpret_cast<float*>(smem_raw + (base - saddr(smem_raw)) + kSPar);
+  stage_params(a.p, spar);
   setup(B, 256);
-  const uint32_t trow = B->tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t trow = B->tmem + ((uint32_t)((warp & 3) * 32) << 16);
   const int64_t tiles = (a.n + kTile - 1) / kTile;
   Pipe p;
   bool ok = true;
   if (tid == 0 && (int64_t)blockIdx.x < tiles) start_load(c_jobs[0], nm, B, base, 0, p);
   for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
     const bool last_tile = t + gridDim.x >= tiles;
-    load_x(a.p, a.iquv, nullptr, t * kTile, a.n, a.nl, base + kSA, tid);
+    load_x(spar, a.iquv, nullptr, t * kTile, a.n, a.nl, base + kSA, row, half);
     fence_proxy_async();
     __syncthreads();
     for (int L = 0; L < 3 && ok; ++L) {
@@ -495,11 +586,11 @@ mlp_infer_kernel(const __grid_constant__ NetMaps nm, const InferArgs a) {
       if (!ok) break;
       tc_fence_after();
       if (L == 0) {
-        hidden_epilogue(trow, 0, a.p->b1, base + kSA, tid, nullptr);
+        hidden_epilogue(trow, 0, spar, base + kSA, row, half, nullptr);
       } else if (L == 1) {
-        hidden_epilogue(trow, 0, a.p->b2, base + kSA, tid, nullptr);
-      } else {
-        const int64_t b = t * kTile + tid;
+        hidden_epilogue(trow, 0, spar + 256, base + kSA, row, half, nullptr);
+      } else if (half == 0) {
+        const int64_t b = t * kTile + row;
         float o[16];
         tmem_ld16(trow, o);
         if (b < a.n) {
@@ -534,8 +625,11 @@ mlp_train_kernel(const __grid_constant__ NetMaps nm, const __grid_constant__ Act
   const uint32_t base = (saddr(smem_raw) + 1023u) & ~1023u;
   Bars* B = reinterpret_cast<Bars*>(smem_raw + (base - saddr(smem_raw)) + kSBar);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int row = tid & (kTile - 1), half = tid >> 7;   // accumulator row, column half
+  float* spar = reinterpret_cast<float*>(smem_raw + (base - saddr(smem_raw)) + kSPar);
+  stage_params(a.p, spar);
   setup(B, 512);
-  const uint32_t trow = B->tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t trow = B->tmem + ((uint32_t)((warp & 3) * 32) << 16);
   const uint32_t sA = base + kSA, sD = base + kSD;
   const int64_t tiles = a.n / kTile;
   Pipe p;
@@ -543,12 +637,12 @@ mlp_train_kernel(const __grid_constant__ NetMaps nm, const __grid_constant__ Act
   if (tid == 0 && (int64_t)blockIdx.x < tiles) start_load(c_jobs[0], nm, B, base, 0, p);
   for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
     const bool last_tile = t + gridDim.x >= tiles;
-    const int64_t b = t * kTile + tid;   // this thread's batch row
+    const int64_t b = t * kTile + row;   // this thread's batch row
     float* zrow = a.zspill + b * kHid;
     // the previous tile's stores must have read the operand tiles
     if (tid == 0) tma_store_wait_read();
     __syncthreads();
-    load_x(a.p, a.iquv, a.idx, t * kTile, a.n, a.nl, sA, tid);
+    load_x(spar, a.iquv, a.idx, t * kTile, a.n, a.nl, sA, row, half);
     fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
@@ -573,44 +667,47 @@ mlp_train_kernel(const __grid_constant__ NetMaps nm, const __grid_constant__ Act
       if (!ok) break;
       tc_fence_after();
       if (L == 0) {
-        hidden_epilogue(trow, 0, a.p->b1, sA, tid, zrow);
+        hidden_epilogue(trow, 0, spar, sA, row, half, zrow);
       } else if (L == 1) {
-        hidden_epilogue(trow, 256, a.p->b2, sA, tid, nullptr);
+        hidden_epilogue(trow, 256, spar + 256, sA, row, half, nullptr);
       } else if (L == 2) {
-        float o[16];
-        tmem_ld16(trow, o);
-        const float* yt = a.y16 + (int64_t)a.idx[b] * 16;
-        float sq = 0.f;
-        float g[kOut];
+        if (half == 0) {   // the 9 outputs: the first warpgroup
+          float o[16];
+          tmem_ld16(trow, o);
+          const float* yt = a.y16 + (int64_t)a.idx[b] * 16;
+          float sq = 0.f;
+          float g[kOut];
 #pragma unroll
-        for (int j = 0; j < kOut; ++j) {
-          const float d = o[j] + a.p->b3[j] - __ldg(yt + j);
-          sq += d * d;
-          g[j] = a.gscale * d;
+          for (int j = 0; j < kOut; ++j) {
+            const float d = o[j] + a.p->b3[j] - __ldg(yt + j);
+            sq += d * d;
+            g[j] = a.gscale * d;
+          }
+          uint32_t w[4] = {pack_bf16(g[0], g[1]), pack_bf16(g[2], g[3]), pack_bf16(g[4], g[5]),
+                           pack_bf16(g[6], g[7])};
+          st_chunk(sD, row, 0, w);
+          w[0] = pack_bf16(g[8], 0.f);
+          w[1] = w[2] = w[3] = 0u;
+          st_chunk(sD, row, 1, w);
+          w[0] = 0u;
+#pragma unroll
+          for (int j = 2; j < 8; ++j) st_chunk(sD, row, j, w);
+#pragma unroll
+          for (int o2 = 16; o2 > 0; o2 >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o2);
+          if (lane == 0) atomicAdd(a.loss, sq);
         }
-        uint32_t w[4] = {pack_bf16(g[0], g[1]), pack_bf16(g[2], g[3]), pack_bf16(g[4], g[5]),
-                         pack_bf16(g[6], g[7])};
-        st_chunk(sD, tid, 0, w);
-        w[0] = pack_bf16(g[8], 0.f);
-        w[1] = w[2] = w[3] = 0u;
-        st_chunk(sD, tid, 1, w);
-        w[0] = 0u;
-#pragma unroll
-        for (int j = 2; j < 8; ++j) st_chunk(sD, tid, j, w);
-#pragma unroll
-        for (int o2 = 16; o2 > 0; o2 >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o2);
-        if (lane == 0) atomicAdd(a.loss, sq);
       } else {
         // dZ = dH GELU'(Z): L 3 -> dZ2 (dH2 at column 0, Z2 at 256);
-        // L 4 -> dZ1 (dH1 at column 256, Z1 from the spill)
+        // L 4 -> dZ1 (dH1 at column 256, Z1 from the spill); this
+        // warpgroup's half of the columns
 #pragma unroll 1
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 4 * half; q < 4 * half + 4; ++q) {
           float dh[32], z[32];
           if (L == 3) {
             tmem_ld32(trow + 32 * q, dh);
             tmem_ld32(trow + 256 + 32 * q, z);   // the product, without its bias
 #pragma unroll
-            for (int e = 0; e < 32; ++e) z[e] += __ldg(a.p->b2 + 32 * q + e);
+            for (int e = 0; e < 32; ++e) z[e] += spar[256 + 32 * q + e];
           } else {
             tmem_ld32(trow + 256 + 32 * q, dh);
             const float4* src = reinterpret_cast<const float4*>(zrow + 32 * q);
@@ -631,7 +728,7 @@ mlp_train_kernel(const __grid_constant__ NetMaps nm, const __grid_constant__ Act
               const int e = 8 * u + 2 * h;
               w[h] = pack_bf16(dh[e] * gelu_grad(z[e]), dh[e + 1] * gelu_grad(z[e + 1]));
             }
-            st_chunk(sA + (q >> 1) * 16384u, tid, (q & 1) * 4 + u, w);
+            st_chunk(sA + (q >> 1) * 16384u, row, (q & 1) * 4 + u, w);
           }
         }
       }
@@ -676,7 +773,7 @@ constexpr uint32_t kWStageBytes = 16384 + 8192;   // A: 2 boxes (m 0..127), B: 1
 constexpr int kWBlocks = 14;
 constexpr size_t kWgradSmem = kWStages * kWStageBytes + 256 + 1024;
 
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kWThreads, 1)
 mlp_wgrad_kernel(const __grid_constant__ WgradMaps wm, const WgradArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const uint32_t base = (saddr(smem_raw) + 1023u) & ~1023u;
@@ -895,6 +992,46 @@ __global__ void mlp_targets_kernel(const double* __restrict__ truth, int64_t n, 
   }
 }
 
+// An epoch's visiting order: a pseudo-random permutation of [0, n) drawn on
+// the device, so that no host shuffle or copy sits between epochs.  A
+// 4-round Feistel network on 2 hb bits (2^(2 hb) >= n), its round function
+// the MurmurHash3 finaliser of (half ^ round key), restricted to [0, n) by
+// cycle walking (Black & Rogaway, "Ciphers with arbitrary finite domains",
+// 2002): re-applying the bijection until the value falls inside keeps the
+// map one to one and ends within the cycle of i, fewer than 4 n steps
+// (expected under 4).  hb = 0 writes the identity.
+__device__ __forceinline__ uint32_t fmix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x85ebca6bu;
+  x ^= x >> 13;
+  x *= 0xc2b2ae35u;
+  x ^= x >> 16;
+  return x;
+}
+
+__global__ void mlp_order_kernel(uint32_t* __restrict__ idx, uint32_t n, int hb, uint64_t key) {
+  const uint32_t mask = hb ? (1u << hb) - 1u : 0u;
+  const uint64_t cap = 4ull * n;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t x = i;
+    if (hb) {
+      uint64_t walk = 0;
+      do {
+        uint32_t l = x >> hb, r = x & mask;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const uint32_t f = fmix32(r ^ (uint32_t)(key >> (16 * k)) ^ (0x9e3779b9u * (uint32_t)(k + 1))) & mask;
+          const uint32_t t = l ^ f;
+          l = r;
+          r = t;
+        }
+        x = (l << hb) | r;
+      } while (x >= n && ++walk < cap);
+    }
+    idx[i] = x;
+  }
+}
+
 // ---------------------------------------------------------------- host
 namespace {
 
@@ -1060,6 +1197,8 @@ cudaError_t predict(const DevNet& d, const float* iquv, int64_t n, int nl, const
                     double* models, int* err, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   if (nl != d.nl || 4 * nl > kIn || !err) return cudaErrorInvalidValue;
+  // the input tiles are read in 16-byte vectors
+  if (reinterpret_cast<uintptr_t>(iquv) & 15u) return cudaErrorInvalidValue;
   NetMaps nm;
   nm.m[kMapW1] = d.mw1;
   nm.m[kMapW2] = d.mw2;
@@ -1095,8 +1234,11 @@ cudaError_t train(gm_mlp* net, const TrainArgs& a, float* loss_out, gm_mlp* grad
   const int64_t B = a.grads_only ? a.n : (int64_t)a.batch;
   if (B <= 0 || B % kTile || a.n < B || B > (int64_t)1 << 30)
     return fail("the batch must be a positive multiple of 128 and at most the pixel count", cudaErrorInvalidValue);
+  if (a.n > (int64_t)1 << 31) return fail("at most 2^31 training pixels", cudaErrorInvalidValue);
   if (a.nl < 1 || 4 * a.nl > kIn || net->nl != a.nl) return fail("the network's grid differs", cudaErrorInvalidValue);
   if (!err) return fail("no error word", cudaErrorInvalidValue);
+  if (reinterpret_cast<uintptr_t>(a.iquv) & 15u)
+    return fail("the profiles must start on a 16-byte boundary", cudaErrorInvalidValue);
   // the data may still be arriving on s
   cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return fail("data upload", e);
@@ -1158,15 +1300,18 @@ cudaError_t train(gm_mlp* net, const TrainArgs& a, float* loss_out, gm_mlp* grad
   const int epochs = a.grads_only ? 1 : std::max(1, a.epochs);
   const int64_t steps_per_epoch = n / B;
   const int64_t total = steps_per_epoch * epochs;
-  std::vector<uint32_t> order((size_t)n);
-  for (int64_t i = 0; i < n; ++i) order[(size_t)i] = (uint32_t)i;
+  // visiting order: the identity for a gradient check, else a fresh
+  // permutation per epoch keyed by the seed
+  int hb = 0;
+  if (!a.grads_only)
+    while ((uint64_t)1 << (2 * hb) < (uint64_t)n) ++hb;
   std::mt19937_64 rng(a.seed);
+  const int order_blocks = (int)std::min<int64_t>((n + 255) / 256, 4 * (int64_t)sm_count());
   int64_t step = 0;
   int64_t t_adam = net->steps;
   for (int ep = 0; ep < epochs && e == cudaSuccess; ++ep) {
-    if (!a.grads_only) std::shuffle(order.begin(), order.end(), rng);
-    e = cudaMemcpyAsync(idx, order.data(), sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(loss, 0, sizeof(float), s);
+    mlp_order_kernel<<<order_blocks, 256, 0, s>>>(idx, (uint32_t)n, hb, rng());
+    e = cudaMemsetAsync(loss, 0, sizeof(float), s);
     for (int64_t st = 0; st < steps_per_epoch && e == cudaSuccess; ++st, ++step) {
       TrainKArgs ka{};
       ka.p = d.p;
@@ -1190,7 +1335,7 @@ cudaError_t train(gm_mlp* net, const TrainArgs& a, float* loss_out, gm_mlp* grad
       wa.rows = B;
       wa.kslices = kslices;
       wa.err = err;
-      mlp_wgrad_kernel<<<kWBlocks * kslices, kThreads, kWgradSmem, s>>>(wm, wa);
+      mlp_wgrad_kernel<<<kWBlocks * kslices, kWThreads, kWgradSmem, s>>>(wm, wa);
       if (!a.grads_only) {
         ++t_adam;
         const double lr = a.lr * 0.5 * (1.0 + std::cos(M_PI * (double)step / (double)std::max<int64_t>(1, total)));

@@ -34,7 +34,7 @@ PIX_LEARNED_INIT = 0x40
 MLP_IN, MLP_HIDDEN, MLP_OUT, MLP_OUT_PAD = 128, 256, 9, 16
 NUMERICS_REFERENCE, NUMERICS_ACCURATE = 0, 1
 KERNEL_AUTO, KERNEL_FUSED = 0, 1
-SERVE_ROUND_ROBIN, SERVE_FIFO, SERVE_SHORTEST_FIRST = 0, 1, 2
+SERVE_ROUND_ROBIN, SERVE_FIFO, SERVE_SHORTEST_FIRST, SERVE_RESPONSE_RATIO = 0, 1, 2, 3
 
 # Symbols include/gmilos.h declares (checked by the tests against the .so).
 EXPORTS = ("gm_create", "gm_destroy", "gm_last_error", "gm_status_string", "gm_config_defaults",
@@ -464,7 +464,8 @@ class Engine:
                self._ctx)
 
     def serving_policy(self, policy):
-        """SERVE_ROUND_ROBIN, SERVE_FIFO or SERVE_SHORTEST_FIRST (gm_serving_policy)."""
+        """SERVE_ROUND_ROBIN, SERVE_FIFO, SERVE_SHORTEST_FIRST or SERVE_RESPONSE_RATIO
+        (gm_serving_policy)."""
         _check(lib().gm_serving_policy(self._ctx, int(policy)), self._ctx)
 
     def submit(self, iquv, model, chi2=None, iters=None, status=None, fix=None):

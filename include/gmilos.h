@@ -79,7 +79,7 @@ typedef enum {
 } gm_init_mode;
 
 /* Learned initial guess: a multilayer perceptron 4 nl -> 256 -> 256 -> 9
- * (GELU), nl <= 32 (120 inputs on the 30-sample grid), that maps a pixel's
+ * (GELU, tanh form), nl <= 32 (120 inputs on the 30-sample grid), that maps a pixel's
  * Stokes profiles to a start model.  Inputs are the profiles [4][nl] in the
  * cube's order, standardised per feature (x' = (x - in_mean) * in_scale,
  * zero past 4 nl).  The 9 outputs, standardised the same way (y = y' *
@@ -325,10 +325,10 @@ gm_status gm_invert_rois(gm_ctx *ctx, const gm_roi *rois, int nroi, const gm_bat
  * slots and device memory free up: at most max_active at a time, their
  * staging within the context's HBM budget.  Admitted requests are cut into
  * chunks of chunk_pixels; `streams` lanes each keep one chunk on the device,
- * taken round robin from the admitted requests, so requests that arrive
- * while others run start within one chunk time and their work overlaps on
- * the device.  Each lane keeps one chunk of wave-kernel state and classical
- * start models on the device (about 270 MB per lane at the default chunk and
+ * taken from the admitted requests by the serving policy (below), so the
+ * work of requests that arrive while others run overlaps on the device.
+ * Each lane keeps one chunk of wave-kernel state and classical start models
+ * on the device (about 270 MB per lane at the default chunk and
  * nl <= 32), so a served pixel runs the kernels of gm_invert and its result
  * is the one gm_invert gives, whatever the mix.  Requests share
  * the configured stray-light profile and wavelength grid: a configuration
@@ -353,15 +353,20 @@ typedef struct {
  * (default 65536), admitted requests at a time (default 16) */
 gm_status gm_serving_options(gm_ctx *ctx, int streams, int64_t chunk_pixels, int max_active);
 /* Which admitted request a free lane serves next (any time):
- * GM_SERVE_ROUND_ROBIN (default) -- the admitted requests in turn, so each
+ * GM_SERVE_ROUND_ROBIN -- the admitted requests in turn, so each
  *   progresses at the same rate and a request's latency grows with its size;
  * GM_SERVE_FIFO -- the earliest submitted first, so requests finish in
  *   arrival order and under load every request waits about as long;
  * GM_SERVE_SHORTEST_FIRST -- the fewest pixels left first (the lowest mean
- *   latency; large requests wait behind small ones). */
+ *   latency; large requests wait behind small ones);
+ * GM_SERVE_RESPONSE_RATIO (default) -- the highest ratio of time since
+ *   submission to the request's pixels first (highest response ratio next):
+ *   small requests go first as with shortest-first, but a request's
+ *   priority grows while it waits, so large requests are not starved. */
 #define GM_SERVE_ROUND_ROBIN 0
 #define GM_SERVE_FIFO 1
 #define GM_SERVE_SHORTEST_FIRST 2
+#define GM_SERVE_RESPONSE_RATIO 3
 gm_status gm_serving_policy(gm_ctx *ctx, int policy);
 gm_status gm_submit(gm_ctx *ctx, const gm_request *req, gm_ticket *ticket);
 /* wait for a request (timeout_us < 0: no limit); consumes the ticket */
@@ -433,7 +438,11 @@ void gm_mlp_train_defaults(gm_mlp_train_opts *o);
  * FP32 parameters).  An untrained net (steps == 0) first takes its
  * standardisation from the data.  loss_per_epoch (optional, [epochs]): mean
  * squared error of the standardised outputs over each epoch.  n must be at
- * least one batch. */
+ * least one batch.  Profiles in device memory must start on a 16-byte
+ * boundary (the kernels read them in 16-byte vectors), as must the cube of
+ * an inversion that starts from the learned guess (GM_INIT_LEARNED);
+ * otherwise the call fails before the network runs (GM_ERR_INVALID here and
+ * in gm_mlp_predict, GM_ERR_CUDA "invalid argument" from an inversion). */
 gm_status gm_mlp_train(gm_ctx *ctx, gm_mlp *net, const float *iquv, const double *truth,
                        int64_t n, const gm_mlp_train_opts *opts, float *loss_per_epoch);
 

@@ -34,16 +34,29 @@ def bf16(x):
     return out
 
 
-def _erf(x):
-    return np.vectorize(math.erf, otypes=[np.float64])(x)
+SQRT_2_OVER_PI = math.sqrt(2.0 / math.pi)
+
+
+def _sigmoid_2u(z):
+    """s = (1 + tanh u) / 2 = 1 / (1 + exp(-2u)), u = sqrt(2/pi) (z + 0.044715 z^3),
+    and d(2u)/dz."""
+    z = np.asarray(z, dtype=np.float64)
+    u2 = 2.0 * SQRT_2_OVER_PI * z * (1.0 + 0.044715 * z * z)
+    du2 = 2.0 * SQRT_2_OVER_PI * (1.0 + 3 * 0.044715 * z * z)
+    with np.errstate(over="ignore"):
+        s = 1.0 / (1.0 + np.exp(-u2))
+    return s, du2
 
 
 def gelu(z):
-    return 0.5 * z * (1.0 + _erf(z / math.sqrt(2.0)))
+    """GELU in its tanh form (Hendrycks & Gimpel, 2016)."""
+    s, _ = _sigmoid_2u(z)
+    return np.asarray(z, dtype=np.float64) * s
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + _erf(z / math.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / math.sqrt(2.0 * math.pi)
+    s, du2 = _sigmoid_2u(z)
+    return s + np.asarray(z, dtype=np.float64) * s * (1.0 - s) * du2
 
 
 def targets(models):

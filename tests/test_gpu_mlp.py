@@ -132,3 +132,24 @@ def test_learned_mode_needs_a_network_for_its_grid(engine):
     _, g20 = config(nl=20, init_mode=G.INIT_LEARNED, mlp=G.mlp_new(30))
     with pytest.raises(G.GmError):
         engine.configure(g20)
+
+
+def test_misaligned_device_profiles_rejected(engine):
+    """The kernels read profiles in 16-byte vectors: a device array that
+    starts 4 bytes past a boundary is refused on the host, before any
+    launch, and the context stays usable."""
+    import torch
+    ocfg, gcfg = config(30)
+    net = H.random_net(3, 30)
+    _, obs = observations(ocfg, 256, 9)
+    engine.configure(gcfg)
+    flat = torch.zeros(obs.size + 1, dtype=torch.float32, device="cuda")
+    flat[1:] = torch.from_numpy(np.ascontiguousarray(obs, dtype=np.float32).ravel()).cuda()
+    bad = flat[1:].view(obs.shape)
+    assert bad.data_ptr() % 16 == 4
+    with pytest.raises(G.GmError, match="16-byte"):
+        engine.mlp_predict(net, bad)
+    good = torch.from_numpy(np.ascontiguousarray(obs, dtype=np.float32)).cuda()
+    got = engine.mlp_predict(net, good).cpu().numpy()
+    want = engine.mlp_predict(net, obs)
+    assert np.array_equal(got, want)

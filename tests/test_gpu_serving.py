@@ -152,12 +152,12 @@ def test_concurrent_submitters():
         np.testing.assert_array_equal(results[k], alone(data[k], FIX9A)["model"])
 
 
-@pytest.mark.parametrize("policy", [G.SERVE_FIFO, G.SERVE_SHORTEST_FIRST])
+@pytest.mark.parametrize("policy", [G.SERVE_FIFO, G.SERVE_SHORTEST_FIRST, G.SERVE_RESPONSE_RATIO])
 def test_every_policy_gives_the_lone_results(policy):
     """The serving policies decide only which request's chunk a free lane
     takes next: results stay those of each request inverted alone, and the
-    shortest-first policy finishes a small request submitted after a large
-    one first."""
+    shortest-first and response-ratio policies finish a small request
+    submitted after a large one first."""
     sizes = [60000, 500, 3000]
     data = [cube(n, 200 + k) for k, n in enumerate(sizes)]
     _, gcfg, _ = config()
@@ -177,5 +177,5 @@ def test_every_policy_gives_the_lone_results(policy):
         ref = alone(d, FIX9A)
         np.testing.assert_array_equal(model, ref["model"])
         np.testing.assert_array_equal(chi2, ref["chi2"])
-    if policy == G.SERVE_SHORTEST_FIRST:
+    if policy in (G.SERVE_SHORTEST_FIRST, G.SERVE_RESPONSE_RATIO):
         assert lat[1] < lat[0]

@@ -88,3 +88,26 @@ def test_mlp_init_on_the_host():
     np.testing.assert_array_equal(a["w2"], same["w2"])
     with pytest.raises(G.GmError):
         G.mlp_new(33)
+
+
+def test_fp64_gradients_match_torch_autograd():
+    """The restatement's backward pass (without the BF16 roundings) against
+    torch's automatic differentiation of the same network in FP64."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(9)
+    p = M.params(random_net(9))
+    X = rng.normal(0, 1, (64, M.IN))
+    X[:, 120:] = 0.0
+    Y = rng.normal(0, 1, (64, M.OUT))
+    loss, g = M.loss_and_grads(p, X, Y, quantize=False)
+    t = {k: torch.tensor(p[k], dtype=torch.float64, requires_grad=True) for k in ("w1", "b1", "w2", "b2", "w3")}
+    t["b3"] = torch.tensor(p["b3"][:M.OUT], dtype=torch.float64, requires_grad=True)
+    gelu = lambda z: 0.5 * z * (1 + torch.tanh(np.sqrt(2.0 / np.pi) * (z + 0.044715 * z ** 3)))
+    h1 = gelu(torch.tensor(X) @ t["w1"].T + t["b1"])
+    h2 = gelu(h1 @ t["w2"].T + t["b2"])
+    out = h2 @ t["w3"].T + t["b3"]
+    lt = ((out - torch.tensor(Y)) ** 2).mean()
+    lt.backward()
+    assert lt.item() == pytest.approx(loss, rel=1e-12)
+    for k in t:
+        np.testing.assert_allclose(g[k], t[k].grad.numpy(), rtol=1e-9, atol=1e-12, err_msg=k)
