@@ -177,7 +177,10 @@ struct WarpSmem {
   double m[11];          // current (last accepted) model: the reference's initModel
   double t[11];          // trial model, persistent like the reference's `model`
   static constexpr int NS = Variant<V>::SOLVES;
-  float A[NS][2][10][11];   // Jacobi working matrix (upper triangle) per damping, double-buffered
+  // Jacobi working matrix per damping, double-buffered, in 2x2 blocks of
+  // the upper triangle (solve10's layout: damping h, buffer b at
+  // h * kSolveH + b * kSolveB)
+  alignas(16) float A[NS == 2 ? 272 : 200];
   float alpha[68];       // undamped normal matrix, packed upper triangle (55 or 66)
   float beta[12];
   float vec[NS][2][12];  // rotated beta per damping, double-buffered; a step lands in vec[d][0]
@@ -957,12 +960,35 @@ __device__ __forceinline__ float chisq(const DevCfg& c, const float (&syn)[LPL][
 // otherwise the group is the warp.  The step loops stay rolled: the kernel
 // is bound by instruction fetch, and a rolled loop keeps the solve's code
 // small.
+//
+// Layout: block (p, q) occupies four consecutive floats (entries (2p, 2q),
+// (2p, 2q + 1), (2p + 1, 2q), (2p + 1, 2q + 1); a diagonal block leaves its
+// lower entry unused) at 4 solve_slot(block), so a lane reads its block
+// with one 16-byte load; entry (i, j), i <= j, lives at solve_addr(i, j).
+// The slot order and the dampings' offset kSolveH were chosen by a search
+// over slot orders on the host, counting the bank conflicts of the step's
+// accesses: they take 13 shared-memory wavefronts (4 for the block loads, 9
+// for the four scattered stores) instead of 21 with row-major 10 x 11
+// matrices.
+constexpr int kSolveH = 68, kSolveB = 2 * kSolveH;   // damping and buffer strides (floats)
+__host__ __device__ constexpr int solve_block(int p, int q) {   // p <= q: index in the lanes' order
+  return p == q ? p : (p == 0 ? 4 + q : (p == 1 ? 7 + q : (p == 2 ? 9 + q : 14)));
+}
+__host__ __device__ constexpr int solve_slot(int b) {
+  constexpr int slot[15] = {10, 15, 5, 11, 12, 8, 6, 1, 3, 9, 4, 14, 7, 0, 13};
+  return slot[b];
+}
+__host__ __device__ constexpr int solve_addr(int i, int j) {
+  return i > j ? solve_addr(j, i) : 4 * solve_slot(solve_block(i / 2, j / 2)) + 2 * (i & 1) + (j & 1);
+}
+
 struct SolvePlan {
   int src;                      // offset of this lane's block in the working matrix
   int d00, d01, d10, d11;       // offsets its four entries move to
   int p, q;                     // block row / column (rotation pair), as group lanes
   int vin, vout0, vout1;        // beta pair read / relabelled write positions
   int base;                     // first lane of this lane's group
+  int wdiag;                    // offset of diagonal entry g (lanes g < 10)
   // packed-triangle entries g + e * (32 / NS) (e < 2 NS, g the group lane)
   // this lane copies in: byte e holds the working-matrix offset, bit 7
   // marking a diagonal entry, 0xff none
@@ -981,11 +1007,9 @@ __device__ __forceinline__ SolvePlan make_solve_plan(int lane) {
   s.p = g < 15 ? bp[g] : 0;
   s.q = g < 15 ? bq[g] : 0;
   const int r0 = 2 * s.p, c0 = 2 * s.q;
-  s.src = r0 * 11 + c0;
-  auto dst = [&](int r, int c) {
-    const int a = pr[r], b = pr[c];
-    return (a < b ? a : b) * 11 + (a < b ? b : a);
-  };
+  s.src = 4 * solve_slot(solve_block(s.p, s.q));
+  s.wdiag = g < 10 ? solve_addr(g, g) : 0;
+  auto dst = [&](int r, int c) { return solve_addr(pr[r], pr[c]); };
   s.d00 = dst(r0, c0);
   s.d01 = dst(r0, c0 + 1);
   s.d10 = dst(r0 + 1, c0);
@@ -1000,7 +1024,7 @@ __device__ __forceinline__ SolvePlan make_solve_plan(int lane) {
     for (int c = r; c < 10; ++c, ++i) {
       if (i >= g && (i - g) % G == 0 && (i - g) / G < 2 * NS) {
         const int e = (i - g) / G;
-        const unsigned b = (unsigned)(r * 11 + c) | (r == c ? 0x80u : 0u);
+        const unsigned b = (unsigned)solve_addr(r, c) | (r == c ? 0x80u : 0u);
         s.initpack = (s.initpack & ~(0xffu << (8 * e))) | (b << (8 * e));
       }
     }
@@ -1023,15 +1047,16 @@ __device__ __noinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, 
   // memory, and unpacked the eleven values spill (+3.6 % pixels/s packed).
   const unsigned w0 = (unsigned)pl.src | (unsigned)pl.d00 << 8 | (unsigned)pl.d01 << 16 | (unsigned)pl.d10 << 24;
   const unsigned w1 = (unsigned)pl.d11 | (unsigned)pl.vin << 8 | (unsigned)pl.vout0 << 16 | (unsigned)pl.vout1 << 24;
-  const unsigned w2 = (unsigned)pl.p | (unsigned)(pl.base + pl.p) << 8 | (unsigned)(pl.base + pl.q) << 16;
+  const unsigned w2 = (unsigned)pl.p | (unsigned)(pl.base + pl.p) << 8 | (unsigned)(pl.base + pl.q) << 16 |
+                     (unsigned)pl.wdiag << 24;
   const unsigned initpack = pl.initpack;
   auto at = [](unsigned w, int i) { return (int)((w >> (8 * i)) & 0xffu); };
   const int h = NS == 2 ? lane >> 4 : 0;
   const int g = lane & (G - 1);
   // damped matrix (diagonal x (1 + lambda), milosUtils.cu:648-652)
   const double damp = 1.0 + (double)(h ? flambda2 : flambda);
-  float* A = &sm.A[h][0][0][0];
-  float* B = &sm.A[h][1][0][0];
+  float* A = &sm.A[h * kSolveH];
+  float* B = A + kSolveB;
 #pragma unroll
   for (int e = 0; e < 2 * NS; ++e) {
     const unsigned b = (initpack >> (8 * e)) & 0xffu;
@@ -1050,8 +1075,9 @@ __device__ __noinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, 
   const bool diag = g < 5, active = g < 15;
 #pragma unroll 1
   for (int step = 0; step < 18; ++step) {
-    const float m00 = A[at(w0, 0)], m01 = A[at(w0, 0) + 1], m11 = A[at(w0, 0) + 12];
-    const float m10 = diag ? m01 : A[at(w0, 0) + 11];
+    const float4 blk = *reinterpret_cast<const float4*>(A + at(w0, 0));
+    const float m00 = blk.x, m01 = blk.y, m11 = blk.w;
+    const float m10 = diag ? m01 : blk.z;
     const float b0 = va[at(w1, 1)], b1 = va[at(w1, 1) + 1];
     float th;
     if (m00 == m11) {
@@ -1077,7 +1103,7 @@ __device__ __noinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, 
     if (active) {
       B[at(w0, 1)] = n00;
       B[at(w0, 2)] = n01;
-      B[at(w0, 3)] = n10;
+      if (!diag) B[at(w0, 3)] = n10;   // a diagonal block's two off-diagonal entries are one
       B[at(w1, 0)] = n11;
     }
     if (diag) {
@@ -1091,7 +1117,7 @@ __device__ __noinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, 
   // 18 steps: the final matrix and vector are back in the first buffers, in
   // the original index order.  z = (V^T beta) / w with the |w| <= 1e-12 cut.
   if (g < 10) {
-    const float w = A[g * 12];
+    const float w = A[at(w2, 3)];
     const float inv = ((double)fabsf(w) > 1e-12) ? (1.f / w) : 0.f;
     va[g] = va[g] * inv;
   }
