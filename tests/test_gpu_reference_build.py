@@ -118,7 +118,8 @@ def test_inversions_match_reference_gpu_build(engine):
     assert rec_g >= rec_r - 0.01
 
 
-@pytest.mark.skipif(not ref.available(gpu=True), reason="libgmref_gpu.so not built")
+@pytest.mark.skipif(not (ref.available(gpu=True) and ref.available()),
+                    reason="libgmref_gpu.so / libgmref_cpu.so not built")
 @pytest.mark.parametrize("psf,stray", [(False, False), (True, True)])
 def test_one_iteration_reference_numerics_vs_reference_gpu_build(engine, psf, stray):
     """One LM iteration (miter = 1, classical-estimate start) in REFERENCE
@@ -133,7 +134,11 @@ def test_one_iteration_reference_numerics_vs_reference_gpu_build(engine, psf, st
     differences (measured: model p99 5e-5 to 1e-4, chi2 p99 1.4e-4 to
     1.9e-4, 99.4-99.7 % of pixels within 1e-3, the largest difference 5 % of
     a parameter -- a step-size difference, far below a whole step, so no
-    accept/reject decision differs)."""
+    accept/reject decision differs).  The same step by the reference's own
+    host build (libm trigonometry) lands within 1e-3 of its sm_100a build
+    on only 0.4-2.9 % of the pixels (p99 0.13-0.27): the engine must
+    reproduce the sm_100a build's step better than that build's own host
+    compilation does."""
     fix = FIX if stray else H.FREE9
     ocfg, s, gcfg, sl = setups(psf, stray, miter=1, numerics=G.NUMERICS_REFERENCE, fix=fix)
     t, obs = cube(ocfg, sl, 4096, 24)
@@ -150,8 +155,18 @@ def test_one_iteration_reference_numerics_vs_reference_gpu_build(engine, psf, st
           "p50 %.2e p99 %.2e max %.2e, chi2 rel p99 %.2e"
           % (same, np.percentile(rel[:, :9], 50), np.percentile(rel[:, :9], 99), rel[:, :9].max(),
              np.percentile(crel, 99)))
+    # the reference's own host build against its sm_100a build, same step
+    mh, ch, ih, _ = ref.invert_cpu(s, obs, slight=sl)
+    relh = np.abs(mh - mr) / np.maximum(np.abs(mr), 1e-3)
+    crelh = np.abs(ch - cr) / cr
+    sameh = (relh[:, :9].max(axis=1) < 1e-3).mean()
+    print("one iteration, reference host build vs its sm_100a build: same decision %.4f, model rel "
+          "p50 %.2e p99 %.2e max %.2e, chi2 rel p99 %.2e"
+          % (sameh, np.percentile(relh[:, :9], 50), np.percentile(relh[:, :9], 99), relh[:, :9].max(),
+             np.percentile(crelh, 99)))
     assert (out["iters"] == ir).all()
-    assert same >= 0.99
+    assert same >= 0.99 and same > sameh
+    assert np.percentile(rel[:, :9], 99) < np.percentile(relh[:, :9], 99)
     assert rel[:, :9].max() < 0.2
     assert np.percentile(rel[:, :9], 99) < 2e-4
     assert np.percentile(crel, 99) < 5e-4
