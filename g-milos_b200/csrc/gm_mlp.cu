@@ -12,7 +12,9 @@
 // of the next weight block overlaps the current product and epilogue.
 // Activations are written into the operand tile by the epilogue threads
 // themselves (the swizzle computed in place), so a tile's three layers run
-// back to back without leaving the SM.
+// back to back without leaving the SM.  Inference keeps two tiles in
+// flight per CTA, a producer warp issuing one tile's products while eight
+// epilogue warps work on the other's accumulator.
 //
 // Training runs per batch: (1) one fused kernel per 128-pixel tile for the
 // forward pass, the loss, and the backward pass through the activations
@@ -40,10 +42,11 @@ namespace gm {
 namespace mlp {
 namespace {
 
-// Inference and training kernels: 8 warps, two per tensor-memory lane
-// quarter -- warp w reads rows 32 (w % 4) .. + 31 of the accumulator, and
-// the two warpgroups split each epilogue's columns (and the input features)
-// in halves.  The weight-gradient kernel: 4 warps, one row each.
+// Inference and training kernels: 8 epilogue warps, two per tensor-memory
+// lane quarter -- warp w reads rows 32 (w % 4) .. + 31 of the accumulator,
+// and the two warpgroups split each epilogue's columns (and the input
+// features) in halves; inference adds a producer warp.  The weight-gradient
+// kernel: 4 warps, one row each.
 constexpr int kThreads = 256;
 constexpr int kWThreads = 128;
 constexpr uint64_t kWaitNs = 2000000000ull;   // a wait gives up after 2 s
@@ -163,7 +166,6 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(bar))
                : "memory");
 }
-// 32 consecutive columns of this thread's tensor-memory lane
 // 32 columns of this warp's 32 lanes: the load is asynchronous; its
 // registers are valid after tmem_wait32 on the same array, whose asm takes
 // them as operands so that no read of them is placed before the wait.
@@ -549,67 +551,240 @@ __device__ __forceinline__ void teardown(Bars* B, Pipe& p, uint32_t ncols, int* 
 }  // namespace
 
 // ---------------------------------------------------------------- inference
-// Persistent: each CTA takes tiles blockIdx.x, blockIdx.x + gridDim.x, ...
-// Per tile: inputs -> layer 1 -> GELU -> layer 2 -> GELU -> layer 3 ->
-// start models.
-__global__ void __launch_bounds__(kThreads, 1)
+// Persistent and warp-specialised, two 128-pixel tiles in flight per CTA
+// (slots 0 and 1: each its own activation tile in shared memory and 256
+// tensor-memory columns).  Warps 0-7 are epilogue warps: they load a
+// slot's inputs, and after each of its products turn the accumulator into
+// the next operand (GELU) or the start models; warp 8's first thread
+// streams the weights through two 32 KB stages by TMA and issues the
+// products.  While the epilogue warps work on one slot, the tensor core
+// works on the other: per pair of tiles (A in slot 0, B in slot 1) the
+// products run L0(A) L0(B) L1(A) L1(B) L2(A) L2(B) and the epilogues
+// E0(A) E0(B) E1(A) E1(B) OUT(A) X(A') OUT(B) X(B'), each product waiting
+// for the epilogue that wrote its operand (hready, all 256 epilogue
+// threads arrive) and each epilogue for its product (zready, a commit).
+constexpr int kIThreads = 288;                 // 8 epilogue warps + the producer warp
+constexpr uint32_t kIAct = 65536;              // one slot's activation tile (4 K-atoms)
+constexpr uint32_t kIW = 2 * kIAct;            // weight stages
+constexpr uint32_t kIStage = 32768;            // one K-atom of a 256-row weight
+constexpr uint32_t kIBar = kIW + 2 * kIStage;
+constexpr uint32_t kIPar = kIBar + 128;
+constexpr size_t kISmemBytes = kIPar + 4 * kParFloats + 1024;
+
+struct IBars {
+  uint64_t full[2], empty[2];   // weight stages: loaded / free again
+  uint64_t zready[2];           // slot's accumulator written (product committed)
+  uint64_t hready[2];           // slot's operand tile written (256 epilogue threads)
+  uint64_t fin;
+  uint32_t tmem;
+  int abort;
+};
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(b)) : "memory");
+}
+
+// Producer state (warp 8, lane 0)
+struct Prod {
+  uint32_t fph[2] = {0, 0}, eph[2] = {0, 0}, hph[2] = {0, 0};
+  bool pend[2] = {false, false}, inflight[2] = {false, false};
+};
+
+// Load `natoms` K-atoms (from atom k0) of a weight into stage st, once the
+// products that last read the stage are done.
+__device__ __forceinline__ bool p_load(Prod& P, IBars* B, uint32_t wbase, int st, const CUtensorMap* map, int k0,
+                                       int natoms, uint32_t atom_bytes, int* err) {
+  if (P.pend[st]) {
+    if (!mbar_wait(&B->empty[st], P.eph[st], &B->abort, err, kErrWaitStage)) return false;
+    P.eph[st] ^= 1u;
+    P.pend[st] = false;
+  }
+  mbar_expect_tx(&B->full[st], atom_bytes * natoms);
+  for (int a = 0; a < natoms; ++a) tma_load_2d(wbase + st * kIStage + a * atom_bytes, map, 64 * (k0 + a), 0, &B->full[st]);
+  P.inflight[st] = true;
+  return true;
+}
+__device__ __forceinline__ bool p_wait(Prod& P, IBars* B, int st, int* err) {
+  if (!mbar_wait(&B->full[st], P.fph[st], &B->abort, err, kErrWaitLoad)) return false;
+  P.fph[st] ^= 1u;
+  P.inflight[st] = false;
+  tc_fence_after();
+  return true;
+}
+__device__ __forceinline__ void p_release(Prod& P, IBars* B, int st) {
+  mma_commit(&B->empty[st]);
+  P.pend[st] = true;
+}
+__device__ __forceinline__ bool p_wait_operand(Prod& P, IBars* B, int slot, int* err) {
+  if (!mbar_wait(&B->hready[slot], P.hph[slot], &B->abort, err, kErrWaitMma)) return false;
+  P.hph[slot] ^= 1u;
+  tc_fence_after();
+  return true;
+}
+// The products of `natoms` K-atoms: A from the slot's tile (atoms a0..),
+// B from a stage (atoms b_atom_bytes apart), N = rows, into tensor column
+// tcol; the first accumulates onto what is there when acc.
+__device__ __forceinline__ void mma_atoms(uint32_t tcol, uint32_t sa, int a0, uint32_t sb, uint32_t b_atom_bytes,
+                                          int natoms, int rows, bool acc) {
+  const uint32_t idesc = idesc_bf16(128, rows, 0, 0);
+  for (int a = 0; a < natoms; ++a)
+    for (int kk = 0; kk < 4; ++kk) {
+      const uint64_t ad = sw128_desc(sa + (a0 + a) * 16384u + kk * 32u, 16, 1024);
+      const uint64_t bd = sw128_desc(sb + a * b_atom_bytes + kk * 32u, 16, 1024);
+      mma_bf16(tcol, ad, bd, idesc, (acc || a > 0 || kk > 0) ? 1u : 0u);
+    }
+}
+
+// Epilogue thread: this thread's shared-memory writes and tensor-memory
+// reads of the slot are done; the producer may go on with it.
+__device__ __forceinline__ void epi_arrive(uint64_t* bar) {
+  fence_proxy_async();
+  tc_fence_before();
+  mbar_arrive(bar);
+}
+
+__global__ void __launch_bounds__(kIThreads, 1)
 mlp_infer_kernel(const __grid_constant__ NetMaps nm, const InferArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   const uint32_t base = (saddr(smem_raw) + 1023u) & ~1023u;
-  Bars* B = reinterpret_cast<Bars*>(smem_raw + (base - saddr(smem_raw)) + kSBar);
+  unsigned char* gbase = smem_raw + (base - saddr(smem_raw));
+  IBars* B = reinterpret_cast<IBars*>(gbase + kIBar);
+  float* spar = reinterpret_cast<float*>(gbase + kIPar);
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int row = tid & (kTile - 1), half = tid >> 7;   // accumulator row, column half
-  float* spar = reinterpret_cast<float*>(smem_raw + (base - saddr(smem_raw)) + kSPar);
-  stage_params(a.p, spar);
-  setup(B, 256);
-  const uint32_t trow = B->tmem + ((uint32_t)((warp & 3) * 32) << 16);
   const int64_t tiles = (a.n + kTile - 1) / kTile;
-  Pipe p;
-  bool ok = true;
-  if (tid == 0 && (int64_t)blockIdx.x < tiles) start_load(c_jobs[0], nm, B, base, 0, p);
-  for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-    const bool last_tile = t + gridDim.x >= tiles;
-    load_x(spar, a.iquv, nullptr, t * kTile, a.n, a.nl, base + kSA, row, half);
-    fence_proxy_async();
-    __syncthreads();
-    for (int L = 0; L < 3 && ok; ++L) {
-      if (tid == 0) {
-        for (int j = layer_first(L, false); j < layer_last(L, false) && ok; ++j) {
-          const Job* nx = (j + 1 < kInferJobs) ? &c_jobs[j + 1] : (last_tile ? nullptr : &c_jobs[0]);
-          ok = run_job(c_jobs[j], nx, false, nm, B, base, p, a.err);
+  const int64_t G = gridDim.x;
+  stage_params(a.p, spar);
+  if (tid == 0) {
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&B->full[i], 1);
+      mbar_init(&B->empty[i], 1);
+      mbar_init(&B->zready[i], 1);
+      mbar_init(&B->hready[i], 256);
+    }
+    mbar_init(&B->fin, 1);
+    B->abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) tmem_alloc(&B->tmem, 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t wbase = base + kIW;
+  if (warp == 8) {
+    // ---- producer: weights and products
+    Prod P;
+    bool ok = true;
+    if ((tid & 31) == 0) {
+      const CUtensorMap* w1 = &nm.m[kMapW1];
+      const CUtensorMap* w2 = &nm.m[kMapW2];
+      const CUtensorMap* w3 = &nm.m[kMapW3];
+      for (int64_t tA = blockIdx.x; tA < tiles && ok; tA += 2 * G) {
+        const bool hasB = tA + G < tiles;
+        const int nslot = hasB ? 2 : 1;
+        // L0: both K-atoms of W1 resident, the products of both slots
+        ok = p_load(P, B, wbase, 0, w1, 0, 1, kIStage, a.err) && p_load(P, B, wbase, 1, w1, 1, 1, kIStage, a.err);
+        ok = ok && p_wait(P, B, 0, a.err) && p_wait(P, B, 1, a.err);
+        for (int sl = 0; sl < nslot && ok; ++sl) {
+          ok = p_wait_operand(P, B, sl, a.err);
+          if (!ok) break;
+          const uint32_t tcol = B->tmem + 256u * sl, sa = base + sl * kIAct;
+          mma_atoms(tcol, sa, 0, wbase, 0, 1, 256, false);
+          mma_atoms(tcol, sa, 1, wbase + kIStage, 0, 1, 256, true);
+          mma_commit(&B->zready[sl]);
+        }
+        if (!ok) break;
+        p_release(P, B, 0);
+        p_release(P, B, 1);
+        // L1: the four K-atoms of W2 streamed through the stages, per slot
+        for (int sl = 0; sl < nslot && ok; ++sl) {
+          const uint32_t tcol = B->tmem + 256u * sl, sa = base + sl * kIAct;
+          ok = p_load(P, B, wbase, 0, w2, 0, 1, kIStage, a.err) && p_load(P, B, wbase, 1, w2, 1, 1, kIStage, a.err);
+          ok = ok && p_wait_operand(P, B, sl, a.err);
+          for (int h = 0; h < 2 && ok; ++h) {
+            if (h == 1)
+              ok = p_load(P, B, wbase, 0, w2, 2, 1, kIStage, a.err) && p_load(P, B, wbase, 1, w2, 3, 1, kIStage, a.err);
+            for (int st = 0; st < 2 && ok; ++st) {
+              ok = p_wait(P, B, st, a.err);
+              if (!ok) break;
+              mma_atoms(tcol, sa, 2 * h + st, wbase + st * kIStage, 0, 1, 256, h + st > 0);
+              p_release(P, B, st);
+            }
+          }
+          if (ok) mma_commit(&B->zready[sl]);
+        }
+        if (!ok) break;
+        // L2: W3 (16 rows, 4 K-atoms of 2 KB) in stage 0 for both slots
+        ok = p_load(P, B, wbase, 0, w3, 0, 4, 16u * 128u, a.err) && p_wait(P, B, 0, a.err);
+        for (int sl = 0; sl < nslot && ok; ++sl) {
+          ok = p_wait_operand(P, B, sl, a.err);
+          if (!ok) break;
+          mma_atoms(B->tmem + 256u * sl, base + sl * kIAct, 0, wbase, 16u * 128u, 4, 16, false);
+          mma_commit(&B->zready[sl]);
+        }
+        if (ok) p_release(P, B, 0);
+      }
+      if (!ok) atomicCAS(a.err, kErrNone, kErrWaitMma);
+      // end: loads still in flight (only after an abort), then every product
+      for (int st = 0; st < 2; ++st)
+        if (P.inflight[st]) mbar_wait(&B->full[st], P.fph[st], &B->abort, a.err, kErrWaitLoad, false);
+      mma_commit(&B->fin);
+      mbar_wait(&B->fin, 0, &B->abort, a.err, kErrWaitMma, false);
+    }
+  } else {
+    // ---- epilogue warps
+    const int row = tid & (kTile - 1), half = tid >> 7;   // accumulator row, column half
+    const uint32_t qoff = (uint32_t)((warp & 3) * 32) << 16;
+    uint32_t zph[2] = {0, 0};
+    bool ok = true;
+    auto zwait = [&](int sl) {
+      ok = ok && mbar_wait(&B->zready[sl], zph[sl], &B->abort, a.err, kErrWaitMma);
+      zph[sl] ^= 1u;
+      tc_fence_after();
+      return ok;
+    };
+    for (int sl = 0; sl < 2; ++sl) {
+      const int64_t t = blockIdx.x + sl * G;
+      if (t < tiles) {
+        load_x(spar, a.iquv, nullptr, t * kTile, a.n, a.nl, base + sl * kIAct, row, half);
+        epi_arrive(&B->hready[sl]);
+      }
+    }
+    for (int64_t tA = blockIdx.x; tA < tiles && ok; tA += 2 * G) {
+      const int nslot = tA + G < tiles ? 2 : 1;
+      for (int L = 0; L < 2 && ok; ++L)
+        for (int sl = 0; sl < nslot; ++sl) {
+          if (!zwait(sl)) break;
+          hidden_epilogue(B->tmem + 256u * sl + qoff, 0, spar + 256 * L, base + sl * kIAct, row, half, nullptr);
+          epi_arrive(&B->hready[sl]);
+        }
+      for (int sl = 0; sl < nslot && ok; ++sl) {
+        if (!zwait(sl)) break;
+        const int64_t t = tA + sl * G;
+        if (half == 0) {
+          const int64_t b = t * kTile + row;
+          float o[16];
+          tmem_ld16(B->tmem + 256u * sl + qoff, o);
+          if (b < a.n) {
+            float y[kOut];
+#pragma unroll
+            for (int j = 0; j < kOut; ++j) y[j] = (o[j] + a.p->b3[j]) * a.p->out_scale[j] + a.p->out_mean[j];
+            double m[11];
+            outputs_to_model(y, a.guess, a.fix, m);
+#pragma unroll
+            for (int i = 0; i < 11; ++i) a.models[b * 11 + i] = m[i];
+          }
+        }
+        // this slot's next tile
+        if (t + 2 * G < tiles) {
+          load_x(spar, a.iquv, nullptr, (t + 2 * G) * kTile, a.n, a.nl, base + sl * kIAct, row, half);
+          epi_arrive(&B->hready[sl]);
         }
       }
-      ok = mbar_wait(&B->mma, p.mph, &B->abort, a.err, kErrWaitMma) && ok;
-      p.mph ^= 1u;
-      __syncthreads();
-      ok = ok && !B->abort;
-      if (!ok) break;
-      tc_fence_after();
-      if (L == 0) {
-        hidden_epilogue(trow, 0, spar, base + kSA, row, half, nullptr);
-      } else if (L == 1) {
-        hidden_epilogue(trow, 0, spar + 256, base + kSA, row, half, nullptr);
-      } else if (half == 0) {
-        const int64_t b = t * kTile + row;
-        float o[16];
-        tmem_ld16(trow, o);
-        if (b < a.n) {
-          float y[kOut];
-#pragma unroll
-          for (int j = 0; j < kOut; ++j) y[j] = (o[j] + a.p->b3[j]) * a.p->out_scale[j] + a.p->out_mean[j];
-          double m[11];
-          outputs_to_model(y, a.guess, a.fix, m);
-#pragma unroll
-          for (int i = 0; i < 11; ++i) a.models[b * 11 + i] = m[i];
-        }
-      }
-      fence_proxy_async();
-      tc_fence_before();
-      __syncthreads();
-      tc_fence_after();
     }
   }
-  teardown(B, p, 256, a.err);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(B->tmem, 512);
 }
 
 // ---------------------------------------------------------------- training: forward + activation backward
@@ -1217,11 +1392,11 @@ cudaError_t predict(const DevNet& d, const float* iquv, int64_t n, int nl, const
   a.models = models;
   a.err = err;
   cudaError_t e =
-      cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+      cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kISmemBytes);
   if (e != cudaSuccess) return e;
   const int64_t tiles = (n + kTile - 1) / kTile;
   const int grid = (int)std::min<int64_t>(tiles, sm_count());
-  mlp_infer_kernel<<<grid, kThreads, kSmemBytes, s>>>(nm, a);
+  mlp_infer_kernel<<<grid, kIThreads, kISmemBytes, s>>>(nm, a);
   return cudaGetLastError();
 }
 

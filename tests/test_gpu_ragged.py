@@ -151,3 +151,22 @@ def test_ragged_batch_refuses_what_it_cannot_do(engine, rois):
     engine.configure(G.make_config(lam, L0, ZG, init=H.GUESS, slight=sl, fix=(1,) * 9 + (0, 1)))
     with pytest.raises(G.GmError):
         batch.invert_rois(engine, rois[:2], psf_for)
+
+
+def test_empty_rois_and_empty_batch(engine, rois):
+    """A ROI without pixels in a batch changes nothing for the others, and a
+    batch without pixels returns at once."""
+    engine.configure(base_config())
+    some = [rois[1], rois[2], rois[4]]
+    empty = (np.zeros((0, 4, len(rois[3][1])), np.float32), rois[3][1])
+    plain, st = batch.invert_rois(engine, some, psf_for)
+    mixed, st2 = batch.invert_rois(engine, [some[0], empty, some[1], some[2]], psf_for)
+    assert st2["pixels"] == st["pixels"]
+    assert len(mixed[1]["model"]) == 0
+    for p, g in zip(plain, [mixed[0], mixed[2], mixed[3]]):
+        for k in ("model", "chi2", "iters", "status"):
+            np.testing.assert_array_equal(p[k], g[k], err_msg=k)
+    none, st0 = batch.invert_rois(engine, [empty], psf_for)
+    assert st0["pixels"] == 0 and len(none[0]["model"]) == 0
+    nothing, stn = batch.invert_rois(engine, [], psf_for)
+    assert stn["pixels"] == 0 and nothing == []
