@@ -974,10 +974,10 @@ constexpr int kSolveH = 68, kSolveB = 2 * kSolveH;   // damping and buffer strid
 __host__ __device__ constexpr int solve_block(int p, int q) {   // p <= q: index in the lanes' order
   return p == q ? p : (p == 0 ? 4 + q : (p == 1 ? 7 + q : (p == 2 ? 9 + q : 14)));
 }
-__host__ __device__ constexpr int solve_slot(int b) {
-  constexpr int slot[15] = {10, 15, 5, 11, 12, 8, 6, 1, 3, 9, 4, 14, 7, 0, 13};
-  return slot[b];
-}
+// slots of the 15 blocks, 4 bits each (10, 15, 5, 11, 12, 8, 6, 1, 3, 9, 4,
+// 14, 7, 0, 13): a shift, not a table that device code would build in
+// local memory at every call
+__host__ __device__ constexpr int solve_slot(int b) { return (int)((0xd07e493168cb5faull >> (4 * b)) & 0xfu); }
 __host__ __device__ constexpr int solve_addr(int i, int j) {
   return i > j ? solve_addr(j, i) : 4 * solve_slot(solve_block(i / 2, j / 2)) + 2 * (i & 1) + (j & 1);
 }
@@ -996,10 +996,10 @@ struct SolvePlan {
 };
 
 template <int NS>
-__device__ __forceinline__ SolvePlan make_solve_plan(int lane) {
+__host__ __device__ constexpr SolvePlan make_solve_plan(int lane) {
   constexpr int G = 32 / NS;
   const int g = lane & (G - 1);
-  SolvePlan s;
+  SolvePlan s{};
   const int bp[15] = {0, 1, 2, 3, 4, 0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
   const int bq[15] = {0, 1, 2, 3, 4, 1, 2, 3, 4, 2, 3, 4, 3, 4, 4};
   const int pr[10] = {0, 2, 4, 1, 6, 3, 8, 5, 9, 7};
@@ -1030,6 +1030,20 @@ __device__ __forceinline__ SolvePlan make_solve_plan(int lane) {
     }
   return s;
 }
+
+// Every lane's plan for one and for two solves per call, built by the
+// compiler: a kernel loads its lane's plan instead of deriving it (a
+// prologue that a warp inverting one pixel per launch would pay in full).
+struct SolvePlans {
+  SolvePlan lane[32];
+};
+template <int NS>
+__host__ __device__ constexpr SolvePlans solve_plans() {
+  SolvePlans t{};
+  for (int l = 0; l < 32; ++l) t.lane[l] = make_solve_plan<NS>(l);
+  return t;
+}
+static __device__ const SolvePlans g_solve_plans[2] = {solve_plans<1>(), solve_plans<2>()};
 
 // Solves for damping 1 + flambda into sm.vec[0][0] and, with two solves per
 // call, for 1 + flambda2 into sm.vec[1][0].  `accurate` (the numerics mode)

@@ -93,7 +93,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
       for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
   }
 
-  const SolvePlan plan = make_solve_plan<Variant<V>::SOLVES>(lane);
+  const SolvePlan plan = g_solve_plans[Variant<V>::SOLVES - 1].lane[lane];
   Solve11Plan plan11;
   if constexpr (NT == 11) plan11 = make_solve11_plan(lane);
   unsigned long long my_iter = 0, my_acc = 0;
@@ -418,7 +418,7 @@ trial_kernel(const DevCfg c0, const InvertArgs a, const WaveArgs w, int wave, co
       for (int s = 0; s < 4; ++s) slg[k][s] = 0.f;
   }
   int cur = -1;   // grid whose constants are loaded (ragged batches)
-  const SolvePlan plan = make_solve_plan<NS>(lane);
+  const SolvePlan plan = g_solve_plans[NS - 1].lane[lane];
   Solve11Plan plan11;
   if constexpr (NT == 11) plan11 = make_solve11_plan(lane);
   const uint32_t n = wave == 0 ? (uint32_t)a.npix : w.cnt[wave - 1].n_next;
