@@ -501,12 +501,18 @@ static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::Inver
                                const float* iquv, const Arg& a_in, const Arg* const* outs, int nouts,
                                int64_t npix, int nl, bool prepass, double* learned, size_t need, cudaStream_t s) {
   const size_t row = 4 * (size_t)nl;
-  // two chunks or more, of at least four times kPipeChunk when there are
-  // more than two: the wave kernels prefer long launches
-  const int nch = (int)std::max<int64_t>(2, std::min<int64_t>(8, npix / (4 * kPipeChunk)));
+  // a short first chunk (kPipeChunk pixels), so that the device starts
+  // while the rest of the cube is still arriving, then one to seven equal
+  // chunks of up to about four times kPipeChunk (the wave kernels prefer
+  // long launches).  Below four times kPipeChunk, two equal halves.
+  const int64_t first = npix >= 4 * kPipeChunk ? kPipeChunk : npix / 2;
+  const int rest =
+      (int)std::max<int64_t>(1, std::min<int64_t>(7, (npix - first + 4 * kPipeChunk - 1) / (4 * kPipeChunk)));
+  const int nch = rest + 1;
+  auto cut = [&](int k) { return k == 0 ? (int64_t)0 : first + (npix - first) * (k - 1) / rest; };
   gm::DevCfg d1 = d;
   if (prepass) d1.init_mode = 1;
-  const int64_t most = (npix + nch - 1) / nch;
+  const int64_t most = std::max<int64_t>(first, (npix - first + rest - 1) / rest);
   // one wave chunk per pipeline chunk and stream
   const bool waves = want_waves(ctx, d1, ia) && wave_chunk_for(ctx, d1, need, most, 2) == most;
   gm::WaveBuffers wb[2];
@@ -523,7 +529,7 @@ static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::Inver
   if (e != cudaSuccess) return cuda_fail(ctx, e, "pipeline set-up");
   cudaEventRecord(ctx->ev0, s);
   for (int k = 0; k < nch && e == cudaSuccess; ++k) {
-    const int64_t a = npix * k / nch, b = npix * (k + 1) / nch, n = b - a;
+    const int64_t a = cut(k), b = cut(k + 1), n = b - a;
     cudaStream_t q = (k & 1) ? ctx->aux : s;
     gm::WorkCounters* w = (k & 1) ? ctx->work2 : ctx->work;
     e = cudaMemcpyAsync((float*)a_in.dev + a * row, iquv + a * row, sizeof(float) * row * n,

@@ -329,6 +329,29 @@ def test_pipelined_host_inversion_equals_one_launch(engine):
     assert st["iterations"] == int(host["iters"].sum())
 
 
+def test_pipelined_host_inversion_in_three_chunks(engine):
+    """A host cube large enough for a short first chunk and two long ones
+    (131 072 + 2 x 284 464 pixels, alternating streams) gives the results of
+    one launch over the cube in device memory, bit for bit."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(711)
+    P = 700000
+    fix = (1,) * 9 + (0, 1)
+    ocfg, gcfg, sl = configs(psf=True, stray=True, fix=fix)
+    engine.configure(gcfg)
+    t = H.truth_models(P, rng, alpha_range=(0.7, 1.0))
+    obs = engine.synthesize(t)
+    obs = np.ascontiguousarray(obs + rng.normal(0, 1e-3, obs.shape).astype(np.float32))
+    host = engine.invert(obs)
+    st = engine.stats()
+    dev = engine.invert(torch.from_numpy(obs).cuda())
+    torch.cuda.synchronize()
+    assert st["pixels"] == P
+    for k in ("model", "model64", "chi2", "iters", "accepted", "status"):
+        np.testing.assert_array_equal(host[k], dev[k].cpu().numpy(), err_msg=k)
+    assert st["iterations"] == int(host["iters"].sum())
+
+
 def test_classical_prepass_equals_in_kernel_estimates(engine):
     """gm_invert forms the classical start models in a pre-pass kernel;
     gm_invert_noalloc forms them inside the fused inversion kernel with the
