@@ -863,9 +863,12 @@ __device__ __forceinline__ int jrow(const DevCfg& c, uint32_t fixmask, int t, in
 // 11 terms) as one product J' W J'^T on the FP64 tensor cores: J' holds the
 // NT response functions and, as row NT, the residual, over the 4 nl columns
 // of the Stokes profiles; W the weights w_s / sigma^2.  alpha is the leading
-// NT x NT block and beta column NT (8x8 tiles (0,0), (0,1), (1,1) of the
-// symmetric 16x16 result; for this operand layout a lane's B element of
-// J'^T is its A element of J').  The reference sums each Stokes parameter in
+// NT x NT block and beta column NT: 8x8 tiles (0,0) and (0,1) of the
+// symmetric 16x16 result on the tensor cores (for this operand layout a
+// lane's B element of J'^T is its A element of J'), and of tile (1,1) the
+// few wanted entries -- rows 8 .. NT - 1 with themselves and with the
+// residual -- on the CUDA cores with warp sums, which frees the FP64 tensor
+// pipe that bounds the accept kernel.  The reference sums each Stokes parameter in
 // float; here the products and sums are double and alpha, beta are rounded
 // to float once.  Results land in sm.alpha (packed) and sm.beta.  alpha's RF
 // is taken from the mixed profile `syn` when alpha_mixed
@@ -898,7 +901,7 @@ __device__ __forceinline__ void normal_eq(const DevCfg& c, const double* m, bool
 #pragma unroll
   for (int i = 0; i < 11; ++i) fixmask |= (c.fix[i] ? 1u : 0u) << i;
   const float* rows0 = &sm.rows[0][0];
-  double d00[2] = {0.0, 0.0}, d01[2] = {0.0, 0.0}, d11[2] = {0.0, 0.0};
+  double d00[2] = {0.0, 0.0}, d01[2] = {0.0, 0.0};
 #pragma unroll 1
   for (int s = 0; s < 4; ++s) {
     bool s0d, s1d;
@@ -911,20 +914,65 @@ __device__ __forceinline__ void normal_eq(const DevCfg& c, const double* m, bool
       const double x0 = (double)r0[k0 + gc] * sc0, x1 = (double)r1[k0 + gc] * sc1;
       dmma_884(d00[0], d00[1], wd * x0, x0);
       dmma_884(d01[0], d01[1], wd * x0, x1);
-      dmma_884(d11[0], d11[1], wd * x1, x1);
     }
   }
-  // lane holds element (gr, 2 gc + i) of each tile
+  // rows 8 .. NT - 1 of J' with themselves and with the residual (tile
+  // (1, 1), of which only R (R + 3) / 2 entries are wanted) on the CUDA
+  // cores: each lane its own samples, then warp sums
+  constexpr int R = NT - 8, NE = R * (R + 3) / 2;
+  double acc[NE];
+#pragma unroll
+  for (int e = 0; e < NE; ++e) acc[e] = 0.0;
+#pragma unroll 1
+  for (int s = 0; s < 4; ++s) {
+    const double wd = (double)c.wsig[s];
+    const float* rr[R + 1];
+    double sc[R + 1];
+#pragma unroll
+    for (int t = 0; t <= R; ++t) {
+      bool scl;
+      rr[t] = rows0 + jrow<LPL, V>(c, fixmask, 8 + t, s, mac_on, scl) * row_pitch<LPL>();
+      sc[t] = scl ? alfa : 1.0;
+    }
+#pragma unroll
+    for (int k = 0; k < LPL; ++k) {
+      const int l = lane + 32 * k;
+      double x[R + 1];
+#pragma unroll
+      for (int t = 0; t <= R; ++t) x[t] = (double)rr[t][l] * sc[t];
+      int e = 0;
+#pragma unroll
+      for (int a = 0; a < R; ++a) {
+        const double wx = wd * x[a];
+#pragma unroll
+        for (int b = a; b <= R; ++b, ++e) acc[e] = fma(wx, x[b], acc[e]);
+      }
+    }
+  }
+  // lane holds element (gr, 2 gc + i) of each tensor-core tile
 #pragma unroll
   for (int i = 0; i < 2; ++i) {
     const int q = 2 * gc + i;
-    const int row[3] = {gr, gr, 8 + gr}, col[3] = {q, 8 + q, 8 + q};
-    const double val[3] = {d00[i], d01[i], d11[i]};
+    const int row[2] = {gr, gr}, col[2] = {q, 8 + q};
+    const double val[2] = {d00[i], d01[i]};
 #pragma unroll
-    for (int e = 0; e < 3; ++e) {
+    for (int e = 0; e < 2; ++e) {
       if (row[e] <= col[e] && col[e] < NT) sm.alpha[upk<NT>(row[e], col[e])] = (float)val[e];
       else if (col[e] == NT && row[e] < NT) sm.beta[row[e]] = (float)val[e];
     }
+  }
+  {
+    int e = 0;
+#pragma unroll
+    for (int a = 0; a < R; ++a)
+#pragma unroll
+      for (int b = a; b <= R; ++b, ++e) {
+        const double v = warp_sum_d(acc[e]);
+        if (lane == 0) {
+          if (b < R) sm.alpha[upk<NT>(8 + a, 8 + b)] = (float)v;
+          else sm.beta[8 + a] = (float)v;
+        }
+      }
   }
   __syncwarp();
 }
