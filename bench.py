@@ -49,7 +49,7 @@ MAXITER = 50
 # dram__bytes_write.sum summed over the 102 launches of an inversion) on
 # 65 536-pixel inversions of this workload with the current kernels;
 # traffic grows with the pixel count.
-DRAM_BYTES_PER_PIXEL = 223300.0
+DRAM_BYTES_PER_PIXEL = 206500.0
 
 # Algorithmic FLOPs per pixel (per-wavelength costs counted from the formulas)
 C_VOIGT, C_RTE, C_DVOIGT, C_DRTE = 100, 85, 23, 870
