@@ -169,6 +169,14 @@ __device__ __forceinline__ double* block_taps() { return reinterpret_cast<double
 // (S0's RF of Stokes I) and a row of zeros, all zero past nl.
 constexpr int kXAlpha = 0, kXRes = 4, kXOne = 8, kXZero = 9, kXRows = 10;
 
+// The 11-term solve's FP64 Jacobi matrix (12x12, double-buffered) and its
+// accumulated rotations; the elimination uses the first matrix.
+template <bool S11>
+struct Jacobi11 {
+  double A[S11 ? 2 : 1][S11 ? 144 : 1];
+  double V[S11 ? 2 : 1][S11 ? 144 : 1];
+};
+
 // Warp-private shared memory.
 template <int LPL, int V>
 struct WarpSmem {
@@ -189,11 +197,16 @@ struct WarpSmem {
   double gk[Variant<V>::MAC ? kMaxNl : 1];   // macroturbulence kernel (PSF folded in)
   double gd[Variant<V>::MAC ? kMaxNl : 1];   // its derivative with respect to v_mac
   double dd[12];         // FP64 step of the 11-term solve
-  double A11[S11 ? 2 : 1][S11 ? 144 : 1];    // 11-term Jacobi matrix (12x12), double-buffered
-  double V11[S11 ? 2 : 1][S11 ? 144 : 1];    // its accumulated rotations
   double b11[S11 ? 12 : 1], z11[S11 ? 12 : 1];
   double c11[S11 ? 6 : 1], s11[S11 ? 6 : 1]; // the step's rotations
-  float rows[NR][row_pitch<LPL>()];   // staged rows (PSF, macroturbulence, RFs)
+  // staged rows (PSF, macroturbulence, RFs), sharing their space with the
+  // 11-term solve's matrices: a trial solves before its synthesis stages
+  // any row, the accept half never solves, and the response functions are
+  // consumed by the normal equations before the next solve
+  union {
+    float rows[NR][row_pitch<LPL>()];
+    Jacobi11<S11> j11;
+  };
   // the normal equations' operand rows (kX*), right after `rows` with the
   // same pitch: row NR + x of the combined array is xrows[x]
   float xrows[kXRows][row_pitch<LPL>()];
@@ -1258,10 +1271,10 @@ __device__ __forceinline__ void solve11(WarpSmem<LPL, V>& sm, const Solve11Plan&
   static_assert(V == 2, "the FP64 solve belongs to the 11-term variant");
   // damped matrix in double (milosUtils.cu:787-791), padded to 12x12
   const double damp = 1.0 + (double)flambda;
-  double* A = sm.A11[0];
-  double* B = sm.A11[1];
-  double* Va = sm.V11[0];
-  double* Vb = sm.V11[1];
+  double* A = sm.j11.A[0];
+  double* B = sm.j11.A[1];
+  double* Va = sm.j11.V[0];
+  double* Vb = sm.j11.V[1];
   for (int i = lane; i < 144; i += 32) {
     const int r = i / 12, c = i - 12 * (i / 12);
     double v = 0.0;
@@ -1357,7 +1370,7 @@ template <int LPL, int V>
 __device__ __forceinline__ bool solve11_elim(WarpSmem<LPL, V>& sm, float flambda, int lane) {
   static_assert(V == 2, "the FP64 solve belongs to the 11-term variant");
   const double damp = 1.0 + (double)flambda;
-  double* A = sm.A11[0];
+  double* A = sm.j11.A[0];
   for (int i = lane; i < 144; i += 32) {
     const int r = i / 12, c = i - 12 * (i / 12);
     double v = 0.0;

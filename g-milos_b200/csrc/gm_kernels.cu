@@ -248,16 +248,28 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
 template <int LPL, int V>
 constexpr int trial_min_blocks() { return V == 2 ? (LPL == 1 ? 5 : 8) : (LPL == 1 ? 7 : 10); }
 template <int LPL, int V>
-constexpr int accept_min_blocks() { return V == 2 ? (LPL == 1 ? 3 : 4) : 5; }
+constexpr int accept_min_blocks() { return V == 2 ? (LPL == 1 ? 5 : 4) : 5; }
 
 // The trial half touches the warp's shared memory only up to the first
-// 8-row tile of staged rows (the synthesis PSF stages rows 0-3), so its
-// warps are packed at that stride: half the footprint, more warps per SM.
+// 8-row tile of staged rows (the synthesis PSF stages rows 0-3) -- or, in
+// the 11-term variant, up to the end of the solve's matrices that share the
+// rows' space -- so its warps are packed at that stride: half the
+// footprint, more warps per SM.
 template <int LPL, int V>
 __host__ __device__ constexpr size_t trial_warp_bytes() {
   using WS = WarpSmem<LPL, V>;
-  return (offsetof(WS, rows) + 8 * row_pitch<LPL>() * sizeof(float) + 15) & ~(size_t)15;
+  constexpr size_t tile = 8 * row_pitch<LPL>() * sizeof(float);
+  constexpr size_t solve = V == 2 ? sizeof(Jacobi11<true>) : 0;   // the 11-term solve's matrices
+  return (offsetof(WS, rows) + (tile > solve ? tile : solve) + 15) & ~(size_t)15;
 }
+template <int LPL, int V>
+constexpr bool xrows_follow_rows() {
+  using WS = WarpSmem<LPL, V>;
+  return offsetof(WS, xrows) == offsetof(WS, rows) + sizeof(WS::rows);
+}
+static_assert(xrows_follow_rows<1, 0>() && xrows_follow_rows<1, 1>() && xrows_follow_rows<1, 2>() &&
+                  xrows_follow_rows<2, 0>() && xrows_follow_rows<2, 1>() && xrows_follow_rows<2, 2>(),
+              "the operand rows must follow the staged rows");
 template <int LPL, int V>
 __device__ __forceinline__ WarpSmem<LPL, V>& trial_smem() {
   return *reinterpret_cast<WarpSmem<LPL, V>*>(gm_dyn_smem + tap_bytes<LPL>() +
