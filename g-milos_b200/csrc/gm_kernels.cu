@@ -248,7 +248,7 @@ invert_kernel(const DevCfg c, const InvertArgs a) {
 template <int LPL, int V>
 constexpr int trial_min_blocks() { return V == 2 ? (LPL == 1 ? 5 : 8) : (LPL == 1 ? 7 : 10); }
 template <int LPL, int V>
-constexpr int accept_min_blocks() { return V == 2 ? (LPL == 1 ? 5 : 4) : 5; }
+constexpr int accept_min_blocks() { return V == 2 ? (LPL == 1 ? 5 : 5) : 5; }
 
 // The trial half touches the warp's shared memory only up to the first
 // 8-row tile of staged rows (the synthesis PSF stages rows 0-3) -- or, in
