@@ -228,8 +228,8 @@ gm_status build_devcfg(gm_ctx* ctx, const gm_config& c, gm::DevCfg* d) {
   d->quirks = c.reference_quirks;
   if (c.numerics != GM_NUMERICS_REFERENCE && c.numerics != GM_NUMERICS_ACCURATE)
     return fail(ctx, GM_ERR_INVALID, "numerics must be GM_NUMERICS_REFERENCE or GM_NUMERICS_ACCURATE");
-  if (c.kernel != GM_KERNEL_AUTO && c.kernel != GM_KERNEL_FUSED)
-    return fail(ctx, GM_ERR_INVALID, "kernel must be GM_KERNEL_AUTO or GM_KERNEL_FUSED");
+  if (c.kernel != GM_KERNEL_AUTO && c.kernel != GM_KERNEL_FUSED && c.kernel != GM_KERNEL_WAVES)
+    return fail(ctx, GM_ERR_INVALID, "kernel must be GM_KERNEL_AUTO, GM_KERNEL_FUSED or GM_KERNEL_WAVES");
   d->numerics = c.numerics;
   d->n_pi = z.n_pi;
   d->n_sig = z.n_sig;
@@ -442,12 +442,22 @@ constexpr int64_t kPipeChunk = 131072;
 constexpr int64_t kWaveChunk = 1 << 20;
 constexpr int64_t kWaveMinChunk = 16384;
 
-// The wave-synchronous kernels cover the launch unless the configuration
-// selects the single persistent kernel (gm_config.kernel = GM_KERNEL_FUSED:
-// the two agree to rounding; the choice serves comparisons and the
-// bit-for-bit tests against gm_invert_noalloc).
-static bool want_waves(const gm_ctx* ctx, const gm::DevCfg& d, const gm::InvertArgs& ia) {
+// Calls (or served requests) of fewer pixels than this run the fused
+// persistent kernel under GM_KERNEL_AUTO: there the wave kernels' ~100 short
+// launches cost more than their split saves (measured on B200 at 30
+// samples: 4096 pixels with a PSF invert 1.4x faster fused, without one
+// 1.9x; the two are even at 16384 pixels with a PSF and at ~32768 without).
+static int64_t fused_below(const gm::DevCfg& d) { return d.use_psf ? 16384 : 32768; }
+
+// Which kernels invert a call of npix pixels: the wave-synchronous kernels
+// where they cover the configuration, unless the configuration selects the
+// single persistent kernel (GM_KERNEL_FUSED: the two agree to rounding; the
+// choice serves comparisons and the bit-for-bit tests against
+// gm_invert_noalloc) or, under GM_KERNEL_AUTO, the call is small.  A served
+// request decides by its whole size, as the lone gm_invert of it does.
+static bool want_waves(const gm_ctx* ctx, const gm::DevCfg& d, const gm::InvertArgs& ia, int64_t npix) {
   if (ctx->cfg.kernel == GM_KERNEL_FUSED) return false;
+  if (ctx->cfg.kernel == GM_KERNEL_AUTO && npix < fused_below(d)) return false;
   return gm::waves_cover(d, ia);
 }
 
@@ -514,7 +524,7 @@ static gm_status invert_chunks(gm_ctx* ctx, const gm::DevCfg& d, const gm::Inver
   if (prepass) d1.init_mode = 1;
   const int64_t most = std::max<int64_t>(first, (npix - first + rest - 1) / rest);
   // one wave chunk per pipeline chunk and stream
-  const bool waves = want_waves(ctx, d1, ia) && wave_chunk_for(ctx, d1, need, most, 2) == most;
+  const bool waves = want_waves(ctx, d1, ia, npix) && wave_chunk_for(ctx, d1, need, most, 2) == most;
   gm::WaveBuffers wb[2];
   if (waves) {
     gm_status st = wave_buffers(ctx, "waves0", d1, most, &wb[0]);
@@ -702,7 +712,7 @@ static gm_status invert_impl(gm_ctx* ctx, const gm::DevCfg& dcfg, const float* i
   }
   gm::InvertGeometry geo;
   const int64_t grid = invert_grid(d, ia.init_models != nullptr && !ia.init_status, ctx->sms, npix, &geo);
-  const int64_t wchunk = want_waves(ctx, d, ia) ? wave_chunk_for(ctx, d, need, npix, 1) : 0;
+  const int64_t wchunk = want_waves(ctx, d, ia, npix) ? wave_chunk_for(ctx, d, need, npix, 1) : 0;
   const bool waves = wchunk > 0;
   gm::WaveBuffers wb{};
   if (waves && (st = wave_buffers(ctx, "waves0", d, wchunk, &wb)) != GM_OK) return st;
@@ -1132,7 +1142,7 @@ gm_status launch_chunk(gm_ctx* ctx, ServeLane& L, const std::shared_ptr<Request>
     ia.init_status = cs;
     d.init_mode = 1;
   }
-  if (lane_ok && want_waves(ctx, d, ia)) {
+  if (lane_ok && want_waves(ctx, d, ia, q.npix)) {
     e = gm::launch_invert_waves(d, ia, gm::wave_buffers(L.scratch, d.nl, d.miter, L.chunk), s, nullptr);
   } else {
     const int64_t grid = invert_grid(d, ia.init_models != nullptr && !ia.init_status, ctx->sms, n, nullptr);

@@ -33,7 +33,7 @@ INIT_CLASSICAL, INIT_GIVEN, INIT_PER_PIXEL, INIT_LEARNED = 0, 1, 2, 3
 PIX_LEARNED_INIT = 0x40
 MLP_IN, MLP_HIDDEN, MLP_OUT, MLP_OUT_PAD = 128, 256, 9, 16
 NUMERICS_REFERENCE, NUMERICS_ACCURATE = 0, 1
-KERNEL_AUTO, KERNEL_FUSED = 0, 1
+KERNEL_AUTO, KERNEL_FUSED, KERNEL_WAVES = 0, 1, 2
 SERVE_ROUND_ROBIN, SERVE_FIFO, SERVE_SHORTEST_FIRST, SERVE_RESPONSE_RATIO = 0, 1, 2, 3
 
 # Symbols include/gmilos.h declares (checked by the tests against the .so).
@@ -265,9 +265,11 @@ def make_config(lam, lambda0, zeeman, psf=None, mu=1.0, weight=(1, 1, 1, 1), noi
     """Engine configuration (gm_config).  lambda_map: optional per-pixel
     wavelength grids [P][nl] (absolute, A; numpy or a CUDA tensor of float64),
     read at each call like a per-pixel stray map; `lam` then only sizes the
-    grid and the PSF stays `psf`.  kernel: KERNEL_AUTO (wave-synchronous
-    kernels where they cover the call) or KERNEL_FUSED (the fused kernel for
-    every call).  mlp: a trained Mlp for init_mode INIT_LEARNED."""
+    grid and the PSF stays `psf`.  kernel: KERNEL_AUTO (the fused kernel for
+    calls of fewer than 16384 pixels, 32768 without a PSF, else the
+    wave-synchronous kernels where they cover the call), KERNEL_FUSED (the
+    fused kernel for every call) or KERNEL_WAVES (the wave kernels wherever
+    they cover the call).  mlp: a trained Mlp for init_mode INIT_LEARNED."""
     c = Config()
     lib().gm_config_defaults(C.byref(c))
     lam = np.asarray(lam, dtype=np.float64)

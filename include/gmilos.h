@@ -152,11 +152,14 @@ typedef struct {
                                      those of `psf`.  The reference's per-pixel
                                      wavelength FITS (utilsFits.c:1488-1500). */
     const double *lambda_map;     /* [P][nl] absolute wavelengths [A], host or device */
-    int kernel;                   /* GM_KERNEL_AUTO (default): the wave-synchronous
-                                     kernels where they cover the call, else the
-                                     fused kernel; GM_KERNEL_FUSED: the fused
-                                     persistent kernel for every call (the kernel
-                                     of gm_invert_noalloc) */
+    int kernel;                   /* GM_KERNEL_AUTO (default): the fused kernel
+                                     for calls of fewer than 16384 pixels (32768
+                                     without a PSF), else the wave-synchronous
+                                     kernels where they cover the call;
+                                     GM_KERNEL_FUSED: the fused persistent kernel
+                                     for every call (the kernel of
+                                     gm_invert_noalloc); GM_KERNEL_WAVES: the
+                                     wave kernels wherever they cover the call */
     const gm_mlp *mlp;            /* network of GM_INIT_LEARNED (host memory, copied
                                      at gm_configure; its nl must be the grid's) */
 } gm_config;
@@ -165,6 +168,7 @@ typedef struct {
  * compiled as different kernels they round differently at the float level. */
 #define GM_KERNEL_AUTO 0
 #define GM_KERNEL_FUSED 1
+#define GM_KERNEL_WAVES 2
 
 /* Trigonometry of the 10x10 Jacobi solve and of the field angles.
  * REFERENCE uses the hardware approximations the reference uses
@@ -197,7 +201,8 @@ gm_status gm_configure(gm_ctx *ctx, const gm_config *cfg);
  * normal equations of the accepted ones, over chunks of up to 2^20 pixels
  * whose LM state (about 4 KB per pixel at nl <= 32, 7.4 KB above) the
  * context keeps in device memory within its HBM budget.  First-step outputs
- * (gm_lm_step), in-kernel classical estimates (gm_invert_noalloc) and calls
+ * (gm_lm_step), in-kernel classical estimates (gm_invert_noalloc), calls of
+ * fewer than 16384 pixels (32768 without a PSF; GM_KERNEL_AUTO) and calls
  * whose budget leaves room for fewer than 16384 pixels of state run one fused
  * persistent kernel.  Both execute the same LM arithmetic; compiled
  * as different kernels they round differently at the float level, so their

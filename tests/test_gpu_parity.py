@@ -195,7 +195,7 @@ def test_wave_and_fused_kernels_agree(engine, nl):
     obs = H.observations(ocfg, t, rng, slight=sl)
     mr, cr, _, _, _ = O.lm_batch_f(ocfg, obs, slight=sl, nthreads=0)
     res = {}
-    for mode, kernel in (("waves", G.KERNEL_AUTO), ("fused", G.KERNEL_FUSED)):
+    for mode, kernel in (("waves", G.KERNEL_WAVES), ("fused", G.KERNEL_FUSED)):
         gcfg.kernel = kernel
         engine.configure(gcfg)
         full = engine.invert(obs)

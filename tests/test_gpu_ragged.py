@@ -98,8 +98,9 @@ def test_graph_replay_and_tuning_change_nothing(engine, rois):
 
 @pytest.mark.parametrize("numerics", [G.NUMERICS_REFERENCE, G.NUMERICS_ACCURATE])
 def test_batch_against_plain_inversions(engine, rois, numerics):
-    """The ragged-batch kernels and the one-grid wave kernels run the same
-    LM arithmetic.  At <= 32 samples they compile to the same results bit
+    """The ragged-batch kernels and the one-grid wave kernels (chosen
+    explicitly: small calls would otherwise run the fused kernel) run the
+    same LM arithmetic.  At <= 32 samples they compile to the same results bit
     for bit; at 33..64 samples they round differently, and in REFERENCE
     numerics (hardware trigonometry in the solve) the trajectories then part
     on some pixels as between any two builds: neither side is worse more
@@ -109,7 +110,7 @@ def test_batch_against_plain_inversions(engine, rois, numerics):
     worse_b, worse_p, agree, tot = 0, 0, 0, 0
     for (a, lam), g in zip(rois[1:6], got[1:6]):
         engine.configure(G.make_config(lam, L0, ZG, psf=psf_for(lam), init=H.GUESS, stop_dchi2=STOP,
-                                       numerics=numerics))
+                                       numerics=numerics, kernel=G.KERNEL_WAVES))
         ref = engine.invert(a)
         same = H.fits_agree(np.asarray(g["model"], dtype=np.float64), ref["model64"])
         wb = ~same & (g["chi2"] > ref["chi2"] * (1 + 1e-3) + 1e-6)
