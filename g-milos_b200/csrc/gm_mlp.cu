@@ -1047,12 +1047,19 @@ mlp_wgrad_kernel(const __grid_constant__ WgradMaps wm, const WgradArgs a) {
     for (int h = 0; h < 2; ++h) {
       float v[32];
       tmem_ld32(trow + 32 * h, v);
+      if (g < 2) {
+        // this thread's 32 columns are contiguous in its row of dW1 / dW2
+        // (16-byte aligned): vector reductions, a quarter of the atomics
+        float* dst = (g == 0 ? a.dw1 + m * kIn : a.dw2 + m * kHid) + nb * 64 + 32 * h;
+#pragma unroll
+        for (int e = 0; e < 32; e += 4)
+          atomicAdd(reinterpret_cast<float4*>(dst + e), make_float4(v[e], v[e + 1], v[e + 2], v[e + 3]));
+      } else {
 #pragma unroll 4
-      for (int e = 0; e < 32; ++e) {
-        const int n = nb * 64 + 32 * h + e;
-        if (g == 0) atomicAdd(a.dw1 + m * kIn + n, v[e]);
-        else if (g == 1) atomicAdd(a.dw2 + m * kHid + n, v[e]);
-        else if (n < kOut) atomicAdd(a.dw3 + n * kHid + m, v[e]);
+        for (int e = 0; e < 32; ++e) {
+          const int n = nb * 64 + 32 * h + e;
+          if (n < kOut) atomicAdd(a.dw3 + n * kHid + m, v[e]);
+        }
       }
     }
   }
