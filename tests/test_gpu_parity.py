@@ -214,6 +214,28 @@ def test_wave_and_fused_kernels_agree(engine, nl):
     assert np.median(w["chi2"]) == pytest.approx(np.median(f["chi2"]), rel=1e-2)
 
 
+def test_small_calls_run_the_fused_kernel(engine):
+    """Under GM_KERNEL_AUTO a call of fewer than 16 384 pixels (with a PSF)
+    runs the fused persistent kernel (pre-pass + one launch), a larger one
+    the wave kernels (pre-pass + 101 launches); GM_KERNEL_WAVES keeps the
+    small call on the wave kernels.  Both fit equally well."""
+    rng = np.random.default_rng(745)
+    ocfg, gcfg, _ = configs(psf=True)
+    small = H.observations(ocfg, H.truth_models(4096, rng), rng)
+    large = H.observations(ocfg, H.truth_models(16384, rng), rng)
+    engine.configure(gcfg)
+    fused = engine.invert(small)
+    assert engine.stats()["kernel_launches"] == 2
+    engine.invert(large)
+    assert engine.stats()["kernel_launches"] == 2 + 2 * 50
+    gcfg.kernel = G.KERNEL_WAVES
+    engine.configure(gcfg)
+    waves = engine.invert(small)
+    assert engine.stats()["kernel_launches"] == 2 + 2 * 50
+    assert np.median(waves["chi2"]) == pytest.approx(np.median(fused["chi2"]), rel=1e-2)
+    assert abs(waves["iters"].mean() - fused["iters"].mean()) < 0.5
+
+
 def test_wave_state_within_the_hbm_budget():
     """The wave kernels keep about 4 KB of LM state per pixel of a chunk in
     the context's budget; a budget with room for fewer than 16 384 pixels
