@@ -63,6 +63,27 @@ def test_inference_matches_oracle(engine, nl, n):
     np.testing.assert_array_equal(got[:, 9:], np.tile(np.asarray(H.GUESS)[9:], (n, 1)))
 
 
+def test_inference_with_tiles_in_flight_matches_oracle(engine):
+    """Enough pixels that every CTA of the persistent inference kernel runs
+    tiles through both of its slots and starts a second pair (3 tiles per
+    CTA on 148 SMs, one CTA 4, the last tile partial): the outputs equal
+    the oracle's as they do for small calls."""
+    ocfg, gcfg = config(30)
+    net = H.random_net(61, 30)
+    n = 148 * 128 * 3 + 77
+    rng = np.random.default_rng(62)
+    engine.configure(gcfg)
+    obs = engine.synthesize(H.truth_models(n, rng))
+    obs = np.ascontiguousarray(obs + rng.normal(0, 1e-3, obs.shape).astype(np.float32))
+    got = engine.mlp_predict(net, obs)
+    want, _ = M.predict(M.params(net), obs, H.GUESS, H.FREE9)
+    p = M.params(net)
+    err = np.abs(M.targets(got) - M.targets(want)) / p["out_scale"][:M.OUT]
+    print("inference with tiles in flight (%d px): standardised output error p50 %.2e p99 %.2e max %.2e"
+          % (n, np.median(err), np.percentile(err, 99), err.max()))
+    assert np.percentile(err, 99) < 5e-3 and np.median(err) < 5e-4
+
+
 def test_gradients_match_oracle(engine):
     ocfg, gcfg = config()
     net = H.random_net(21)
