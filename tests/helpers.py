@@ -123,3 +123,24 @@ def random_net(seed, nl=30, realistic=True):
         a["in_mean"][:4 * nl] = rng.normal(0, 0.1, 4 * nl)
         a["in_scale"][:4 * nl] = rng.uniform(5, 20, 4 * nl)
     return net
+
+
+def invert_each_kernel(engine, gcfg, obs, **kw):
+    """Yields ("waves", out) and ("fused", out): `obs` inverted once by the
+    wave-synchronous kernels and once by the fused persistent kernel under
+    the configuration `gcfg` (restored to the automatic choice afterwards).
+    Calls of a few thousand pixels run the fused kernel by default, so the
+    inversion parity tests run both kernels against one oracle result."""
+    import gmilos_b200 as G
+    try:
+        for name, kernel in (("waves", G.KERNEL_WAVES), ("fused", G.KERNEL_FUSED)):
+            gcfg.kernel = kernel
+            engine.configure(gcfg)
+            out = engine.invert(obs, **kw)
+            launches = engine.stats()["kernel_launches"]
+            if len(obs):
+                assert (launches > 2) if name == "waves" else (launches <= 2), (name, launches)
+            yield name, out
+    finally:
+        gcfg.kernel = G.KERNEL_AUTO
+        engine.configure(gcfg)

@@ -163,22 +163,21 @@ def test_inversion_matches_reference(engine, psf, stray):
     ocfg, gcfg, sl = configs(psf=psf, stray=stray, fix=fix, numerics=1)
     t = H.truth_models(1024, rng, alpha_range=(0.7, 1.0) if stray else None)
     obs = H.observations(ocfg, t, rng, slight=sl)
-    engine.configure(gcfg)
-    out = engine.invert(obs, fitted=True)
     mr, cr, ir, ar, fr = O.lm_batch_f(ocfg, obs, slight=sl, nthreads=0)
-    mg, cg = out["model64"], out["chi2"]
-    ok = close_enough(mg, cg, mr, cr)
-    no_worse = cg <= cr * (1 + 1e-3) + 1e-6
-    print("agree %.4f  chi2-no-worse %.4f  iters gpu %.1f ref %.1f" % (ok.mean(), no_worse.mean(),
-                                                                       out["iters"].mean(), ir.mean()))
-    assert ok.mean() >= 0.95
-    assert (ok | no_worse).mean() >= 0.99
-    same = ok & (out["iters"] == ir)
-    # where the trajectories agree, the fitted profiles agree too; the fitted
-    # output is the last trial, which may be a rejected step taken with a
-    # large damping, and rounding can still move that one
-    frel = H.rel_to_I(out["fitted"][same], fr[same]).max(axis=-1)
-    assert (frel < 1e-4).mean() >= 0.98, np.percentile(frel, [50, 99])
+    for name, out in H.invert_each_kernel(engine, gcfg, obs, fitted=True):
+        mg, cg = out["model64"], out["chi2"]
+        ok = close_enough(mg, cg, mr, cr)
+        no_worse = cg <= cr * (1 + 1e-3) + 1e-6
+        print("%s: agree %.4f  chi2-no-worse %.4f  iters gpu %.1f ref %.1f"
+              % (name, ok.mean(), no_worse.mean(), out["iters"].mean(), ir.mean()))
+        assert ok.mean() >= 0.95, name
+        assert (ok | no_worse).mean() >= 0.99, name
+        same = ok & (out["iters"] == ir)
+        # where the trajectories agree, the fitted profiles agree too; the
+        # fitted output is the last trial, which may be a rejected step taken
+        # with a large damping, and rounding can still move that one
+        frel = H.rel_to_I(out["fitted"][same], fr[same]).max(axis=-1)
+        assert (frel < 1e-4).mean() >= 0.98, (name, np.percentile(frel, [50, 99]))
 
 
 @pytest.mark.parametrize("nl", [30, 45])
@@ -285,21 +284,21 @@ def test_calls_on_two_streams_take_the_scratch_in_turn(engine):
 def test_inversion_edge_cases(engine):
     rng = np.random.default_rng(500)
     ocfg, gcfg, _ = configs(numerics=1)
-    engine.configure(gcfg)
     t = H.truth_models(37, rng)                         # not a multiple of the warps per block
     obs = H.observations(ocfg, t, rng)
     obs[3] = np.nan                                     # a bad pixel
     obs[5, 0, :3] = -1.0                                # leading "ghost" samples
-    out = engine.invert(obs)
-    assert out["iters"].min() >= 1 and out["iters"].max() <= 50
     mr, cr, ir, ar, fr = O.lm_batch_f(ocfg, obs)
     good = np.ones(len(t), bool)
     good[3] = False
-    ok = close_enough(out["model64"][good], out["chi2"][good], mr[good], cr[good])
-    nw = out["chi2"][good] <= cr[good] * (1 + 1e-3) + 1e-6
-    assert (ok | nw).mean() >= 0.95
-    assert out["status"][3] & (G.PIX_NONFINITE | G.PIX_INIT_NAN)
+    for name, out in H.invert_each_kernel(engine, gcfg, obs):
+        assert out["iters"].min() >= 1 and out["iters"].max() <= 50, name
+        ok = close_enough(out["model64"][good], out["chi2"][good], mr[good], cr[good])
+        nw = out["chi2"][good] <= cr[good] * (1 + 1e-3) + 1e-6
+        assert (ok | nw).mean() >= 0.95, name
+        assert out["status"][3] & (G.PIX_NONFINITE | G.PIX_INIT_NAN), name
     # an empty request is fine
+    engine.configure(gcfg)
     empty = np.zeros((0, 4, 30), np.float32)
     o0 = engine.invert(empty)
     assert o0["chi2"].shape == (0,)
@@ -309,15 +308,17 @@ def test_results_do_not_depend_on_scheduling(engine):
     """Work stealing changes which warp takes a pixel, never its result."""
     rng = np.random.default_rng(600)
     ocfg, gcfg, _ = configs(psf=True)
-    engine.configure(gcfg)
     t = H.truth_models(300, rng)
     obs = H.observations(ocfg, t, rng)
-    a = engine.invert(obs)
-    b = engine.invert(obs[::-1].copy())
-    np.testing.assert_array_equal(a["model"], b["model"][::-1])
-    np.testing.assert_array_equal(a["chi2"], b["chi2"][::-1])
-    single = engine.invert(obs[7:8].copy())
-    np.testing.assert_array_equal(single["model"][0], a["model"][7])
+    for kernel in (G.KERNEL_WAVES, G.KERNEL_FUSED):
+        gcfg.kernel = kernel
+        engine.configure(gcfg)
+        a = engine.invert(obs)
+        b = engine.invert(obs[::-1].copy())
+        np.testing.assert_array_equal(a["model"], b["model"][::-1])
+        np.testing.assert_array_equal(a["chi2"], b["chi2"][::-1])
+        single = engine.invert(obs[7:8].copy())
+        np.testing.assert_array_equal(single["model"][0], a["model"][7])
 
 
 def test_pipelined_host_inversion_equals_one_launch(engine):
@@ -429,14 +430,13 @@ def test_inversion_across_grid_sizes(engine, nl, psf):
     ocfg, gcfg, _ = configs(nl=nl, psf=psf, numerics=1)
     t = H.truth_models(512, rng)
     obs = H.observations(ocfg, t, rng)
-    engine.configure(gcfg)
-    out = engine.invert(obs)
     mr, cr, ir, ar, fr = O.lm_batch_f(ocfg, obs, nthreads=0)
-    ok = close_enough(out["model64"], out["chi2"], mr, cr)
-    no_worse = out["chi2"] <= cr * (1 + 1e-3) + 1e-6
-    print("nl %d: agree %.4f  chi2-no-worse %.4f" % (nl, ok.mean(), no_worse.mean()))
-    assert ok.mean() >= 0.95
-    assert (ok | no_worse).mean() >= 0.99
+    for name, out in H.invert_each_kernel(engine, gcfg, obs):
+        ok = close_enough(out["model64"], out["chi2"], mr, cr)
+        no_worse = out["chi2"] <= cr * (1 + 1e-3) + 1e-6
+        print("nl %d %s: agree %.4f  chi2-no-worse %.4f" % (nl, name, ok.mean(), no_worse.mean()))
+        assert ok.mean() >= 0.95, name
+        assert (ok | no_worse).mean() >= 0.99, name
 
 
 def test_twelve_sample_grid(engine):
@@ -462,17 +462,17 @@ def test_twelve_sample_grid(engine):
                     / max(np.linalg.norm(O.lm_step_f(ocfg, start[p], obs[p], 0.1)[0][:9]), 1e-30)
                     for p in range(256)])
     assert np.percentile(rel, 99) < 1e-4, np.percentile(rel, [50, 99])
-    out = engine.invert(obs)
     mr, cr, ir, ar, fr = O.lm_batch_f(ocfg, obs, nthreads=0)
-    mg, cg = out["model64"], out["chi2"]
-    agree = close_enough(mg, cg, mr, cr)
-    worse_g = ~agree & (cg > cr * (1 + 1e-3) + 1e-6)
-    worse_r = ~agree & (cr > cg * (1 + 1e-3) + 1e-6)
-    print("nl 12: agree %.4f  engine worse %.4f  oracle worse %.4f  median chi2 %.4f / %.4f"
-          % (agree.mean(), worse_g.mean(), worse_r.mean(), np.median(cg), np.median(cr)))
-    assert agree.mean() >= 0.88
-    assert worse_g.mean() <= worse_r.mean() + 0.02
-    assert np.median(cg) == pytest.approx(np.median(cr), rel=0.01)
+    for name, out in H.invert_each_kernel(engine, gcfg, obs):
+        mg, cg = out["model64"], out["chi2"]
+        agree = close_enough(mg, cg, mr, cr)
+        worse_g = ~agree & (cg > cr * (1 + 1e-3) + 1e-6)
+        worse_r = ~agree & (cr > cg * (1 + 1e-3) + 1e-6)
+        print("nl 12 %s: agree %.4f  engine worse %.4f  oracle worse %.4f  median chi2 %.4f / %.4f"
+              % (name, agree.mean(), worse_g.mean(), worse_r.mean(), np.median(cg), np.median(cr)))
+        assert agree.mean() >= 0.88, name
+        assert worse_g.mean() <= worse_r.mean() + 0.02, name
+        assert np.median(cg) == pytest.approx(np.median(cr), rel=0.01), name
 
 
 @pytest.mark.parametrize("fix", [(1, 1, 1, 1, 1, 1, 1, 0, 0, 0, 0),      # 7 free, S0 S1 fixed
@@ -487,13 +487,12 @@ def test_fixed_parameter_sets(engine, fix):
         t[:, 3] = H.GUESS[3]
         t[:, 4] = H.GUESS[4]
     obs = H.observations(ocfg, t, rng)
-    engine.configure(gcfg)
-    out = engine.invert(obs)
-    for i in range(11):
-        if not fix[i] and i not in (1, 2, 5, 6):
-            assert (out["model64"][:, i] == H.GUESS[i]).all()
     mr, cr, ir, ar, fr = O.lm_batch_f(ocfg, obs)
-    assert close_enough(out["model64"], out["chi2"], mr, cr).mean() >= 0.95
+    for name, out in H.invert_each_kernel(engine, gcfg, obs):
+        for i in range(11):
+            if not fix[i] and i not in (1, 2, 5, 6):
+                assert (out["model64"][:, i] == H.GUESS[i]).all(), name
+        assert close_enough(out["model64"], out["chi2"], mr, cr).mean() >= 0.95, name
 
 
 def test_stray_light_map_per_pixel(engine):
@@ -509,11 +508,10 @@ def test_stray_light_map_per_pixel(engine):
     obs = H.observations(ocfg, t, rng, slight=slmap, slight_per_pixel=True)
     gcfg = G.make_config(lam, l0, G.zeeman_from_levels(2, 1, 1.0, 2, 2, 0.0, 1.0), fix=fix, init=H.GUESS,
                          slight=slmap, slight_per_pixel=True, numerics=1)
-    engine.configure(gcfg)
-    out = engine.invert(obs)
     mr, cr, ir, ar, fr = O.lm_batch_f(ocfg, obs, slight=slmap, slight_per_pixel=True)
-    assert close_enough(out["model64"], out["chi2"], mr, cr).mean() >= 0.95
-    assert np.abs(out["model64"][:, 10] - mr[:, 10]).max() < 0.05
+    for name, out in H.invert_each_kernel(engine, gcfg, obs):
+        assert close_enough(out["model64"], out["chi2"], mr, cr).mean() >= 0.95, name
+        assert np.abs(out["model64"][:, 10] - mr[:, 10]).max() < 0.05, name
 
 
 @pytest.mark.parametrize("weight,logc", [((1, 0, 0, 1), 0), ((1, 1, 1, 1), 1)])
@@ -524,13 +522,12 @@ def test_zero_weights_and_logclambda(engine, weight, logc):
     ocfg, gcfg, _ = configs(weight=weight, logclambda=logc, numerics=1)
     t = H.truth_models(256, rng)
     obs = H.observations(ocfg, t, rng)
-    engine.configure(gcfg)
-    out = engine.invert(obs)
     mr, cr, ir, ar, fr = O.lm_batch_f(ocfg, obs)
-    ok = close_enough(out["model64"], out["chi2"], mr, cr)
-    nw = out["chi2"] <= cr * (1 + 1e-3) + 1e-6
-    assert (ok | nw).mean() >= 0.95
-    assert np.median(out["chi2"]) == pytest.approx(np.median(cr), rel=0.02)
+    for name, out in H.invert_each_kernel(engine, gcfg, obs):
+        ok = close_enough(out["model64"], out["chi2"], mr, cr)
+        nw = out["chi2"] <= cr * (1 + 1e-3) + 1e-6
+        assert (ok | nw).mean() >= 0.95, name
+        assert np.median(out["chi2"]) == pytest.approx(np.median(cr), rel=0.02), name
 
 
 @pytest.mark.parametrize("psf", [False, True])
@@ -542,14 +539,13 @@ def test_reference_numerics_fit_quality(engine, psf):
     ocfg, gcfg, _ = configs(psf=psf, numerics=0)
     t = H.truth_models(1024, rng)
     obs = H.observations(ocfg, t, rng)
-    engine.configure(gcfg)
-    out = engine.invert(obs)
     mr, cr, ir, ar, fr = O.lm_batch_f(ocfg, obs)
-    assert np.median(out["chi2"]) == pytest.approx(np.median(cr), rel=0.02)
-    rec_g = (np.abs(out["model64"][:, 1] - t[:, 1]) < 50).mean()
     rec_r = (np.abs(mr[:, 1] - t[:, 1]) < 50).mean()
-    assert abs(rec_g - rec_r) < 0.03
-    assert abs(out["iters"].mean() - ir.mean()) < 2.0
+    for name, out in H.invert_each_kernel(engine, gcfg, obs):
+        assert np.median(out["chi2"]) == pytest.approx(np.median(cr), rel=0.02), name
+        rec_g = (np.abs(out["model64"][:, 1] - t[:, 1]) < 50).mean()
+        assert abs(rec_g - rec_r) < 0.03, name
+        assert abs(out["iters"].mean() - ir.mean()) < 2.0, name
 
 
 def test_invalid_configurations_are_errors(engine):

@@ -63,16 +63,16 @@ def test_one_iteration_matches_reference_host_build(engine, psf, stray):
     fix = FIX if stray else H.FREE9
     ocfg, s, gcfg, sl = setups(psf, stray, miter=1, numerics=G.NUMERICS_ACCURATE, fix=fix)
     t, obs = cube(ocfg, sl, 1024, 21)
-    engine.configure(gcfg)
-    out = engine.invert(obs)
     mr, cr, ir, _ = ref.invert_cpu(s, obs, slight=sl)
-    rel = np.abs(out["model64"] - mr) / np.maximum(np.abs(mr), 1e-3)
-    crel = np.abs(out["chi2"] - cr) / cr
-    print("one iteration vs reference host build: model rel p50 %.2e p99 %.2e max %.2e, chi2 rel max %.2e"
-          % (np.percentile(rel[:, :9], 50), np.percentile(rel[:, :9], 99), rel[:, :9].max(), crel.max()))
-    assert (out["iters"] == ir).all()
-    assert np.percentile(rel[:, :9], 99) < 1e-4
-    assert np.percentile(crel, 99) < 1e-4
+    for name, out in H.invert_each_kernel(engine, gcfg, obs):
+        rel = np.abs(out["model64"] - mr) / np.maximum(np.abs(mr), 1e-3)
+        crel = np.abs(out["chi2"] - cr) / cr
+        print("%s, one iteration vs reference host build: model rel p50 %.2e p99 %.2e max %.2e, "
+              "chi2 rel max %.2e" % (name, np.percentile(rel[:, :9], 50), np.percentile(rel[:, :9], 99),
+                                     rel[:, :9].max(), crel.max()))
+        assert (out["iters"] == ir).all(), name
+        assert np.percentile(rel[:, :9], 99) < 1e-4, name
+        assert np.percentile(crel, 99) < 1e-4, name
 
 
 @pytest.mark.skipif(not (ref.available(gpu=True) and ref.available()),
@@ -142,19 +142,8 @@ def test_one_iteration_reference_numerics_vs_reference_gpu_build(engine, psf, st
     fix = FIX if stray else H.FREE9
     ocfg, s, gcfg, sl = setups(psf, stray, miter=1, numerics=G.NUMERICS_REFERENCE, fix=fix)
     t, obs = cube(ocfg, sl, 4096, 24)
-    engine.configure(gcfg)
-    out = engine.invert(obs)
     mr, cr, ir, _, rep = ref.invert_gpu(s, obs, slight=sl, nstreams=16)
     assert rep["malloc_failures"] == 0
-    rel = np.abs(out["model64"] - mr) / np.maximum(np.abs(mr), 1e-3)
-    crel = np.abs(out["chi2"] - cr) / cr
-    # the output is the last accepted model: a different accept/reject
-    # decision shows as a whole step's difference, far above 1e-3
-    same = (rel[:, :9].max(axis=1) < 1e-3).mean()
-    print("one iteration, REFERENCE numerics vs reference sm_100a build: same decision %.4f, model rel "
-          "p50 %.2e p99 %.2e max %.2e, chi2 rel p99 %.2e"
-          % (same, np.percentile(rel[:, :9], 50), np.percentile(rel[:, :9], 99), rel[:, :9].max(),
-             np.percentile(crel, 99)))
     # the reference's own host build against its sm_100a build, same step
     mh, ch, ih, _ = ref.invert_cpu(s, obs, slight=sl)
     relh = np.abs(mh - mr) / np.maximum(np.abs(mr), 1e-3)
@@ -164,12 +153,22 @@ def test_one_iteration_reference_numerics_vs_reference_gpu_build(engine, psf, st
           "p50 %.2e p99 %.2e max %.2e, chi2 rel p99 %.2e"
           % (sameh, np.percentile(relh[:, :9], 50), np.percentile(relh[:, :9], 99), relh[:, :9].max(),
              np.percentile(crelh, 99)))
-    assert (out["iters"] == ir).all()
-    assert same >= 0.99 and same > sameh
-    assert np.percentile(rel[:, :9], 99) < np.percentile(relh[:, :9], 99)
-    assert rel[:, :9].max() < 0.2
-    assert np.percentile(rel[:, :9], 99) < 2e-4
-    assert np.percentile(crel, 99) < 5e-4
+    for name, out in H.invert_each_kernel(engine, gcfg, obs):
+        rel = np.abs(out["model64"] - mr) / np.maximum(np.abs(mr), 1e-3)
+        crel = np.abs(out["chi2"] - cr) / cr
+        # the output is the last accepted model: a different accept/reject
+        # decision shows as a whole step's difference, far above 1e-3
+        same = (rel[:, :9].max(axis=1) < 1e-3).mean()
+        print("%s, one iteration, REFERENCE numerics vs reference sm_100a build: same decision %.4f, "
+              "model rel p50 %.2e p99 %.2e max %.2e, chi2 rel p99 %.2e"
+              % (name, same, np.percentile(rel[:, :9], 50), np.percentile(rel[:, :9], 99), rel[:, :9].max(),
+                 np.percentile(crel, 99)))
+        assert (out["iters"] == ir).all(), name
+        assert same >= 0.99 and same > sameh, name
+        assert np.percentile(rel[:, :9], 99) < np.percentile(relh[:, :9], 99), name
+        assert rel[:, :9].max() < 0.2, name
+        assert np.percentile(rel[:, :9], 99) < 2e-4, name
+        assert np.percentile(crel, 99) < 5e-4, name
 
 
 @pytest.mark.skipif(not ref.available(), reason="libgmref_cpu.so not built")
@@ -192,13 +191,12 @@ def test_macroturbulence_iteration_matches_reference_host_build(engine, fix):
     t = H.truth_models(1024, rng, alpha_range=(0.7, 1.0))
     t[:, 9] = rng.uniform(0.3, 2.0, len(t))
     obs = H.observations(ocfg, t, rng, slight=sl)
-    engine.configure(gcfg)
-    out = engine.invert(obs)
     mr, cr, ir, _ = ref.invert_cpu(ref.setup_from_cfg(ocfg), obs, slight=sl)
-    rel = np.abs(out["model64"] - mr) / np.maximum(np.abs(mr), 1e-3)
-    crel = np.abs(out["chi2"] - cr) / cr
-    print("v_mac one iteration (%d terms): model rel p99 %.2e, chi2 rel p99 %.2e"
-          % (engine.nterms, np.percentile(rel, 99), np.percentile(crel, 99)))
-    assert (out["iters"] == ir).all()
-    assert np.percentile(rel, 99) < 1e-4
-    assert np.percentile(crel, 99) < 1e-4
+    for name, out in H.invert_each_kernel(engine, gcfg, obs):
+        rel = np.abs(out["model64"] - mr) / np.maximum(np.abs(mr), 1e-3)
+        crel = np.abs(out["chi2"] - cr) / cr
+        print("%s, v_mac one iteration (%d terms): model rel p99 %.2e, chi2 rel p99 %.2e"
+              % (name, engine.nterms, np.percentile(rel, 99), np.percentile(crel, 99)))
+        assert (out["iters"] == ir).all(), name
+        assert np.percentile(rel, 99) < 1e-4, name
+        assert np.percentile(crel, 99) < 1e-4, name
