@@ -13,6 +13,7 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 
 #include "gmilos.h"
@@ -871,29 +872,199 @@ __device__ __forceinline__ int jrow(const DevCfg& c, uint32_t fixmask, int t, in
   return r;
 }
 
+// Entry e of the normal equations in the order they are summed and stored:
+// alpha's packed upper triangle (e < NT (NT + 1) / 2, row-major, as upk),
+// then beta (column NT of J' W J'^T).  Returns a * 16 + b for operand rows
+// a <= b (b = NT: the residual).
+template <int NT>
+__host__ __device__ constexpr int ne_entry(int e) {
+  int a = 0, len = NT;
+  while (a < NT && e >= len) {
+    e -= len;
+    ++a;
+    len = NT - a;
+  }
+  return a < NT ? a * 16 + a + e : e * 16 + NT;
+}
+template <int NT>
+__host__ __device__ constexpr int ne_entries() { return NT * (NT + 1) / 2 + NT; }
+
+// Factors of the stray-light fraction alpha in entry e (0, 1 or 2: one per
+// operand row that me_der.cu:191-211 scales, every RF but alpha's own), two
+// bits per entry, 32 entries per word.
+template <int NT>
+__host__ __device__ constexpr uint64_t ne_alfa_bits(int word) {
+  uint64_t w = 0;
+  for (int i = 0; i < 32; ++i) {
+    const int e = 32 * word + i;
+    if (e >= ne_entries<NT>()) break;
+    const int ab = ne_entry<NT>(e), a = ab >> 4, b = ab & 15;
+    w |= (uint64_t)((a < NT - 1 ? 1 : 0) + (b < NT - 1 ? 1 : 0)) << (2 * i);
+  }
+  return w;
+}
+
+// Reduce-scatter of N per-lane partial sums (N a power of two, <= 32) over
+// the warp by a shuffle butterfly: at each of the five steps a lane keeps
+// half of its values and adds its partner's copy of them, so every step
+// halves the values a lane holds; once a lane holds one value the rest of
+// the steps are plain butterfly sums.  Returns, in every lane, the warp sum
+// of entry lane >> (5 - log2 N).
+template <int N>
+__device__ __forceinline__ float warp_reduce_scatter(float (&v)[N], int lane) {
+  static_assert(N >= 1 && N <= 32 && (N & (N - 1)) == 0, "N must be a power of two <= 32");
+#pragma unroll
+  for (int st = 0; st < 5; ++st) {
+    const int m = 16 >> st, h = (N >> st) / 2;
+    if (h >= 1) {
+      const bool up = (lane & m) != 0;
+#pragma unroll
+      for (int j = 0; j < h; ++j) {
+        const float send = up ? v[j] : v[j + h];
+        const float keep = up ? v[j + h] : v[j];
+        v[j] = keep + __shfl_xor_sync(kFull, send, m);
+      }
+    } else {
+      v[0] += __shfl_xor_sync(kFull, v[0], m);
+    }
+  }
+  return v[0];
+}
+
+// acc[i] += w x_a x_b for entry P0 + i = (a, b) of every i in I..., the
+// operand rows of each entry fixed at compile time.
+template <int NT, int E>
+__device__ __forceinline__ void ne_product(float& acc, const float (&x)[NT + 1], float w) {
+  if constexpr (E < ne_entries<NT>()) {
+    constexpr int ab = ne_entry<NT>(E), a = ab >> 4, b = ab & 15;
+    acc = fmaf(w * x[a], x[b], acc);
+  }
+}
+template <int NT, int P0, int N, int... I>
+__device__ __forceinline__ void ne_products(float (&acc)[N], const float (&x)[NT + 1], float w,
+                                            std::integer_sequence<int, I...>) {
+  (ne_product<NT, P0 + I>(acc[I], x, w), ...);
+}
+
+// The operand rows of term t = 0 .. NT (NT: the residual) for Stokes s, as
+// offsets into the staged rows, and this lane's samples of them.
+template <int LPL, int V>
+__device__ __forceinline__ void ne_operands(const DevCfg& c, uint32_t fixmask, bool mac_on, const float* rows0,
+                                            int s, int l, float (&x)[Variant<V>::NT + 1]) {
+  constexpr int NT = Variant<V>::NT;
+#pragma unroll
+  for (int t = 0; t <= NT; ++t) {
+    bool scaled;
+    x[t] = rows0[jrow<LPL, V>(c, fixmask, t, s, mac_on, scaled) * row_pitch<LPL>() + l];
+  }
+}
+
+// Entries [P0, P0 + N) of the normal equations (ne_entry order; entries past
+// the last are zero): each lane sums w_s x_a x_b over its own samples and
+// the four Stokes parameters in FP32, then warp_reduce_scatter adds the
+// lanes' sums.  The operand rows are read unscaled by alpha.
+template <int LPL, int V, int P0, int N>
+__device__ __forceinline__ float ne_pass(const DevCfg& c, uint32_t fixmask, bool mac_on, const float* rows0,
+                                         int lane) {
+  constexpr int NT = Variant<V>::NT;
+  float acc[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) acc[i] = 0.f;
+#pragma unroll 1
+  for (int s = 0; s < 4; ++s) {
+    const float w = c.wsig[s];
+#pragma unroll
+    for (int k = 0; k < LPL; ++k) {
+      float x[NT + 1];
+      ne_operands<LPL, V>(c, fixmask, mac_on, rows0, s, lane + 32 * k, x);
+      ne_products<NT, P0>(acc, x, w, std::make_integer_sequence<int, N>{});
+    }
+  }
+  return warp_reduce_scatter<N>(acc, lane);
+}
+
+// Entries [0, 64) in one pass (the operand rows are read once): the
+// butterfly's first step leaves 32 values per lane, the remaining four
+// halve them as in warp_reduce_scatter, and lane L ends with entries 2L and
+// 2L + 1.
+template <int LPL, int V>
+__device__ __forceinline__ float2 ne_pass64(const DevCfg& c, uint32_t fixmask, bool mac_on, const float* rows0,
+                                            int lane) {
+  constexpr int NT = Variant<V>::NT;
+  float acc[64];
+#pragma unroll
+  for (int i = 0; i < 64; ++i) acc[i] = 0.f;
+#pragma unroll 1
+  for (int s = 0; s < 4; ++s) {
+    const float w = c.wsig[s];
+#pragma unroll
+    for (int k = 0; k < LPL; ++k) {
+      float x[NT + 1];
+      ne_operands<LPL, V>(c, fixmask, mac_on, rows0, s, lane + 32 * k, x);
+      ne_products<NT, 0>(acc, x, w, std::make_integer_sequence<int, 64>{});
+    }
+  }
+  // a lane keeps entries [0, 32) (lane bit 4 clear) or [32, 64) and adds
+  // its partner's sums of them
+  float v[32];
+  const bool up = (lane & 16) != 0;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const float send = up ? acc[j] : acc[32 + j];
+    v[j] = (up ? acc[32 + j] : acc[j]) + __shfl_xor_sync(kFull, send, 16);
+  }
+#pragma unroll
+  for (int st = 1; st < 5; ++st) {
+    const int m = 16 >> st, h = 32 >> st;
+    const bool u = (lane & m) != 0;
+#pragma unroll
+    for (int j = 0; j < h; ++j) {
+      const float send = u ? v[j] : v[j + h];
+      const float keep = u ? v[j + h] : v[j];
+      v[j] = keep + __shfl_xor_sync(kFull, send, m);
+    }
+  }
+  return make_float2(v[0], v[1]);
+}
+
+// Store entry e of the normal equations: times alpha once per scaled operand
+// row (me_der.cu:191-211; in FP64, then rounded to float), into sm.alpha
+// (packed) or sm.beta.
+template <int LPL, int V>
+__device__ __forceinline__ void ne_store(const DevCfg& c, double alfa, int e, float v, WarpSmem<LPL, V>& sm) {
+  constexpr int NT = Variant<V>::NT, NA = NT * (NT + 1) / 2;
+  constexpr uint64_t w0 = ne_alfa_bits<NT>(0), w1 = ne_alfa_bits<NT>(1), w2 = ne_alfa_bits<NT>(2);
+  if (c.use_slight) {
+    const uint64_t w = e < 32 ? w0 : e < 64 ? w1 : w2;
+    const int f = (int)((w >> (2 * (e & 31))) & 3u);
+    if (f) v = (float)((double)v * (f == 2 ? alfa * alfa : alfa));
+  }
+  if (e < NA) sm.alpha[e] = v;
+  else sm.beta[e - NA] = v;
+}
+
 // Normal equations alpha = sum_s w_s/sigma^2 J^T J and beta = sum_s w_s J^T
 // (syn - obs) / sigma^2 (covarmf, lib.cu:65-118; covarm, lib.cu:12-63 for
-// 11 terms) as one product J' W J'^T on the FP64 tensor cores: J' holds the
-// NT response functions and, as row NT, the residual, over the 4 nl columns
-// of the Stokes profiles; W the weights w_s / sigma^2.  alpha is the leading
-// NT x NT block and beta column NT: 8x8 tiles (0,0) and (0,1) of the
-// symmetric 16x16 result on the tensor cores (for this operand layout a
-// lane's B element of J'^T is its A element of J'), and of tile (1,1) the
-// few wanted entries -- rows 8 .. NT - 1 with themselves and with the
-// residual -- on the CUDA cores with warp sums, which frees the FP64 tensor
-// pipe that bounds the accept kernel.  The reference sums each Stokes parameter in
-// float; here the products and sums are double and alpha, beta are rounded
-// to float once.  Results land in sm.alpha (packed) and sm.beta.  alpha's RF
-// is taken from the mixed profile `syn` when alpha_mixed
-// (milosUtils.cu:675), else from the unmixed `pure`.
+// 11 terms) in FP32 with warp-level reductions, as the reference sums them
+// in FP32: J' holds the NT response functions and, as row NT, the residual,
+// over the 4 nl columns of the Stokes profiles.  Each lane forms the
+// weighted products of its own samples for the first 64 entries and a
+// shuffle butterfly sums them over the warp, then the last 1 (10 terms) or
+// 13 (11 terms) entries the same way.  The reference sums each Stokes
+// parameter sequentially and then the four in order; here every entry is
+// one FP32 sum over the weighted products, in the order of a lane's
+// samples, then a tree over the lanes.  The stray-light factor alpha of the
+// scaled rows (me_der.cu:191-211) is applied to the sums in FP64.  alpha's
+// RF is taken from the mixed profile `syn` when alpha_mixed
+// (milosUtils.cu:675), else from the unmixed `pure`.  Results land in
+// sm.alpha (packed) and sm.beta.
 template <int LPL, int V>
 __device__ __forceinline__ void normal_eq(const DevCfg& c, const double* m, bool alpha_mixed,
                                           const float (&pure)[LPL][4], const float (&sl)[LPL][4],
                                           const float (&syn)[LPL][4], const float (&ob)[LPL][4],
                                           const bool (&valid)[LPL], int lane, WarpSmem<LPL, V>& sm) {
-  constexpr int NT = Variant<V>::NT;
-  constexpr int S = 32 * LPL;
-  static_assert(NT < 16, "the residual row must fit the 16-row operand");
+  constexpr int NT = Variant<V>::NT, NE = ne_entries<NT>();
+  static_assert(NE > 64 && NE <= 80, "64 entries, then up to 16");
   const double alfa = m[ALFA];
   bool mac_on = false;
   if constexpr (Variant<V>::MAC) mac_on = m[MAC] > 0.0001;
@@ -909,84 +1080,18 @@ __device__ __forceinline__ void normal_eq(const DevCfg& c, const double* m, bool
     }
   }
   __syncwarp();
-  const int gr = lane >> 2, gc = lane & 3;
   uint32_t fixmask = 0;
 #pragma unroll
   for (int i = 0; i < 11; ++i) fixmask |= (c.fix[i] ? 1u : 0u) << i;
   const float* rows0 = &sm.rows[0][0];
-  double d00[2] = {0.0, 0.0}, d01[2] = {0.0, 0.0};
-#pragma unroll 1
-  for (int s = 0; s < 4; ++s) {
-    bool s0d, s1d;
-    const float* r0 = rows0 + jrow<LPL, V>(c, fixmask, gr, s, mac_on, s0d) * row_pitch<LPL>();
-    const float* r1 = rows0 + jrow<LPL, V>(c, fixmask, 8 + gr, s, mac_on, s1d) * row_pitch<LPL>();
-    const double sc0 = s0d ? alfa : 1.0, sc1 = s1d ? alfa : 1.0;
-    const double wd = (double)c.wsig[s];
-#pragma unroll 4
-    for (int k0 = 0; k0 < S; k0 += 4) {
-      const double x0 = (double)r0[k0 + gc] * sc0, x1 = (double)r1[k0 + gc] * sc1;
-      dmma_884(d00[0], d00[1], wd * x0, x0);
-      dmma_884(d01[0], d01[1], wd * x0, x1);
-    }
-  }
-  // rows 8 .. NT - 1 of J' with themselves and with the residual (tile
-  // (1, 1), of which only R (R + 3) / 2 entries are wanted) on the CUDA
-  // cores: each lane its own samples, then warp sums
-  constexpr int R = NT - 8, NE = R * (R + 3) / 2;
-  double acc[NE];
-#pragma unroll
-  for (int e = 0; e < NE; ++e) acc[e] = 0.0;
-#pragma unroll 1
-  for (int s = 0; s < 4; ++s) {
-    const double wd = (double)c.wsig[s];
-    const float* rr[R + 1];
-    double sc[R + 1];
-#pragma unroll
-    for (int t = 0; t <= R; ++t) {
-      bool scl;
-      rr[t] = rows0 + jrow<LPL, V>(c, fixmask, 8 + t, s, mac_on, scl) * row_pitch<LPL>();
-      sc[t] = scl ? alfa : 1.0;
-    }
-#pragma unroll
-    for (int k = 0; k < LPL; ++k) {
-      const int l = lane + 32 * k;
-      double x[R + 1];
-#pragma unroll
-      for (int t = 0; t <= R; ++t) x[t] = (double)rr[t][l] * sc[t];
-      int e = 0;
-#pragma unroll
-      for (int a = 0; a < R; ++a) {
-        const double wx = wd * x[a];
-#pragma unroll
-        for (int b = a; b <= R; ++b, ++e) acc[e] = fma(wx, x[b], acc[e]);
-      }
-    }
-  }
-  // lane holds element (gr, 2 gc + i) of each tensor-core tile
-#pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const int q = 2 * gc + i;
-    const int row[2] = {gr, gr}, col[2] = {q, 8 + q};
-    const double val[2] = {d00[i], d01[i]};
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      if (row[e] <= col[e] && col[e] < NT) sm.alpha[upk<NT>(row[e], col[e])] = (float)val[e];
-      else if (col[e] == NT && row[e] < NT) sm.beta[row[e]] = (float)val[e];
-    }
-  }
-  {
-    int e = 0;
-#pragma unroll
-    for (int a = 0; a < R; ++a)
-#pragma unroll
-      for (int b = a; b <= R; ++b, ++e) {
-        const double v = warp_sum_d(acc[e]);
-        if (lane == 0) {
-          if (b < R) sm.alpha[upk<NT>(8 + a, 8 + b)] = (float)v;
-          else sm.beta[8 + a] = (float)v;
-        }
-      }
-  }
+  const float2 v01 = ne_pass64<LPL, V>(c, fixmask, mac_on, rows0, lane);
+  ne_store<LPL, V>(c, alfa, 2 * lane, v01.x, sm);
+  ne_store<LPL, V>(c, alfa, 2 * lane + 1, v01.y, sm);
+  constexpr int R = NE - 64, NL = R <= 1 ? 1 : R <= 2 ? 2 : R <= 4 ? 4 : R <= 8 ? 8 : 16;
+  const float v2 = ne_pass<LPL, V, 64, NL>(c, fixmask, mac_on, rows0, lane);
+  constexpr int sh = NL == 1 ? 5 : NL == 2 ? 4 : NL == 4 ? 3 : NL == 8 ? 2 : 1;
+  const int e2 = 64 + (lane >> sh);
+  if ((lane & ((1 << sh) - 1)) == 0 && e2 < NE) ne_store<LPL, V>(c, alfa, e2, v2, sm);
   __syncwarp();
 }
 
