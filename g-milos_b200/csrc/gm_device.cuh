@@ -6,10 +6,11 @@
 // follows the reference's precision choices: FP32 with the same fast
 // intrinsics (__fdividef, __sincosf), FP64 for the Voigt polynomials and
 // wherever the reference keeps PRECISION=double (model parameters,
-// classical estimates, the PSF convolution).  The two matrix products of a
-// step -- the PSF convolution of the staged rows and the normal equations --
-// run on the FP64 tensor cores (mma.sync m8n8k4).  file:line citations name
-// the reference code each piece reproduces.
+// classical estimates, the PSF convolution).  The PSF convolution of the
+// staged rows runs on the FP64 tensor cores (mma.sync m8n8k4); the normal
+// equations are FP32 sums with warp-level reductions, as the reference
+// forms them in FP32.  file:line citations name the reference code each
+// piece reproduces.
 #pragma once
 
 #include <cstdint>
