@@ -126,13 +126,13 @@ def test_one_iteration_reference_numerics_vs_reference_gpu_build(engine, psf, st
     numerics -- the reference's __sincosf / __fdividef in the solve and the
     angles -- against the reference's own sm_100a build.  The two builds
     round the synthesis, the response functions and the normal equations
-    differently (FMA contraction chosen by two compilations; the engine's
-    normal equations in FP64 on the tensor cores where the reference sums
-    them in FP32, lib.cu:65-118 -- on the CPU restatement that difference
-    alone moves one step by p99 1.5e-5), and the 18-step Jacobi with the
-    hardware trigonometry amplifies last-bit differences of alpha into step
-    differences (measured: model p99 5e-5 to 1e-4, chi2 p99 1.4e-4 to
-    1.9e-4, 99.4-99.7 % of pixels within 1e-3, the largest difference 5 % of
+    differently (FMA contraction chosen by two compilations; both sum the
+    normal equations in FP32, the reference each Stokes parameter in
+    sequence, lib.cu:65-118, the engine per lane and then as a tree over
+    the lanes), and the 18-step Jacobi with the hardware trigonometry
+    amplifies last-bit differences of alpha into step differences
+    (measured: model p99 5e-5 to 1e-4, chi2 p99 1.6e-4 to 1.9e-4,
+    99.3-99.6 % of pixels within 1e-3, the largest difference 5 % of
     a parameter -- a step-size difference, far below a whole step, so no
     accept/reject decision differs).  The same step by the reference's own
     host build (libm trigonometry) lands within 1e-3 of its sm_100a build
