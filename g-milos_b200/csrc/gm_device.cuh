@@ -212,6 +212,9 @@ struct WarpSmem {
   // the normal equations' operand rows (kX*), right after `rows` with the
   // same pitch: row NR + x of the combined array is xrows[x]
   float xrows[kXRows][row_pitch<LPL>()];
+  // offsets of the normal equations' operand rows per Stokes parameter and
+  // term (jrow times the pitch; 12 per parameter, the last unused)
+  alignas(16) int nero[4][12];
 };
 
 template <int LPL>
@@ -947,17 +950,23 @@ __device__ __forceinline__ void ne_products(float (&acc)[N], const float (&x)[NT
   (ne_product<NT, P0 + I>(acc[I], x, w), ...);
 }
 
-// The operand rows of term t = 0 .. NT (NT: the residual) for Stokes s, as
-// offsets into the staged rows, and this lane's samples of them.
+// This lane's samples l of the operand rows of term t = 0 .. NT (NT: the
+// residual) for one Stokes parameter, whose row offsets are ro[0 .. 11].
 template <int LPL, int V>
-__device__ __forceinline__ void ne_operands(const DevCfg& c, uint32_t fixmask, bool mac_on, const float* rows0,
-                                            int s, int l, float (&x)[Variant<V>::NT + 1]) {
+__device__ __forceinline__ void ne_operands(const int* ro, const float* rows0, int l,
+                                            float (&x)[Variant<V>::NT + 1]) {
   constexpr int NT = Variant<V>::NT;
+  int o[12];
 #pragma unroll
-  for (int t = 0; t <= NT; ++t) {
-    bool scaled;
-    x[t] = rows0[jrow<LPL, V>(c, fixmask, t, s, mac_on, scaled) * row_pitch<LPL>() + l];
+  for (int q = 0; q < 3; ++q) {
+    const int4 v = reinterpret_cast<const int4*>(ro)[q];
+    o[4 * q] = v.x;
+    o[4 * q + 1] = v.y;
+    o[4 * q + 2] = v.z;
+    o[4 * q + 3] = v.w;
   }
+#pragma unroll
+  for (int t = 0; t <= NT; ++t) x[t] = rows0[o[t] + l];
 }
 
 // Entries [P0, P0 + N) of the normal equations (ne_entry order; entries past
@@ -965,8 +974,7 @@ __device__ __forceinline__ void ne_operands(const DevCfg& c, uint32_t fixmask, b
 // the four Stokes parameters in FP32, then warp_reduce_scatter adds the
 // lanes' sums.  The operand rows are read unscaled by alpha.
 template <int LPL, int V, int P0, int N>
-__device__ __forceinline__ float ne_pass(const DevCfg& c, uint32_t fixmask, bool mac_on, const float* rows0,
-                                         int lane) {
+__device__ __forceinline__ float ne_pass(const DevCfg& c, const WarpSmem<LPL, V>& sm, int lane) {
   constexpr int NT = Variant<V>::NT;
   float acc[N];
 #pragma unroll
@@ -977,7 +985,7 @@ __device__ __forceinline__ float ne_pass(const DevCfg& c, uint32_t fixmask, bool
 #pragma unroll
     for (int k = 0; k < LPL; ++k) {
       float x[NT + 1];
-      ne_operands<LPL, V>(c, fixmask, mac_on, rows0, s, lane + 32 * k, x);
+      ne_operands<LPL, V>(sm.nero[s], &sm.rows[0][0], lane + 32 * k, x);
       ne_products<NT, P0>(acc, x, w, std::make_integer_sequence<int, N>{});
     }
   }
@@ -989,8 +997,7 @@ __device__ __forceinline__ float ne_pass(const DevCfg& c, uint32_t fixmask, bool
 // halve them as in warp_reduce_scatter, and lane L ends with entries 2L and
 // 2L + 1.
 template <int LPL, int V>
-__device__ __forceinline__ float2 ne_pass64(const DevCfg& c, uint32_t fixmask, bool mac_on, const float* rows0,
-                                            int lane) {
+__device__ __forceinline__ float2 ne_pass64(const DevCfg& c, const WarpSmem<LPL, V>& sm, int lane) {
   constexpr int NT = Variant<V>::NT;
   float acc[64];
 #pragma unroll
@@ -1001,7 +1008,7 @@ __device__ __forceinline__ float2 ne_pass64(const DevCfg& c, uint32_t fixmask, b
 #pragma unroll
     for (int k = 0; k < LPL; ++k) {
       float x[NT + 1];
-      ne_operands<LPL, V>(c, fixmask, mac_on, rows0, s, lane + 32 * k, x);
+      ne_operands<LPL, V>(sm.nero[s], &sm.rows[0][0], lane + 32 * k, x);
       ne_products<NT, 0>(acc, x, w, std::make_integer_sequence<int, 64>{});
     }
   }
@@ -1080,16 +1087,21 @@ __device__ __forceinline__ void normal_eq(const DevCfg& c, const double* m, bool
       sm.xrows[kXRes + s][l] = valid[k] ? syn[k][s] - ob[k][s] : 0.f;
     }
   }
-  __syncwarp();
   uint32_t fixmask = 0;
 #pragma unroll
   for (int i = 0; i < 11; ++i) fixmask |= (c.fix[i] ? 1u : 0u) << i;
-  const float* rows0 = &sm.rows[0][0];
-  const float2 v01 = ne_pass64<LPL, V>(c, fixmask, mac_on, rows0, lane);
+  // the operand rows' offsets: one (Stokes, term) pair per lane
+  for (int i = lane; i < 48; i += 32) {
+    const int s = i / 12, t = i - 12 * s;
+    bool scaled;
+    sm.nero[s][t] = t <= NT ? jrow<LPL, V>(c, fixmask, t, s, mac_on, scaled) * row_pitch<LPL>() : 0;
+  }
+  __syncwarp();
+  const float2 v01 = ne_pass64<LPL, V>(c, sm, lane);
   ne_store<LPL, V>(c, alfa, 2 * lane, v01.x, sm);
   ne_store<LPL, V>(c, alfa, 2 * lane + 1, v01.y, sm);
   constexpr int R = NE - 64, NL = R <= 1 ? 1 : R <= 2 ? 2 : R <= 4 ? 4 : R <= 8 ? 8 : 16;
-  const float v2 = ne_pass<LPL, V, 64, NL>(c, fixmask, mac_on, rows0, lane);
+  const float v2 = ne_pass<LPL, V, 64, NL>(c, sm, lane);
   constexpr int sh = NL == 1 ? 5 : NL == 2 ? 4 : NL == 4 ? 3 : NL == 8 ? 2 : 1;
   const int e2 = 64 + (lane >> sh);
   if ((lane & ((1 << sh) - 1)) == 0 && e2 < NE) ne_store<LPL, V>(c, alfa, e2, v2, sm);
