@@ -1,10 +1,12 @@
-"""Host-side layout of the wave-synchronous inversion state (no device):
+"""Host-side layout checks (no device).  The wave-synchronous inversion state:
 the buffer that gm::wave_buffers carves for a chunk -- LM records, staging
 blocks, wave counters, three pixel lists -- must hold every region inside
 gm::wave_buffer_bytes, disjoint and aligned, for every grid size and
 iteration limit.  A small host program is compiled against the engine's
 headers and linked to the engine library; it only does pointer arithmetic
-on a made-up base address."""
+on a made-up base address.  The normal equations' compile-time entry
+table: alpha's packed upper triangle, then beta, each operand pair once,
+with the stray-light factor of each entry."""
 import os
 import shutil
 import subprocess
@@ -70,6 +72,51 @@ def test_wave_buffers_fit_and_do_not_overlap(tmp_path):
     src.write_text(PROGRAM)
     cmd = [NVCC, "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(PKG, "csrc"), str(src),
            "-o", str(exe), "-L", os.path.dirname(LIB), "-lgmilos", "-Xlinker", "-rpath=" + os.path.dirname(LIB)]
+    build = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+    assert build.returncode == 0, build.stderr[-2000:]
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert run.returncode == 0 and run.stdout.strip().endswith("OK"), run.stdout[-2000:] + run.stderr[-500:]
+
+
+NE_PROGRAM = r"""
+#include <cstdio>
+#include "gm_device.cuh"
+
+// The normal equations' entry table (host-evaluated constexpr functions):
+// alpha's packed upper triangle in upk order, then beta, every operand pair
+// once; the stray-light factor bits count the scaled rows of each entry.
+template <int NT>
+int check() {
+  int bad = 0;
+  constexpr int NE = gm::ne_entries<NT>(), NA = NT * (NT + 1) / 2;
+  static_assert(NE == NA + NT, "entries");
+  int seen[16][16] = {};
+  for (int e = 0; e < NE; ++e) {
+    const int ab = gm::ne_entry<NT>(e), a = ab >> 4, b = ab & 15;
+    if (!(a >= 0 && a < NT && b >= a && b <= NT)) { std::printf("FAIL range NT=%d e=%d\n", NT, e); ++bad; continue; }
+    if (e < NA && (b == NT || gm::upk<NT>(a, b) != e)) { std::printf("FAIL alpha NT=%d e=%d\n", NT, e); ++bad; }
+    if (e >= NA && (b != NT || a != e - NA)) { std::printf("FAIL beta NT=%d e=%d\n", NT, e); ++bad; }
+    if (seen[a][b]++) { std::printf("FAIL twice NT=%d e=%d\n", NT, e); ++bad; }
+    const int f = (int)((gm::ne_alfa_bits<NT>(e / 32) >> (2 * (e % 32))) & 3u);
+    if (f != (a < NT - 1) + (b < NT - 1)) { std::printf("FAIL alfa NT=%d e=%d\n", NT, e); ++bad; }
+  }
+  return bad;
+}
+
+int main() {
+  const int bad = check<10>() + check<11>();
+  std::printf(bad ? "FAILED %d\n" : "OK\n", bad);
+  return bad ? 1 : 0;
+}
+"""
+
+
+def test_normal_equation_entry_table(tmp_path):
+    src = tmp_path / "ne.cu"
+    exe = tmp_path / "ne"
+    src.write_text(NE_PROGRAM)
+    cmd = [NVCC, "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(PKG, "csrc"), str(src),
+           "-o", str(exe)]
     build = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
     assert build.returncode == 0, build.stderr[-2000:]
     run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
