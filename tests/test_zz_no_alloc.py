@@ -96,7 +96,13 @@ def test_noalloc_matches_gm_invert_twice(nl, stray):
         np.testing.assert_allclose(got["chi2"], ref["chi2"], rtol=1e-6)
         np.testing.assert_array_equal(got["iters"], ref["iters"])
         np.testing.assert_array_equal(got["status"], ref["status"])
-        assert H.rel_to_I(got["fitted"], ref["fitted"]).max() < 1e-6
+        # the fitted profile is the last trial's synthesis, as the reference
+        # returns its working profile (milosUtils.cu:606); a rejected last
+        # trial of a pixel that wandered can be non-finite, in both calls alike
+        np.testing.assert_array_equal(np.isfinite(got["fitted"]), np.isfinite(ref["fitted"]))
+        fin = np.isfinite(ref["fitted"]).all(axis=(1, 2))
+        assert fin.mean() > 0.9
+        assert H.rel_to_I(got["fitted"][fin], ref["fitted"][fin]).max() < 1e-6
 
 
 def test_noalloc_rejects_what_it_cannot_do():
