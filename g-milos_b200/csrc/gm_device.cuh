@@ -1308,26 +1308,32 @@ __device__ __noinline__ void solve10(WarpSmem<LPL, V>& sm, const SolvePlan& pl, 
     float* tv = va; va = vb; vb = tv;
   }
   // 18 steps: the final matrix and vector are back in the first buffers, in
-  // the original index order.  z = (V^T beta) / w with the |w| <= 1e-12 cut.
+  // the original index order.  z = (V^T beta) / w with the |w| <= 1e-12 cut,
+  // component g in group lane g's register.
+  float y = 0.f;
   if (g < 10) {
     const float w = A[at(w2, 3)];
     const float inv = ((double)fabsf(w) > 1e-12) ? (1.f / w) : 0.f;
-    va[g] = va[g] * inv;
+    y = va[g] * inv;
   }
-  __syncwarp();
-  // delta = V z: undo the steps in reverse order
+  // delta = V z: undo the steps in reverse order.  Step `step` rotated
+  // components (2k, 2k + 1) of pair k and relabelled them to positions
+  // (r[2k], r[2k + 1]) of the round-robin permutation r = {0, 2, 4, 1, 6, 3,
+  // 8, 5, 9, 7}; undoing it, component g takes pair k = g / 2's two
+  // relabelled components from their lanes (shuffles; positions packed one
+  // nibble per pair) and that pair's rotation, transposed.
+  const int k = g < 10 ? g >> 1 : 4, base = lane - g;
+  const int y0_lane = base + (int)((0x98640u >> (4 * k)) & 0xfu);
+  const int y1_lane = base + (int)((0x75312u >> (4 * k)) & 0xfu);
+  const bool second = (g & 1) != 0;
 #pragma unroll 1
   for (int step = 17; step >= 0; --step) {
-    const float y0 = va[at(w1, 2)], y1 = va[at(w1, 3)];
-    const float cs = sm.cs[h][step][at(w2, 0)], sn = sm.sn[h][step][at(w2, 0)];
-    if (diag) {
-      vb[at(w1, 1)] = cs * y0 + sn * y1;
-      vb[at(w1, 1) + 1] = -sn * y0 + cs * y1;
-    }
-    __syncwarp();
-    float* tv = va; va = vb; vb = tv;
+    const float y0 = __shfl_sync(kFull, y, y0_lane), y1 = __shfl_sync(kFull, y, y1_lane);
+    const float cs = sm.cs[h][step][k], sn = sm.sn[h][step][k];
+    y = second ? -sn * y0 + cs * y1 : cs * y0 + sn * y1;
   }
-  // 18 swaps: the result is in sm.vec[h][0]
+  if (g < 10) sm.vec[h][0][g] = y;
+  __syncwarp();
 }
 
 // --------------------------------------------------------------- 11x11 solve (FP64)
